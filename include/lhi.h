@@ -1,0 +1,274 @@
+/*
+ * lhi.h -- C-ABI of the B200 liquid step (drop-in for the reference's
+ * LiquidModel<3> / CGSolver<3> pair).
+ *
+ * Every entry point returns an int status (LHI_OK == 0).  On failure the
+ * message is available from lhi_last_error() (thread-local).  No torch types,
+ * no C++ types: plain pointers and sizes only.
+ *
+ * Host buffers passed to the lhi_liquid_* calls are typed by the handle's
+ * precision: float for LHI_PRECISION_FP32 and LHI_PRECISION_MIXED, double for
+ * LHI_PRECISION_FP64 ("host scalar").  Integer fields are documented per field.
+ *
+ * Array layout of every grid field follows the reference's Array3
+ * (Array.h:78-83): index (x * ny + y) * nz + z, z fastest.
+ *   vx, wx, liquidWx, tempVx : (nx+1) x  ny    x  nz
+ *   vy, wy, liquidWy, tempVy :  nx    x (ny+1) x  nz
+ *   vz, wz, liquidWz, tempVz :  nx    x  ny    x (nz+1)
+ *   pressure, liquidPhi      :  nx    x  ny    x  nz
+ *   solidPhi, isValid        : (nx+1) x (ny+1) x (nz+1)
+ * Particles cross the boundary as AoS triples (x, y, z) per particle, like
+ * Particle<3>::position / velocity (ParticleSystem.h:5-22); the affine matrix
+ * is 9 values per particle in Eigen's column-major order (col a = C[3a..3a+2]).
+ *
+ * Threading: one host thread drives a handle; calls on one handle are not
+ * thread-safe; distinct handles are independent.  All device work of a handle
+ * is ordered on its own CUDA stream; calls that return host data synchronise.
+ */
+#ifndef LHI_H_
+#define LHI_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define LHI_API __declspec(dllexport)
+#else
+#define LHI_API __attribute__((visibility("default")))
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define LHI_OK 0
+#define LHI_E_INVALID_ARG 1
+#define LHI_E_CUDA 2
+#define LHI_E_OOM 3
+#define LHI_E_NOT_CONVERGED 4
+#define LHI_E_TIMEOUT 5
+#define LHI_E_NAN 6
+#define LHI_E_UNSUPPORTED 7
+
+/* ------------------------------------------------------------- precision */
+#define LHI_PRECISION_FP32 0  /* everything float: reference-compatible      */
+#define LHI_PRECISION_MIXED 1 /* float grid/particles/V-cycle, double CG x,
+                                 dots, true residual and final check         */
+#define LHI_PRECISION_FP64 2  /* everything double                            */
+
+/* preconditioner: CGSolver<3>::PrecondType (PressureSolver.h:84-86) */
+#define LHI_PRECOND_NONE 0
+#define LHI_PRECOND_JACOBI 1
+#define LHI_PRECOND_MULTIGRID 2
+
+/* stopping rule */
+#define LHI_TOL_ABSOLUTE 0 /* ||r|| < tol, as PressureSolver.cpp:871      */
+#define LHI_TOL_RELATIVE 1 /* ||r|| < tol * ||r0||                         */
+
+/* CG update of beta */
+#define LHI_CG_REFERENCE 0 /* Fletcher-Reeves rz_new/rz_old (PressureSolver.cpp:906) */
+#define LHI_CG_FLEXIBLE 1  /* Polak-Ribiere, safe for a varying preconditioner     */
+
+/* extrapolation flag semantics */
+#define LHI_EXTRAP_JACOBI 0 /* flags read from the previous sweep (deterministic) */
+
+typedef struct lhi_grid_desc {
+    int32_t dim[3];        /* gridDimension (SceneParameter.h:137)          */
+    int32_t reserved;
+    double min_coord[3];   /* minCoord, converted to the handle's scalar    */
+    double max_coord[3];   /* maxCoord                                      */
+} lhi_grid_desc;
+
+typedef struct lhi_solver_params {   /* SolverParameter<3> (SceneParameter.h:10-45) */
+    int32_t max_iterations;
+    int32_t preconditioner;          /* LHI_PRECOND_*                          */
+    double tolerance;
+    int32_t num_level;
+    int32_t num_pre_smooth;
+    int32_t num_post_smooth;
+    int32_t num_final_smooth;
+    double smoothing_factor;
+    int32_t tolerance_mode;          /* LHI_TOL_*        (0 = reference)       */
+    int32_t cg_variant;              /* LHI_CG_*         (0 = reference)       */
+    int32_t true_residual_every;     /* MIXED/FP64: recompute r = b - A x every
+                                        k iterations (0 = never)               */
+    int32_t reserved[5];
+} lhi_solver_params;
+
+typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> */
+    double density;                  /* liquid density (rho)                   */
+    double gravity;                  /* gravity along y                        */
+    double particle_radius;          /* 0 => 2 * dx.x (ParticleSystem.cpp:8)   */
+    int32_t extrapolate_iterations;  /* 0 => 5 (LiquidModel.cpp:948)           */
+    int32_t reserved[7];
+} lhi_liquid_params;
+
+typedef struct lhi_solve_stats {
+    int32_t iterations;        /* PCG iterations taken                        */
+    int32_t status;            /* LHI_OK or LHI_E_NOT_CONVERGED / LHI_E_NAN   */
+    double initial_residual;   /* ||r0|| over all cells (PressureSolver.cpp:868) */
+    double final_residual;     /* recursive ||r|| over interior fluid cells   */
+    double true_residual;      /* ||b - A x|| over interior fluid cells, or -1 */
+    double solve_ms;           /* device time of the solve (CUDA events)      */
+} lhi_solve_stats;
+
+/* Boundary tree node: BaseBoundary<3> family (Boundary.h:6-96). */
+#define LHI_BOUNDARY_RECT 0         /* RectBoundary                            */
+#define LHI_BOUNDARY_SOLID 1        /* SolidBoundary stub: Compute() == 1      */
+#define LHI_BOUNDARY_UNION 2        /* OperatorBoundary::Union  = min(l, r)    */
+#define LHI_BOUNDARY_INTERSECTION 3 /* OperatorBoundary::Intersection = max    */
+#define LHI_BOUNDARY_SUBTRACT 4     /* OperatorBoundary::Substract max(l, -r)  */
+#define LHI_BOUNDARY_NONE 5         /* OperatorBoundary::None = left child     */
+typedef struct lhi_boundary_node {
+    int32_t kind;
+    int32_t use_inside;
+    int32_t left;              /* child node index, -1 if none */
+    int32_t right;
+    double center[3];
+    double half_extent[3];
+} lhi_boundary_node;
+
+/* Fluid primitive for the seeded scene generator. */
+#define LHI_FLUID_BOX 0     /* a = min corner, b = max corner (half-open [a, b)) */
+#define LHI_FLUID_SPHERE 1  /* a = centre, b[0] = radius                        */
+typedef struct lhi_fluid_prim {
+    int32_t kind;
+    int32_t reserved;
+    double a[3];
+    double b[3];
+    double velocity[3];
+} lhi_fluid_prim;
+
+/* Grid / solver fields for lhi_liquid_get_field / lhi_liquid_set_field. */
+#define LHI_FIELD_VX 0
+#define LHI_FIELD_VY 1
+#define LHI_FIELD_VZ 2
+#define LHI_FIELD_WX 3
+#define LHI_FIELD_WY 4
+#define LHI_FIELD_WZ 5
+#define LHI_FIELD_LIQUID_WX 6
+#define LHI_FIELD_LIQUID_WY 7
+#define LHI_FIELD_LIQUID_WZ 8
+#define LHI_FIELD_TEMP_VX 9
+#define LHI_FIELD_TEMP_VY 10
+#define LHI_FIELD_TEMP_VZ 11
+#define LHI_FIELD_PRESSURE 12
+#define LHI_FIELD_LIQUID_PHI 13
+#define LHI_FIELD_SOLID_PHI 14
+#define LHI_FIELD_IS_VALID 15   /* uint8, (nx+1)(ny+1)(nz+1)                  */
+#define LHI_FIELD_RHS 16        /* CGSolver m_rhs                             */
+#define LHI_FIELD_X 17          /* CGSolver m_x                               */
+#define LHI_FIELD_P 18          /* CGSolver m_p                               */
+#define LHI_FIELD_R 19          /* CGSolver m_r[level]                        */
+#define LHI_FIELD_Z 20          /* CGSolver m_z[level]                        */
+#define LHI_FIELD_ADIAG 21      /* CGSolver m_Adiag[level]                    */
+#define LHI_FIELD_ACOEF 22      /* CGSolver m_Acoef[level]: 6 per cell, order
+                                   right, left, top, bottom, front, back
+                                   (read-only; expanded from face storage)   */
+#define LHI_FIELD_CELL_KEY 23   /* int32 per particle, device (sorted) order:
+                                   linear cell index of Point2Index(pos)      */
+#define LHI_FIELD_PARTICLE_ID 24 /* int32 per particle, device order: caller's
+                                   particle index                             */
+#define LHI_FIELD_CELL_START 25 /* int32, ncells + 1: first sorted particle of
+                                   each cell                                  */
+#define LHI_FIELD_COUNT 26
+
+typedef struct lhi_liquid lhi_liquid;  /* opaque handle: owns all device memory */
+
+/* ------------------------------------------------------------ lifecycle */
+/* LiquidModel<3>::LiquidModel (LiquidModel.cpp:479-504) + Grid<3>::Grid
+   (Grid.cpp:86-98) + CGSolver<3>::CGSolver (PressureSolver.cpp:422-447). */
+LHI_API int lhi_liquid_create(const lhi_grid_desc* grid, const lhi_solver_params* solver,
+                              const lhi_liquid_params* liquid, int32_t precision,
+                              lhi_liquid** out);
+LHI_API int lhi_liquid_destroy(lhi_liquid* h);
+LHI_API const char* lhi_last_error(void);
+LHI_API int lhi_liquid_precision(const lhi_liquid* h, int32_t* precision);
+LHI_API int lhi_liquid_sync(lhi_liquid* h);
+/* Grid spacing dx (Grid.cpp:94-97) as the handle computed it. */
+LHI_API int lhi_liquid_get_dx(const lhi_liquid* h, double dx[3]);
+
+/* ---------------------------------------------------------- scene input */
+/* LiquidModel<3>::ComputeSolidPhi (LiquidModel.cpp:563-611): evaluates the
+   boundary tree at the (N+1)^3 nodes on the device, then the face fractions. */
+LHI_API int lhi_liquid_set_boundary(lhi_liquid* h, const lhi_boundary_node* nodes,
+                                    int32_t count, int32_t root);
+/* Same, for a node SDF evaluated by the caller (BaseBoundary<3>::Compute on
+   the host): uploads solidPhi then computes liquidWx/y/z on the device. */
+LHI_API int lhi_liquid_set_solid_phi(lhi_liquid* h, const void* node_phi);
+/* ParticleSystem<3>::Resize + Set* (ParticleSystem.cpp:11-21, .h:40-45).
+   vel / affine may be NULL (zero).  Radius is the handle's particle radius. */
+LHI_API int lhi_liquid_set_particles(lhi_liquid* h, int64_t n, const void* pos,
+                                     const void* vel, const void* affine);
+/* ParticleSystem<3>::Get* in the caller's particle order; NULL skips. */
+LHI_API int lhi_liquid_get_particles(lhi_liquid* h, void* pos, void* vel, void* affine);
+LHI_API int lhi_liquid_num_particles(const lhi_liquid* h, int64_t* n);
+
+/* ------------------------------------------------------------ the step */
+/* LiquidModel<3>::PreStep (LiquidModel.cpp:514-517): Clear + ComputeLiquidPhi */
+LHI_API int lhi_liquid_pre_step(lhi_liquid* h, double dt);
+/* LiquidModel<3>::Step (LiquidModel.cpp:520-528): P2G, gravity, projection,
+   extrapolation, G2P, advection */
+LHI_API int lhi_liquid_step(lhi_liquid* h, double dt);
+/* LiquidModel<3>::PostStep (LiquidModel.cpp:531-537): divergence diagnostic */
+LHI_API int lhi_liquid_post_step(lhi_liquid* h, double dt);
+
+/* ------------------------------------------------------- stage entries */
+LHI_API int lhi_liquid_clear(lhi_liquid* h);                      /* Grid.cpp:157-169     */
+LHI_API int lhi_liquid_sort_particles(lhi_liquid* h);             /* cell-key radix sort  */
+LHI_API int lhi_liquid_compute_liquid_phi(lhi_liquid* h);         /* LiquidModel.cpp:540  */
+LHI_API int lhi_liquid_particle_to_grid(lhi_liquid* h);           /* LiquidModel.cpp:614  */
+LHI_API int lhi_liquid_apply_gravity(lhi_liquid* h, double dt);   /* LiquidModel.cpp:899  */
+LHI_API int lhi_liquid_projection(lhi_liquid* h, double dt);      /* LiquidModel.cpp:826-896 */
+LHI_API int lhi_liquid_velocity_update(lhi_liquid* h, double dt); /* LiquidModel.cpp:834-889 */
+LHI_API int lhi_liquid_extrapolate(lhi_liquid* h);                /* LiquidModel.cpp:938  */
+LHI_API int lhi_liquid_grid_to_particle(lhi_liquid* h);           /* LiquidModel.cpp:724  */
+LHI_API int lhi_liquid_advect_particles(lhi_liquid* h, double dt);/* LiquidModel.cpp:913  */
+/* LiquidModel<3>::ComputeDivergence (LiquidModel.cpp:1066-1083): mean over
+   fluid cells; max_abs is the max-norm of the same per-cell divergence. */
+LHI_API int lhi_liquid_compute_divergence(lhi_liquid* h, double* mean, double* max_abs);
+/* LiquidModel<3>::GetCFL (LiquidModel.h:49-55) */
+LHI_API int lhi_liquid_get_cfl(lhi_liquid* h, double* dt_out);
+
+/* -------------------------------------------------------------- solver */
+LHI_API int lhi_solver_init(lhi_liquid* h);                               /* PressureSolver.cpp:666 */
+LHI_API int lhi_solver_build_rhs(lhi_liquid* h);                          /* PressureSolver.cpp:682 */
+LHI_API int lhi_solver_build_lhs(lhi_liquid* h, double density, double dt); /* PressureSolver.cpp:544 */
+LHI_API int lhi_solver_apply_preconditioner(lhi_liquid* h);               /* PressureSolver.cpp:719 */
+/* CGSolver<3>::Solve (PressureSolver.cpp:839-934); stats may be NULL. */
+LHI_API int lhi_solver_solve(lhi_liquid* h, double density, double dt, lhi_solve_stats* stats);
+LHI_API int lhi_solver_get_stats(lhi_liquid* h, lhi_solve_stats* stats);
+/* CGSolver<3>::GetAx (PressureSolver.cpp:700-717) applied to a whole level:
+   out = A_level * x (host buffers, ncells(level) host scalars). */
+LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void* out);
+
+/* -------------------------------------------------------------- fields */
+LHI_API int lhi_liquid_field_size(const lhi_liquid* h, int32_t field, int32_t level,
+                                  int64_t* count, int32_t* elem_bytes);
+LHI_API int lhi_liquid_get_field(lhi_liquid* h, int32_t field, int32_t level, void* out);
+LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, const void* in);
+
+/* ------------------------------------------------- seeded scene builder */
+/* RectBoundary / OperatorBoundary::Compute (Boundary.h:38-90) on the host,
+   in the given precision (0 float, 2 double), at n points (xyz triples). */
+LHI_API int lhi_boundary_eval(const lhi_boundary_node* nodes, int32_t count, int32_t root,
+                              int32_t precision, const void* points, int64_t n, void* out);
+/* Seeds 8 jittered particles per fluid cell (2x2x2 sub-cells, jitter
+   +-0.25 sub-cell, counter-based RNG keyed by seed): a cell is seeded when
+   its centre is inside a fluid primitive and the boundary SDF there is >= 0.
+   Call with pos == NULL to get the count; then with buffers of that size. */
+LHI_API int lhi_scene_seed_particles(const lhi_grid_desc* grid, const lhi_boundary_node* nodes,
+                                     int32_t count, int32_t root, const lhi_fluid_prim* prims,
+                                     int32_t nprims, uint64_t seed, int32_t precision,
+                                     int64_t* n_out, void* pos, void* vel);
+/* ParticleSystem<3>::SpawnParticles (ParticleSystem.cpp:45-64): lattice of
+   spacing 0.5 * default_radius over [min, max), capped at max_count. */
+LHI_API int lhi_scene_spawn_lattice(const double min_coord[3], const double max_coord[3],
+                                    double default_radius, int64_t max_count,
+                                    int32_t precision, int64_t* n_out, void* pos);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LHI_H_ */
