@@ -69,8 +69,15 @@ extern "C" {
 #define LHI_CG_REFERENCE 0 /* Fletcher-Reeves rz_new/rz_old (PressureSolver.cpp:906) */
 #define LHI_CG_FLEXIBLE 1  /* Polak-Ribiere, safe for a varying preconditioner     */
 
-/* extrapolation flag semantics */
-#define LHI_EXTRAP_JACOBI 0 /* flags read from the previous sweep (deterministic) */
+/* cells on which PCG updates x and r and takes p.Ap and ||r|| */
+#define LHI_REGION_INTERIOR 0 /* fluid cells of [1, N-2]^3, as PressureSolver.cpp:874-899 */
+#define LHI_REGION_FLUID 1    /* every fluid cell: a consistent CG when fluid cells lie on
+                                 the domain's outer layer (one-cell walls)               */
+
+/* red-black smoother update */
+#define LHI_SMOOTHER_REFERENCE 0 /* z = (1 - w) z + w (r - A z) / diag, as PressureSolver.cpp:832:
+                                    A z includes the diagonal, so w = 0.5 gives z_GS / 2     */
+#define LHI_SMOOTHER_DAMPED_GS 1 /* z = z + w (r - A z) / diag: damped Gauss-Seidel           */
 
 typedef struct lhi_grid_desc {
     int32_t dim[3];        /* gridDimension (SceneParameter.h:137)          */
@@ -90,9 +97,11 @@ typedef struct lhi_solver_params {   /* SolverParameter<3> (SceneParameter.h:10-
     double smoothing_factor;
     int32_t tolerance_mode;          /* LHI_TOL_*        (0 = reference)       */
     int32_t cg_variant;              /* LHI_CG_*         (0 = reference)       */
-    int32_t true_residual_every;     /* MIXED/FP64: recompute r = b - A x every
-                                        k iterations (0 = never)               */
-    int32_t reserved[5];
+    int32_t true_residual_every;     /* recompute r = b - A x every k iterations
+                                        (0 = never)                            */
+    int32_t update_region;           /* LHI_REGION_* (0 = reference)           */
+    int32_t smoother;                /* LHI_SMOOTHER_* (0 = reference)         */
+    int32_t reserved[3];
 } lhi_solver_params;
 
 typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> */
@@ -225,7 +234,8 @@ LHI_API int lhi_liquid_extrapolate(lhi_liquid* h);                /* LiquidModel
 LHI_API int lhi_liquid_grid_to_particle(lhi_liquid* h);           /* LiquidModel.cpp:724  */
 LHI_API int lhi_liquid_advect_particles(lhi_liquid* h, double dt);/* LiquidModel.cpp:913  */
 /* LiquidModel<3>::ComputeDivergence (LiquidModel.cpp:1066-1083): mean over
-   fluid cells; max_abs is the max-norm of the same per-cell divergence. */
+   fluid cells; max_abs is the max-norm of the same per-cell divergence over
+   the fluid cells whose six faces the projection updates ([1, N-3]^3). */
 LHI_API int lhi_liquid_compute_divergence(lhi_liquid* h, double* mean, double* max_abs);
 /* LiquidModel<3>::GetCFL (LiquidModel.h:49-55) */
 LHI_API int lhi_liquid_get_cfl(lhi_liquid* h, double* dt_out);

@@ -38,6 +38,12 @@ TOL_RELATIVE = 1
 CG_REFERENCE = 0
 CG_FLEXIBLE = 1
 
+REGION_INTERIOR = 0
+REGION_FLUID = 1
+
+SMOOTHER_REFERENCE = 0
+SMOOTHER_DAMPED_GS = 1
+
 BOUNDARY_RECT = 0
 BOUNDARY_SOLID = 1
 BOUNDARY_UNION = 2
@@ -98,7 +104,8 @@ class SolverParams(C.Structure):
                 ("num_pre_smooth", C.c_int32), ("num_post_smooth", C.c_int32),
                 ("num_final_smooth", C.c_int32), ("smoothing_factor", C.c_double),
                 ("tolerance_mode", C.c_int32), ("cg_variant", C.c_int32),
-                ("true_residual_every", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("true_residual_every", C.c_int32), ("update_region", C.c_int32),
+                ("smoother", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class LiquidParams(C.Structure):
@@ -138,7 +145,7 @@ def make_grid_desc(dim, min_coord, max_coord):
 def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECOND_MULTIGRID,
                        num_level=4, num_pre_smooth=5, num_post_smooth=5, num_final_smooth=20,
                        smoothing_factor=0.5, tolerance_mode=TOL_ABSOLUTE, cg_variant=CG_REFERENCE,
-                       true_residual_every=0):
+                       true_residual_every=0, update_region=REGION_INTERIOR, smoother=SMOOTHER_REFERENCE):
     s = SolverParams()
     s.max_iterations = int(max_iterations)
     s.tolerance = float(tolerance)
@@ -151,6 +158,8 @@ def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECON
     s.tolerance_mode = int(tolerance_mode)
     s.cg_variant = int(cg_variant)
     s.true_residual_every = int(true_residual_every)
+    s.update_region = int(update_region)
+    s.smoother = int(smoother)
     return s
 
 

@@ -1,0 +1,310 @@
+// api.cu -- the C-ABI of include/lhi.h: argument checking, error reporting
+// (thread-local last error, int status codes) and dispatch to the handle's
+// precision-specific implementation.  No exception crosses the boundary.
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "impl.cuh"
+#include "lhi.h"
+
+struct lhi_liquid {
+    std::unique_ptr<lhi::LiquidBase> impl;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int from_cuda(const lhi::CudaError& e) {
+    int code = (e.code == cudaErrorMemoryAllocation) ? LHI_E_OOM : LHI_E_CUDA;
+    return fail(code, e.what());
+}
+
+template <class F> int guarded(F f) {
+    try {
+        return f();
+    } catch (const lhi::CudaError& e) {
+        return from_cuda(e);
+    } catch (const std::invalid_argument& e) {
+        return fail(LHI_E_INVALID_ARG, e.what());
+    } catch (const std::bad_alloc& e) {
+        return fail(LHI_E_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(LHI_E_CUDA, e.what());
+    }
+}
+
+#define NEED_HANDLE(h) \
+    if (!(h) || !(h)->impl) return fail(LHI_E_INVALID_ARG, "null handle")
+
+// Converts the caller's boundary tree (root + child indices, BaseBoundary
+// ownership layout of Boundary.h) into post-order so the device evaluates
+// each node once, children first.
+void emit(const lhi_boundary_node* nodes, int32_t count, int32_t idx, lhi::BoundaryProgram& prog, int depth,
+          int* slot) {
+    if (idx < 0 || idx >= count) throw std::invalid_argument("boundary tree: child index out of range");
+    if (depth > 64) throw std::invalid_argument("boundary tree: too deep (cycle?)");
+    const lhi_boundary_node& n = nodes[idx];
+    int l = -1, r = -1;
+    switch (n.kind) {
+        case LHI_BOUNDARY_RECT:
+        case LHI_BOUNDARY_SOLID: break;
+        case LHI_BOUNDARY_UNION:
+        case LHI_BOUNDARY_INTERSECTION:
+        case LHI_BOUNDARY_SUBTRACT:
+            emit(nodes, count, n.left, prog, depth + 1, &l);
+            emit(nodes, count, n.right, prog, depth + 1, &r);
+            break;
+        case LHI_BOUNDARY_NONE: emit(nodes, count, n.left, prog, depth + 1, &l); break;
+        default: throw std::invalid_argument("boundary tree: unknown node kind");
+    }
+    if (prog.count >= lhi::kMaxBoundaryNodes) throw std::invalid_argument("boundary tree: more than 32 nodes");
+    int k = prog.count++;
+    prog.kind[k] = n.kind;
+    prog.use_inside[k] = n.use_inside;
+    prog.left[k] = l;
+    prog.right[k] = r;
+    for (int i = 0; i < 3; ++i) {
+        prog.center[k][i] = n.center[i];
+        prog.half[k][i] = n.half_extent[i];
+    }
+    *slot = k;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lhi_set_error_message(const char* msg) { g_last_error = msg ? msg : ""; }
+
+LHI_API const char* lhi_last_error(void) { return g_last_error.c_str(); }
+
+LHI_API int lhi_liquid_create(const lhi_grid_desc* grid, const lhi_solver_params* solver,
+                              const lhi_liquid_params* liquid, int32_t precision, lhi_liquid** out) {
+    if (!grid || !solver || !liquid || !out) return fail(LHI_E_INVALID_ARG, "null argument");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        std::unique_ptr<lhi_liquid> h(new lhi_liquid());
+        switch (precision) {
+            case LHI_PRECISION_FP32:
+                h->impl.reset(new lhi::LiquidImpl<float, float>(*grid, *solver, *liquid, precision));
+                break;
+            case LHI_PRECISION_MIXED:
+                h->impl.reset(new lhi::LiquidImpl<float, double>(*grid, *solver, *liquid, precision));
+                break;
+            case LHI_PRECISION_FP64:
+                h->impl.reset(new lhi::LiquidImpl<double, double>(*grid, *solver, *liquid, precision));
+                break;
+            default: return fail(LHI_E_INVALID_ARG, "unknown precision");
+        }
+        *out = h.release();
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_destroy(lhi_liquid* h) {
+    if (!h) return LHI_OK;
+    return guarded([&]() -> int {
+        delete h;
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_precision(const lhi_liquid* h, int32_t* precision) {
+    NEED_HANDLE(h);
+    if (!precision) return fail(LHI_E_INVALID_ARG, "null argument");
+    *precision = h->impl->precision();
+    return LHI_OK;
+}
+
+LHI_API int lhi_liquid_sync(lhi_liquid* h) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        h->impl->sync();
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_get_dx(const lhi_liquid* h, double dx[3]) {
+    NEED_HANDLE(h);
+    if (!dx) return fail(LHI_E_INVALID_ARG, "null argument");
+    h->impl->dx(dx);
+    return LHI_OK;
+}
+
+LHI_API int lhi_liquid_set_boundary(lhi_liquid* h, const lhi_boundary_node* nodes, int32_t count, int32_t root) {
+    NEED_HANDLE(h);
+    if (!nodes || count <= 0) return fail(LHI_E_INVALID_ARG, "empty boundary tree");
+    return guarded([&]() -> int {
+        lhi::BoundaryProgram prog;
+        std::memset(&prog, 0, sizeof(prog));
+        int slot = -1;
+        emit(nodes, count, root, prog, 0, &slot);
+        prog.root = slot;
+        h->impl->set_boundary(prog);
+        h->impl->sync();
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_set_solid_phi(lhi_liquid* h, const void* node_phi) {
+    NEED_HANDLE(h);
+    if (!node_phi) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->set_solid_phi(node_phi);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_set_particles(lhi_liquid* h, int64_t n, const void* pos, const void* vel, const void* affine) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        h->impl->set_particles(n, pos, vel, affine);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_get_particles(lhi_liquid* h, void* pos, void* vel, void* affine) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        h->impl->get_particles(pos, vel, affine);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_num_particles(const lhi_liquid* h, int64_t* n) {
+    NEED_HANDLE(h);
+    if (!n) return fail(LHI_E_INVALID_ARG, "null argument");
+    *n = h->impl->num_particles();
+    return LHI_OK;
+}
+
+#define STAGE(name, call)                 \
+    LHI_API int name {                    \
+        NEED_HANDLE(h);                   \
+        return guarded([&]() -> int {     \
+            call;                         \
+            return LHI_OK;                \
+        });                               \
+    }
+
+STAGE(lhi_liquid_clear(lhi_liquid* h), h->impl->clear())
+STAGE(lhi_liquid_sort_particles(lhi_liquid* h), h->impl->sort_particles())
+STAGE(lhi_liquid_compute_liquid_phi(lhi_liquid* h), h->impl->compute_liquid_phi())
+STAGE(lhi_liquid_particle_to_grid(lhi_liquid* h), h->impl->particle_to_grid())
+STAGE(lhi_liquid_apply_gravity(lhi_liquid* h, double dt), h->impl->apply_gravity(dt))
+STAGE(lhi_liquid_velocity_update(lhi_liquid* h, double dt), h->impl->velocity_update(dt))
+STAGE(lhi_liquid_extrapolate(lhi_liquid* h), h->impl->extrapolate())
+STAGE(lhi_liquid_grid_to_particle(lhi_liquid* h), h->impl->grid_to_particle())
+STAGE(lhi_liquid_advect_particles(lhi_liquid* h, double dt), h->impl->advect(dt))
+STAGE(lhi_liquid_post_step(lhi_liquid* h, double dt), (void)dt; h->impl->sync())
+STAGE(lhi_solver_init(lhi_liquid* h), h->impl->solver_init())
+STAGE(lhi_solver_build_rhs(lhi_liquid* h), h->impl->build_rhs())
+STAGE(lhi_solver_build_lhs(lhi_liquid* h, double density, double dt), h->impl->build_lhs(density, dt))
+STAGE(lhi_solver_apply_preconditioner(lhi_liquid* h), h->impl->apply_preconditioner())
+
+// Projection and step report a NaN in the solve; a solve that stops at the
+// iteration cap is not an error here (the reference carries on as well), its
+// status is available from lhi_solver_get_stats.
+LHI_API int lhi_liquid_projection(lhi_liquid* h, double dt) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        int st = h->impl->projection(dt);
+        if (st == LHI_E_NAN) return fail(LHI_E_NAN, "pressure solve produced NaN/Inf");
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_pre_step(lhi_liquid* h, double dt) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int { return h->impl->pre_step(dt); });
+}
+
+LHI_API int lhi_liquid_step(lhi_liquid* h, double dt) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        int st = h->impl->step(dt);
+        if (st == LHI_E_NAN) return fail(LHI_E_NAN, "pressure solve produced NaN/Inf");
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_compute_divergence(lhi_liquid* h, double* mean, double* max_abs) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        h->impl->divergence(mean, max_abs);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_get_cfl(lhi_liquid* h, double* dt_out) {
+    NEED_HANDLE(h);
+    if (!dt_out) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        *dt_out = h->impl->cfl();
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_solver_solve(lhi_liquid* h, double density, double dt, lhi_solve_stats* stats) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        int st = h->impl->solve(density, dt);
+        if (stats) *stats = h->impl->stats();
+        if (st == LHI_E_NAN) return fail(LHI_E_NAN, "pressure solve produced NaN/Inf");
+        if (st == LHI_E_NOT_CONVERGED) return fail(LHI_E_NOT_CONVERGED, "pressure solve hit the iteration cap");
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_solver_get_stats(lhi_liquid* h, lhi_solve_stats* stats) {
+    NEED_HANDLE(h);
+    if (!stats) return fail(LHI_E_INVALID_ARG, "null argument");
+    *stats = h->impl->stats();
+    return LHI_OK;
+}
+
+LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void* out) {
+    NEED_HANDLE(h);
+    if (!x || !out) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->get_ax(level, x, out);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_field_size(const lhi_liquid* h, int32_t field, int32_t level, int64_t* count,
+                                  int32_t* elem_bytes) {
+    NEED_HANDLE(h);
+    if (!count || !elem_bytes) return fail(LHI_E_INVALID_ARG, "null argument");
+    int rc = h->impl->field_size(field, level, count, elem_bytes);
+    if (rc) return fail(rc, "unknown field or level");
+    return LHI_OK;
+}
+
+LHI_API int lhi_liquid_get_field(lhi_liquid* h, int32_t field, int32_t level, void* out) {
+    NEED_HANDLE(h);
+    if (!out) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->get_field(field, level, out);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, const void* in) {
+    NEED_HANDLE(h);
+    if (!in) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->set_field(field, level, in);
+        return LHI_OK;
+    });
+}
+
+}  // extern "C"

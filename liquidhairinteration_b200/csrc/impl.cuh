@@ -1,0 +1,222 @@
+// impl.cuh -- device state and host orchestration of one liquid handle.
+//
+// LiquidImpl<T, TX> owns every device buffer of one scene: the MAC grid of
+// Grid<3> (Grid.h:146-171) in the reference's x-major / z-fastest layout, the
+// particle state as structure-of-arrays kept physically sorted by cell, and
+// the multigrid levels of CGSolver<3> (PressureSolver.h:121-145) with the
+// 7-point matrix stored per face instead of per row.
+//   T  : grid, particle, matrix and V-cycle scalar (float or double)
+//   TX : scalar of the outer CG iterate x (double in the mixed mode)
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "lhi.h"
+
+namespace lhi {
+
+constexpr int kMaxBoundaryNodes = 32;
+constexpr int kMaxLevels = 10;
+
+// Boundary tree in evaluation (post-) order: children precede parents.
+struct BoundaryProgram {
+    int count;
+    int root;
+    int kind[kMaxBoundaryNodes];
+    int use_inside[kMaxBoundaryNodes];
+    int left[kMaxBoundaryNodes];
+    int right[kMaxBoundaryNodes];
+    double center[kMaxBoundaryNodes][3];
+    double half[kMaxBoundaryNodes][3];
+};
+
+// Device-resident PCG scalars (one cache line group, read by the kernels).
+struct SolveScalars {
+    double rz_old;   // r.z of the previous iteration
+    double rz_new;
+    double denom;    // p.Ap over interior fluid cells
+    double res2;     // sum r^2 over interior fluid cells (recursive residual)
+    double apz;      // Ap.z over interior fluid cells (flexible beta)
+    double rr_all;   // sum r^2 over all cells (initial residual)
+    double true2;    // sum (b - A x)^2 over interior fluid cells
+    double div[3];   // divergence diagnostic: sum, count, max |div|
+    double vmax;     // max |v| over particles (CFL)
+    double pad[5];
+};
+
+struct GridGeom {
+    int nx, ny, nz;
+};
+
+template <class T> struct LevelDev {
+    int nx, ny, nz;
+    long long n;
+    T* diag = nullptr;
+    T* cf[3] = {nullptr, nullptr, nullptr};  // coefficient of the +x/+y/+z face of each cell
+    uint8_t* type = nullptr;                 // 0 air (phi>0), 1 phi==0, 2 fluid (phi<0)
+    T* phi = nullptr;                        // GetApproxLiquidPhi at this level
+    T* r = nullptr;
+    T* z = nullptr;
+    T h[3];                                  // level spacing: factor * dx
+};
+
+// Polymorphic front so the C-ABI can hold any precision behind one pointer.
+class LiquidBase {
+public:
+    virtual ~LiquidBase() {}
+    virtual int precision() const = 0;
+    virtual void dx(double out[3]) const = 0;
+    virtual void set_boundary(const BoundaryProgram& prog) = 0;
+    virtual void set_solid_phi(const void* host) = 0;
+    virtual void set_particles(int64_t n, const void* pos, const void* vel, const void* aff) = 0;
+    virtual void get_particles(void* pos, void* vel, void* aff) = 0;
+    virtual int64_t num_particles() const = 0;
+    virtual void clear() = 0;
+    virtual void sort_particles() = 0;
+    virtual void compute_liquid_phi() = 0;
+    virtual void particle_to_grid() = 0;
+    virtual void apply_gravity(double dt) = 0;
+    virtual int projection(double dt) = 0;
+    virtual void velocity_update(double dt) = 0;
+    virtual void extrapolate() = 0;
+    virtual void grid_to_particle() = 0;
+    virtual void advect(double dt) = 0;
+    virtual int pre_step(double dt) = 0;
+    virtual int step(double dt) = 0;
+    virtual void divergence(double* mean, double* max_abs) = 0;
+    virtual double cfl() = 0;
+    virtual void solver_init() = 0;
+    virtual void build_rhs() = 0;
+    virtual void build_lhs(double rho, double dt) = 0;
+    virtual void apply_preconditioner() = 0;
+    virtual int solve(double rho, double dt) = 0;
+    virtual lhi_solve_stats stats() const = 0;
+    virtual void get_ax(int level, const void* x, void* out) = 0;
+    virtual int field_size(int field, int level, int64_t* count, int32_t* eb) = 0;
+    virtual void get_field(int field, int level, void* out) = 0;
+    virtual void set_field(int field, int level, const void* in) = 0;
+    virtual void sync() = 0;
+};
+
+template <class T, class TX> class LiquidImpl : public LiquidBase {
+public:
+    LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& sp, const lhi_liquid_params& lp, int precision);
+    ~LiquidImpl() override;
+
+    int precision() const override { return precision_; }
+    void dx(double out[3]) const override {
+        for (int i = 0; i < 3; ++i) out[i] = double(dx_[i]);
+    }
+    void set_boundary(const BoundaryProgram& prog) override;
+    void set_solid_phi(const void* host) override;
+    void set_particles(int64_t n, const void* pos, const void* vel, const void* aff) override;
+    void get_particles(void* pos, void* vel, void* aff) override;
+    int64_t num_particles() const override { return np_; }
+    void clear() override;
+    void sort_particles() override;
+    void compute_liquid_phi() override;
+    void particle_to_grid() override;
+    void apply_gravity(double dt) override;
+    int projection(double dt) override;
+    void velocity_update(double dt) override;
+    void extrapolate() override;
+    void grid_to_particle() override;
+    void advect(double dt) override;
+    int pre_step(double dt) override;
+    int step(double dt) override;
+    void divergence(double* mean, double* max_abs) override;
+    double cfl() override;
+    void solver_init() override;
+    void build_rhs() override;
+    void build_lhs(double rho, double dt) override;
+    void apply_preconditioner() override;
+    int solve(double rho, double dt) override;
+    lhi_solve_stats stats() const override { return stats_; }
+    void get_ax(int level, const void* x, void* out) override;
+    int field_size(int field, int level, int64_t* count, int32_t* eb) override;
+    void get_field(int field, int level, void* out) override;
+    void set_field(int field, int level, const void* in) override;
+    void sync() override { LHI_CUDA(cudaStreamSynchronize(stream_)); }
+
+    // ---- internals shared by the .cu files
+    void alloc_particles(int64_t cap);
+    void ensure_sorted();
+    void p2g_accumulate();
+    void p2g_normalize(bool with_gravity, T gdt);
+    void g2p(bool advect, T dt);
+    void smooth(int level, int sweeps);
+    void restrict_to(int level);
+    void prolong_to(int level);
+    void vcycle();
+    void spmv(int level, const T* x, T* y);
+    void get_acoef(int level, T* host_out);
+    void device_sum_launch_prep();
+    template <class F> void with_partials(F f);
+    double read_scalar(const double* dptr);
+    void read_scalars();
+
+    int precision_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+
+    // grid (Grid<3>)
+    int nx_, ny_, nz_;
+    T min_[3], max_[3], dx_[3];
+    T radius_, density_, gravity_;
+    int extrap_iters_;
+    long long ncell_, nface_[3], nnode_;
+    T* v_[3] = {};    // current vx, vy, vz
+    T* tv_[3] = {};   // current tempVx, tempVy, tempVz
+    T* w_[3] = {};
+    T* lw_[3] = {};   // liquidWx/y/z
+    T* pressure_ = nullptr;
+    T* liquid_phi_ = nullptr;
+    T* solid_phi_ = nullptr;
+    uint8_t* valid_ = nullptr;  // isValid: 255 invalid, else the sweep it became valid
+    uint8_t* occ_ = nullptr;    // 4^3-cell block occupancy for the liquid SDF
+    int occ_dim_[3];
+
+    // particles (SoA, sorted by cell): 15 scalars + caller id, double-buffered
+    int64_t np_ = 0, pcap_ = 0;
+    T* pdata_[2] = {nullptr, nullptr};  // [15][pcap]: px py pz ux uy uz c0..c8
+    int32_t* pid_[2] = {nullptr, nullptr};
+    int pcur_ = 0;
+    bool sorted_ = false;
+    bool keys_fresh_ = false;  // keys_[0]/vals_[0] hold (cell key, identity) of the current order
+    uint32_t* keys_[2] = {nullptr, nullptr};
+    int32_t* vals_[2] = {nullptr, nullptr};
+    uint32_t* hist_ = nullptr;  // radix histograms
+    long long hist_cap_ = 0;
+    int32_t* cell_count_ = nullptr;  // ncell + 1
+    int32_t* cell_start_ = nullptr;  // ncell + 1
+    void* scan_tmp_ = nullptr;
+    long long scan_tmp_bytes_ = 0;
+
+    // solver (CGSolver<3>)
+    lhi_solver_params sp_;
+    int nlev_;
+    LevelDev<T> lv_[kMaxLevels];
+    T* rhs_ = nullptr;
+    TX* x_ = nullptr;
+    T* p_ = nullptr;
+    T* ap_ = nullptr;
+    SolveScalars* sc_ = nullptr;      // device
+    SolveScalars* sc_host_ = nullptr; // pinned mirror
+    double* partials_ = nullptr;
+    unsigned* counter_ = nullptr;
+    int sum_blocks_ = 0;
+    lhi_solve_stats stats_{};
+
+    T* p_ptr(int k) const { return pdata_[pcur_] + size_t(k) * size_t(pcap_); }
+};
+
+// radix-sort / scan helpers (k_sort.cu)
+void device_exclusive_scan_i32(const int32_t* in, int32_t* out, long long n, void* tmp, long long tmp_bytes,
+                               cudaStream_t s);
+long long scan_tmp_bytes(long long n);
+void radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], int& cur, long long n, int key_bits, uint32_t* hist,
+                      void* tmp, long long tmp_bytes, cudaStream_t s);
+long long radix_hist_entries(long long n);
+
+}  // namespace lhi

@@ -1,0 +1,776 @@
+// k_particles.cu -- particle side of the liquid step.
+//
+//   keys -> radix sort -> permute  : particles stay physically sorted by cell
+//   liquid SDF (ComputeLiquidPhi)  : per-cell gather over the sorted cells
+//   P2G (Particle2Grid)            : 8^3-cell tiles accumulated in shared
+//                                    memory, flushed once per node
+//   G2P + advection                : one thread per particle, exact rounding
+#include "impl.cuh"
+
+namespace lhi {
+
+template <class T> struct GridP {
+    int nx, ny, nz;
+    T mn[3], mx[3], dx[3];
+};
+
+template <class T> __device__ __forceinline__ int cell_trunc(T p, T mn, T dx) {
+    return int(X<T>::div(X<T>::sub(p, mn), dx));  // Point2Index: static_cast<Integer>
+}
+
+template <class T> __device__ __forceinline__ uint32_t cell_key(const GridP<T>& g, T x, T y, T z) {
+    int cx = min(max(cell_trunc(x, g.mn[0], g.dx[0]), 0), g.nx - 1);
+    int cy = min(max(cell_trunc(y, g.mn[1], g.dx[1]), 0), g.ny - 1);
+    int cz = min(max(cell_trunc(z, g.mn[2], g.dx[2]), 0), g.nz - 1);
+    return uint32_t((long long)(cx * g.ny + cy) * g.nz + cz);
+}
+
+// ------------------------------------------------------------------ keys
+template <class T>
+__global__ void k_keys(GridP<T> g, const T* __restrict__ pd, long long cap, long long n, uint32_t* __restrict__ keys,
+                       int32_t* __restrict__ vals) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    keys[i] = cell_key(g, pd[i], pd[cap + i], pd[2 * cap + i]);
+    vals[i] = int32_t(i);
+}
+
+template <class T>
+__global__ void k_permute(const T* __restrict__ src, T* __restrict__ dst, long long cap,
+                          const int32_t* __restrict__ sid, int32_t* __restrict__ did,
+                          const int32_t* __restrict__ order, long long n) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    long long s = order[k];
+#pragma unroll
+    for (int c = 0; c < 15; ++c) dst[c * cap + k] = src[c * cap + s];
+    did[k] = sid[s];
+}
+
+__global__ void k_cell_count(const uint32_t* __restrict__ keys, long long n, int32_t* __restrict__ count) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < n;
+    uint32_t key = valid ? keys[i] : 0xffffffffu;
+    unsigned peers = __match_any_sync(0xffffffffu, key);
+    unsigned lane = threadIdx.x & 31;
+    if (valid && (peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&count[key], int(__popc(peers)));
+}
+
+__global__ void k_occupancy(const int32_t* __restrict__ cs, int nx, int ny, int nz, uint8_t* __restrict__ occ,
+                            int ox, int oy, int oz) {
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long nc = (long long)nx * ny * nz;
+    if (c >= nc) return;
+    if (cs[c + 1] == cs[c]) return;
+    int z = int(c % nz), y = int((c / nz) % ny), x = int(c / ((long long)ny * nz));
+    occ[((long long)(x >> 2) * oy + (y >> 2)) * oz + (z >> 2)] = 1;
+}
+
+// AoS host layout <-> SoA device layout
+template <class T>
+__global__ void k_aos_to_soa(const T* __restrict__ aos, T* __restrict__ pd, long long cap, int32_t* __restrict__ id,
+                             long long n, int has_vel, int has_aff) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T* pos = aos;
+    const T* vel = aos + 3 * n;
+    const T* aff = aos + 6 * n;
+    for (int k = 0; k < 3; ++k) pd[k * cap + i] = pos[3 * i + k];
+    for (int k = 0; k < 3; ++k) pd[(3 + k) * cap + i] = has_vel ? vel[3 * i + k] : T(0);
+    for (int k = 0; k < 9; ++k) pd[(6 + k) * cap + i] = has_aff ? aff[9 * i + k] : T(0);
+    id[i] = int32_t(i);
+}
+
+template <class T>
+__global__ void k_soa_to_aos(const T* __restrict__ pd, long long cap, const int32_t* __restrict__ id,
+                             T* __restrict__ aos, long long n) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    long long i = id[k];
+    T* pos = aos;
+    T* vel = aos + 3 * n;
+    T* aff = aos + 6 * n;
+    for (int c = 0; c < 3; ++c) pos[3 * i + c] = pd[c * cap + k];
+    for (int c = 0; c < 3; ++c) vel[3 * i + c] = pd[(3 + c) * cap + k];
+    for (int c = 0; c < 9; ++c) aff[9 * i + c] = pd[(6 + c) * cap + k];
+}
+
+// ------------------------------------------------------------ liquid SDF
+// LiquidModel<3>::ComputeLiquidPhi (LiquidModel.cpp:540-560) as a gather:
+// cell c takes min(|x_c - x_p| - r) over particles p whose Point2Index cell
+// lies within +-d of c.  The minimum does not depend on visiting order, so
+// the result is bit-identical to the reference.  Window cells that provably
+// cannot lower the current minimum are skipped (bound with safety margin).
+template <class T>
+__global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* __restrict__ cs,
+                                                    const uint8_t* __restrict__ occ, int ox, int oy, int oz,
+                                                    const T* __restrict__ pd, long long cap, T radius, int d0, int d1,
+                                                    int d2, T* __restrict__ phi) {
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long nc = (long long)g.nx * g.ny * g.nz;
+    if (c >= nc) return;
+    int cz = int(c % g.nz), cy = int((c / g.nz) % g.ny), cx = int(c / ((long long)g.ny * g.nz));
+    int x0 = max(0, cx - d0), x1 = min(g.nx - 1, cx + d0);
+    int y0 = max(0, cy - d1), y1 = min(g.ny - 1, cy + d1);
+    int z0 = max(0, cz - d2), z1 = min(g.nz - 1, cz + d2);
+    bool any = false;
+    for (int bx = x0 >> 2; bx <= (x1 >> 2) && !any; ++bx)
+        for (int by = y0 >> 2; by <= (y1 >> 2) && !any; ++by)
+            for (int bz = z0 >> 2; bz <= (z1 >> 2); ++bz)
+                if (occ[((long long)bx * oy + by) * oz + bz]) {
+                    any = true;
+                    break;
+                }
+    if (!any) return;
+    T cur = phi[c];
+    // Index2Point: (index + 0.5) * dx + minCoord
+    const T cpx = X<T>::add(X<T>::mul(X<T>::add(T(cx), T(0.5)), g.dx[0]), g.mn[0]);
+    const T cpy = X<T>::add(X<T>::mul(X<T>::add(T(cy), T(0.5)), g.dx[1]), g.mn[1]);
+    const T cpz = X<T>::add(X<T>::mul(X<T>::add(T(cz), T(0.5)), g.dx[2]), g.mn[2]);
+    const T* px = pd;
+    const T* py = pd + cap;
+    const T* pz = pd + 2 * cap;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int wx = x0; wx <= x1; ++wx)
+            for (int wy = y0; wy <= y1; ++wy) {
+                int ax = abs(wx - cx), ay = abs(wy - cy);
+                long long rowc = ((long long)wx * g.ny + wy) * g.nz;
+                for (int wz = z0; wz <= z1; ++wz) {
+                    int az = abs(wz - cz);
+                    bool inner = ax <= 1 && ay <= 1 && az <= 1;
+                    if (inner != (pass == 0)) continue;
+                    long long w = rowc + wz;
+                    int s = cs[w], e = cs[w + 1];
+                    if (s == e) continue;
+                    if (pass == 1) {
+                        // every particle of cell w is at least lb away from the centre
+                        T lx = T(fmax(double(ax) - 0.5, 0.0)) * g.dx[0];
+                        T ly = T(fmax(double(ay) - 0.5, 0.0)) * g.dx[1];
+                        T lz = T(fmax(double(az) - 0.5, 0.0)) * g.dx[2];
+                        double lb = sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
+                                    double(radius) * (1.0 + 1e-6);
+                        if (double(cur) < lb) continue;
+                    }
+                    for (int p = s; p < e; ++p) {
+                        T qx = px[p], qy = py[p], qz = pz[p];
+                        int tx = cell_trunc(qx, g.mn[0], g.dx[0]);
+                        int ty = cell_trunc(qy, g.mn[1], g.dx[1]);
+                        int tz = cell_trunc(qz, g.mn[2], g.dx[2]);
+                        if (abs(tx - cx) > d0 || abs(ty - cy) > d1 || abs(tz - cz) > d2) continue;
+                        T dist = X<T>::sqrt(sqnorm3(X<T>::sub(cpx, qx), X<T>::sub(cpy, qy), X<T>::sub(cpz, qz)));
+                        T ph = X<T>::sub(dist, radius);
+                        cur = (cur < ph) ? cur : ph;
+                    }
+                }
+            }
+    }
+    phi[c] = cur;
+}
+
+// ------------------------------------------------------------------ P2G
+constexpr int kTile = 8;
+
+template <class T> struct NodeRange {
+    int lo, hi;
+};
+
+// Per-axis node offsets around the particle's cell for face component a on
+// axis i: the quadratic B-spline is non-zero for offsets [-1, 2] along the
+// face normal and [-1, 1] across it; the reference's window +-d clips it.
+__device__ __forceinline__ int off_lo(int d) { return max(-1, -d); }
+__device__ __forceinline__ int off_hi(int i, int a, int d) { return min(i == a ? 2 : 1, d); }
+
+template <class T, int A>
+__device__ __forceinline__ void p2g_particle(const GridP<T>& g, const int d[3], const T q[3], const T g3[3],
+                                             const int ci[3], T vel, const T* Ccol, T* sw, T* sv, int lox, int loy,
+                                             int loz, bool use_smem, T* gw, T* gv) {
+    const int ext_y = kTile + 2 + (A == 1), ext_z = kTile + 2 + (A == 2);
+    const int hx = g.nx - 1 + (A == 0), hy = g.ny - 1 + (A == 1), hz = g.nz - 1 + (A == 2);
+    T ew[3][4], cc[3][4];
+    bool ok[3][4];
+    int lo[3], hi[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        lo[i] = off_lo(d[i]);
+        hi[i] = off_hi(i, A, d[i]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int o = k - 1;
+            int node = ci[i] + o;
+            T c = (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
+            T e = X<T>::sub(g3[i], c);
+            cc[i][k] = c;
+            ok[i][k] = (o >= lo[i] && o <= hi[i] && !(fabs(e) >= T(1.5f)));
+            ew[i][k] = ok[i][k] ? qweight(e) : T(0);
+        }
+    }
+    for (int kx = 0; kx < 4; ++kx) {
+        if (!ok[0][kx]) continue;
+        int xi = ci[0] + kx - 1;
+        if (xi < 0 || xi > hx) continue;
+        for (int ky = 0; ky < 4; ++ky) {
+            if (!ok[1][ky]) continue;
+            int yi = ci[1] + ky - 1;
+            if (yi < 0 || yi > hy) continue;
+            T wxy = X<T>::mul(ew[0][kx], ew[1][ky]);
+            T d0 = X<T>::sub(q[0], X<T>::add(X<T>::mul(cc[0][kx], g.dx[0]), g.mn[0]));
+            T d1 = X<T>::sub(q[1], X<T>::add(X<T>::mul(cc[1][ky], g.dx[1]), g.mn[1]));
+            for (int kz = 0; kz < 4; ++kz) {
+                if (!ok[2][kz]) continue;
+                int zi = ci[2] + kz - 1;
+                if (zi < 0 || zi > hz) continue;
+                T weight = X<T>::mul(wxy, ew[2][kz]);
+                T d2 = X<T>::sub(q[2], X<T>::add(X<T>::mul(cc[2][kz], g.dx[2]), g.mn[2]));
+                T val = X<T>::mul(weight, X<T>::add(vel, dot3(Ccol[0], Ccol[1], Ccol[2], d0, d1, d2)));
+                if (use_smem) {
+                    int idx = ((xi - lox) * ext_y + (yi - loy)) * ext_z + (zi - loz);
+                    atomicAdd(&sw[idx], weight);
+                    atomicAdd(&sv[idx], val);
+                } else {
+                    long long gi = ((long long)xi * (g.ny + (A == 1)) + yi) * (g.nz + (A == 2)) + zi;
+                    atomicAdd(&gw[gi], weight);
+                    atomicAdd(&gv[gi], val);
+                }
+            }
+        }
+    }
+}
+
+template <class T> struct P2GOut {
+    T* v[3];
+    T* w[3];
+};
+
+__host__ __device__ constexpr int p2g_region(int a) {
+    return (kTile + 2 + (a == 0)) * (kTile + 2 + (a == 1)) * (kTile + 2 + (a == 2));
+}
+
+// LiquidModel<3>::Particle2Grid accumulation (LiquidModel.cpp:614-701):
+// one CTA per 8^3-cell tile; its particles are the sorted runs of the tile's
+// 64 (x, y) rows.  Contributions are summed in shared memory, then each
+// touched node is added to global memory once.
+template <class T>
+__global__ void __launch_bounds__(256) k_p2g(GridP<T> g, const int32_t* __restrict__ cs, const T* __restrict__ pd,
+                                             long long cap, int d0, int d1, int d2, P2GOut<T> out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* acc = reinterpret_cast<T*>(smem_raw);
+    __shared__ int row_start[kTile * kTile];
+    __shared__ int row_pre[kTile * kTile + 1];
+    const int x0 = blockIdx.z * kTile, y0 = blockIdx.y * kTile, z0 = blockIdx.x * kTile;
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int r = 0; r < kTile * kTile; ++r) {
+            int x = x0 + r / kTile, y = y0 + r % kTile;
+            int cnt = 0, st = 0;
+            if (x < g.nx && y < g.ny) {
+                long long c0 = ((long long)x * g.ny + y) * g.nz + z0;
+                long long c1 = ((long long)x * g.ny + y) * g.nz + min(z0 + kTile, g.nz);
+                st = cs[c0];
+                cnt = cs[c1] - st;
+            }
+            row_start[r] = st;
+            row_pre[r] = run;
+            run += cnt;
+        }
+        row_pre[kTile * kTile] = run;
+    }
+    __syncthreads();
+    const int total = row_pre[kTile * kTile];
+    if (total == 0) return;
+    const int R0 = p2g_region(0), R1 = p2g_region(1), R2 = p2g_region(2);
+    const int ntot = 2 * (R0 + R1 + R2);
+    for (int i = threadIdx.x; i < ntot; i += blockDim.x) acc[i] = T(0);
+    __syncthreads();
+    T* sw[3] = {acc, acc + 2 * R0, acc + 2 * (R0 + R1)};
+    T* sv[3] = {acc + R0, acc + 2 * R0 + R1, acc + 2 * (R0 + R1) + R2};
+    const int d[3] = {d0, d1, d2};
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+        int lo = 0, hi = kTile * kTile;  // find row: row_pre[r] <= k < row_pre[r+1]
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (row_pre[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        long long p = (long long)row_start[lo] + (k - row_pre[lo]);
+        T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
+        T vel[3] = {pd[3 * cap + p], pd[4 * cap + p], pd[5 * cap + p]};
+        T C[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) C[c] = pd[(6 + c) * cap + p];
+        T g3[3];
+        int ci[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            g3[i] = X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]);  // cwiseQuotient
+            ci[i] = int(g3[i]);                                      // cast<Integer>
+        }
+        bool in_tile = ci[0] >= x0 && ci[0] < x0 + kTile && ci[1] >= y0 && ci[1] < y0 + kTile && ci[2] >= z0 &&
+                       ci[2] < z0 + kTile;
+        p2g_particle<T, 0>(g, d, q, g3, ci, vel[0], &C[0], sw[0], sv[0], x0 - 1, y0 - 1, z0 - 1, in_tile, out.w[0],
+                           out.v[0]);
+        p2g_particle<T, 1>(g, d, q, g3, ci, vel[1], &C[3], sw[1], sv[1], x0 - 1, y0 - 1, z0 - 1, in_tile, out.w[1],
+                           out.v[1]);
+        p2g_particle<T, 2>(g, d, q, g3, ci, vel[2], &C[6], sw[2], sv[2], x0 - 1, y0 - 1, z0 - 1, in_tile, out.w[2],
+                           out.v[2]);
+    }
+    __syncthreads();
+    // flush: one global add per touched node
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int ey = kTile + 2 + (a == 1), ez = kTile + 2 + (a == 2);
+        const int R = (a == 0) ? R0 : (a == 1) ? R1 : R2;
+        const int fy = g.ny + (a == 1), fz = g.nz + (a == 2);
+        const int hx = g.nx - 1 + (a == 0);
+        for (int i = threadIdx.x; i < R; i += blockDim.x) {
+            T wv = sw[a][i], vv = sv[a][i];
+            if (wv == T(0) && vv == T(0)) continue;
+            int lz = i % ez, ly = (i / ez) % ey, lx = i / (ey * ez);
+            int xi = x0 - 1 + lx, yi = y0 - 1 + ly, zi = z0 - 1 + lz;
+            if (xi < 0 || xi > hx || yi < 0 || yi >= fy || zi < 0 || zi >= fz) continue;
+            long long gi = ((long long)xi * fy + yi) * fz + zi;
+            atomicAdd(&out.w[a][gi], wv);
+            atomicAdd(&out.v[a][gi], vv);
+        }
+    }
+}
+
+// v = !IsSmall(w) ? v / w : 0 (LiquidModel.cpp:703-720), optionally fused
+// with ApplyGravity (LiquidModel.cpp:899-910) on the y component.
+template <class T>
+__global__ void k_p2g_normalize(T* __restrict__ v, const T* __restrict__ w, int fx, int fy, int fz, int gravity,
+                                T gdt, int nx, int ny, int nz) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long n = (long long)fx * fy * fz;
+    if (i >= n) return;
+    T wv = w[i];
+    T r = !is_small(wv) ? X<T>::div(v[i], wv) : T(0);
+    if (gravity) {
+        int z = int(i % fz), y = int((i / fz) % fy), x = int(i / ((long long)fy * fz));
+        if (x >= 1 && x < nx - 1 && y >= 1 && y < ny && z >= 1 && z < nz - 1) r = X<T>::add(r, gdt);
+    }
+    v[i] = r;
+}
+
+// ------------------------------------------------------------ G2P + advect
+template <class T> struct SolidView {
+    const T* phi;  // (nx+1)(ny+1)(nz+1)
+};
+
+template <class T> __device__ __forceinline__ bool in_grid(const GridP<T>& g, T x, T y, T z) {
+    return g.mn[0] <= x && g.mn[1] <= y && g.mn[2] <= z && x <= g.mx[0] && y <= g.mx[1] && z <= g.mx[2];
+}
+
+// Grid<3>::GetSolidPhi for a point inside the grid (Grid.cpp:144-154)
+template <class T> __device__ T solid_phi_in(const GridP<T>& g, const T* sp, T x, T y, T z) {
+    T lx = X<T>::div(X<T>::sub(x, g.mn[0]), g.dx[0]);
+    T ly = X<T>::div(X<T>::sub(y, g.mn[1]), g.dx[1]);
+    T lz = X<T>::div(X<T>::sub(z, g.mn[2]), g.dx[2]);
+    int xi, yi, zi;
+    T fx, fy, fz;
+    barycentric(lx, 0, g.nx + 1, xi, fx);
+    barycentric(ly, 0, g.ny + 1, yi, fy);
+    barycentric(lz, 0, g.nz + 1, zi, fz);
+    const long long sy = g.nz + 1, sx = (long long)(g.ny + 1) * (g.nz + 1);
+    const T* b = sp + xi * sx + yi * sy + zi;
+    return trilerp(b[0], b[sx], b[sy], b[sx + sy], b[1], b[sx + 1], b[sy + 1], b[sx + sy + 1], fx, fy, fz);
+}
+
+template <class T> __device__ void clamp_to_valid(const GridP<T>& g, T& x, T& y, T& z) {
+    x = clampS(x, X<T>::add(g.mn[0], g.dx[0]), X<T>::sub(g.mx[0], g.dx[0]));
+    y = clampS(y, X<T>::add(g.mn[1], g.dx[1]), X<T>::sub(g.mx[1], g.dx[1]));
+    z = clampS(z, X<T>::add(g.mn[2], g.dx[2]), X<T>::sub(g.mx[2], g.dx[2]));
+}
+
+template <class T> __device__ void normalized3(T v0, T v1, T v2, T out[3]) {
+    T n2 = sqnorm3(v0, v1, v2);
+    if (n2 > T(0)) {
+        T n = X<T>::sqrt(n2);
+        out[0] = X<T>::div(v0, n);
+        out[1] = X<T>::div(v1, n);
+        out[2] = X<T>::div(v2, n);
+    } else {
+        out[0] = v0;
+        out[1] = v1;
+        out[2] = v2;
+    }
+}
+
+// GetSolidGradient at a point whose +-eps neighbours are inside the grid
+template <class T> __device__ void solid_grad_inner(const GridP<T>& g, const T* sp, T x, T y, T z, T out[3]) {
+    const T eps = T(1e-4);
+    T left = solid_phi_in(g, sp, X<T>::sub(x, eps), y, z);
+    T right = solid_phi_in(g, sp, X<T>::add(x, eps), y, z);
+    T bottom = solid_phi_in(g, sp, x, X<T>::sub(y, eps), z);
+    T top = solid_phi_in(g, sp, x, X<T>::add(y, eps), z);
+    T front = solid_phi_in(g, sp, x, y, X<T>::add(z, eps));
+    T back = solid_phi_in(g, sp, x, y, X<T>::sub(z, eps));
+    T dv = T(__dmul_rn(2.0, double(eps)));
+    normalized3(X<T>::div(X<T>::sub(right, left), dv), X<T>::div(X<T>::sub(top, bottom), dv),
+                X<T>::div(X<T>::sub(front, back), dv), out);
+}
+
+// Grid<3>::GetSolidPhi (Grid.cpp:128-155) for any point
+template <class T> __device__ T solid_phi_at(const GridP<T>& g, const T* sp, T x, T y, T z) {
+    if (in_grid(g, x, y, z)) return solid_phi_in(g, sp, x, y, z);
+    T vx = x, vy = y, vz = z;
+    clamp_to_valid(g, vx, vy, vz);
+    T gr[3];
+    solid_grad_inner(g, sp, vx, vy, vz, gr);
+    T r = solid_phi_in(g, sp, vx, vy, vz);
+    r = X<T>::add(r, X<T>::mul(gr[0], X<T>::sub(x, vx)));
+    r = X<T>::add(r, X<T>::mul(gr[1], X<T>::sub(y, vy)));
+    r = X<T>::add(r, X<T>::mul(gr[2], X<T>::sub(z, vz)));
+    return r;
+}
+
+// Grid<3>::GetSolidGradient (Grid.cpp:175-192) for any point
+template <class T> __device__ void solid_grad_at(const GridP<T>& g, const T* sp, T x, T y, T z, T out[3]) {
+    if (!in_grid(g, x, y, z)) {
+        clamp_to_valid(g, x, y, z);
+        solid_grad_inner(g, sp, x, y, z, out);
+        return;
+    }
+    const T eps = T(1e-4);
+    T left = solid_phi_at(g, sp, X<T>::sub(x, eps), y, z);
+    T right = solid_phi_at(g, sp, X<T>::add(x, eps), y, z);
+    T bottom = solid_phi_at(g, sp, x, X<T>::sub(y, eps), z);
+    T top = solid_phi_at(g, sp, x, X<T>::add(y, eps), z);
+    T front = solid_phi_at(g, sp, x, y, X<T>::add(z, eps));
+    T back = solid_phi_at(g, sp, x, y, X<T>::sub(z, eps));
+    T dv = T(__dmul_rn(2.0, double(eps)));
+    normalized3(X<T>::div(X<T>::sub(right, left), dv), X<T>::div(X<T>::sub(top, bottom), dv),
+                X<T>::div(X<T>::sub(front, back), dv), out);
+}
+
+// Gather of one face component (LiquidModel.cpp:738-761 and its y/z twins).
+template <class T, int A>
+__device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3], const T g3[3], const int ci[3],
+                                              const T* __restrict__ vf, T& velA, T col[3]) {
+    const int hx = g.nx - 1 + (A == 0), hy = g.ny - 1 + (A == 1), hz = g.nz - 1 + (A == 2);
+    const long long fy = g.ny + (A == 1), fz = g.nz + (A == 2);
+    T ew[3][4], eg[3][4];
+    bool ok[3][4];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        int lo = off_lo(d[i]), hi = off_hi(i, A, d[i]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int o = k - 1;
+            int node = ci[i] + o;
+            T c = (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
+            T e = X<T>::sub(g3[i], c);
+            ok[i][k] = (o >= lo && o <= hi && !(fabs(e) >= T(1.5f)));
+            ew[i][k] = ok[i][k] ? qweight(e) : T(0);
+            eg[i][k] = ok[i][k] ? gqweight(e) : T(0);
+        }
+    }
+    for (int kx = 0; kx < 4; ++kx) {
+        if (!ok[0][kx]) continue;
+        int xi = ci[0] + kx - 1;
+        if (xi < 0 || xi > hx) continue;
+        for (int ky = 0; ky < 4; ++ky) {
+            if (!ok[1][ky]) continue;
+            int yi = ci[1] + ky - 1;
+            if (yi < 0 || yi > hy) continue;
+            for (int kz = 0; kz < 4; ++kz) {
+                if (!ok[2][kz]) continue;
+                int zi = ci[2] + kz - 1;
+                if (zi < 0 || zi > hz) continue;
+                T wX = ew[0][kx], wY = ew[1][ky], wZ = ew[2][kz];
+                T gX = eg[0][kx], gY = eg[1][ky], gZ = eg[2][kz];
+                T weight = X<T>::mul(X<T>::mul(wX, wY), wZ);
+                T gw0 = X<T>::mul(X<T>::mul(gX, wY), wZ);
+                T gw1 = X<T>::mul(X<T>::mul(wX, gY), wZ);
+                T gw2 = X<T>::mul(X<T>::mul(wX, wY), gZ);
+                T val = vf[((long long)xi * fy + yi) * fz + zi];
+                velA = X<T>::add(velA, X<T>::mul(val, weight));
+                col[0] = X<T>::add(col[0], X<T>::mul(val, gw0));
+                col[1] = X<T>::add(col[1], X<T>::mul(val, gw1));
+                col[2] = X<T>::add(col[2], X<T>::mul(val, gw2));
+            }
+        }
+    }
+}
+
+// LiquidModel<3>::Grid2Particle (LiquidModel.cpp:724-823) fused with
+// AdvectParticle (LiquidModel.cpp:913-935) and the next step's cell key.
+template <class T>
+__global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, long long cap, long long n, int d0,
+                                             int d1, int d2, const T* __restrict__ vx, const T* __restrict__ vy,
+                                             const T* __restrict__ vz, int do_g2p, int do_advect, T dt,
+                                             const T* __restrict__ sp, uint32_t* __restrict__ keys,
+                                             int32_t* __restrict__ vals) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T q[3] = {pd[i], pd[cap + i], pd[2 * cap + i]};
+    T vel[3];
+    if (do_g2p) {
+        const int d[3] = {d0, d1, d2};
+        T g3[3];
+        int ci[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            g3[k] = X<T>::div(X<T>::sub(q[k], g.mn[k]), g.dx[k]);
+            ci[k] = int(g3[k]);
+        }
+        T C[9];
+        vel[0] = vel[1] = vel[2] = T(0);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) C[k] = T(0);
+        g2p_component<T, 0>(g, d, g3, ci, vx, vel[0], &C[0]);
+        g2p_component<T, 1>(g, d, g3, ci, vy, vel[1], &C[3]);
+        g2p_component<T, 2>(g, d, g3, ci, vz, vel[2], &C[6]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pd[(3 + k) * cap + i] = vel[k];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) pd[(6 + k) * cap + i] = C[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) vel[k] = pd[(3 + k) * cap + i];
+    }
+    if (do_advect) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) q[k] = X<T>::add(q[k], X<T>::mul(vel[k], dt));
+        T sphi = solid_phi_at(g, sp, q[0], q[1], q[2]);
+        if (sphi < T(0)) {
+            T gr[3];
+            solid_grad_at(g, sp, q[0], q[1], q[2], gr);
+            T s = X<T>::add(sphi, eps8<T>());
+#pragma unroll
+            for (int k = 0; k < 3; ++k) q[k] = X<T>::sub(q[k], X<T>::mul(s, gr[k]));
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pd[k * cap + i] = q[k];
+        keys[i] = cell_key(g, q[0], q[1], q[2]);
+        vals[i] = int32_t(i);
+    }
+}
+
+// max |v| over particles for GetCFL (LiquidModel.h:49-55)
+template <class T>
+__global__ void k_vmax(const T* __restrict__ pd, long long cap, long long n, double* __restrict__ partials,
+                       unsigned* __restrict__ counter, double* __restrict__ out) {
+    double m = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; ++k) m = fmax(m, fabs(double(pd[(3 + k) * cap + i])));
+    m = block_max(m);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = m;
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) a = fmax(a, ((volatile double*)partials)[b]);
+    a = block_max(a);
+    if (threadIdx.x == 0) {
+        *out = a;
+        *counter = 0u;
+    }
+}
+
+// ------------------------------------------------------------- host side
+template <class T, class TX> static GridP<T> gridp(const LiquidImpl<T, TX>& s) {
+    GridP<T> g;
+    g.nx = s.nx_;
+    g.ny = s.ny_;
+    g.nz = s.nz_;
+    for (int i = 0; i < 3; ++i) {
+        g.mn[i] = s.min_[i];
+        g.mx[i] = s.max_[i];
+        g.dx[i] = s.dx_[i];
+    }
+    return g;
+}
+
+template <class T> static int window(T r, T dx) { return int(std::ceil(r / dx)); }
+
+template <class T, class TX> void LiquidImpl<T, TX>::alloc_particles(int64_t cap) {
+    if (cap <= pcap_) return;
+    for (int b = 0; b < 2; ++b) {
+        if (pdata_[b]) cudaFree(pdata_[b]);
+        if (pid_[b]) cudaFree(pid_[b]);
+        if (keys_[b]) cudaFree(keys_[b]);
+        if (vals_[b]) cudaFree(vals_[b]);
+        LHI_CUDA(cudaMalloc(&pdata_[b], sizeof(T) * 15 * size_t(cap)));
+        LHI_CUDA(cudaMalloc(&pid_[b], sizeof(int32_t) * size_t(cap)));
+        LHI_CUDA(cudaMalloc(&keys_[b], sizeof(uint32_t) * size_t(cap)));
+        LHI_CUDA(cudaMalloc(&vals_[b], sizeof(int32_t) * size_t(cap)));
+    }
+    long long he = radix_hist_entries(cap);
+    if (he > hist_cap_) {
+        if (hist_) cudaFree(hist_);
+        LHI_CUDA(cudaMalloc(&hist_, sizeof(uint32_t) * size_t(he)));
+        hist_cap_ = he;
+    }
+    long long need = std::max(scan_tmp_bytes(he), scan_tmp_bytes(ncell_ + 1));
+    if (need > scan_tmp_bytes_) {
+        if (scan_tmp_) cudaFree(scan_tmp_);
+        LHI_CUDA(cudaMalloc(&scan_tmp_, size_t(need)));
+        scan_tmp_bytes_ = need;
+    }
+    pcap_ = cap;
+    pcur_ = 0;
+}
+
+template <class T, class TX>
+void LiquidImpl<T, TX>::set_particles(int64_t n, const void* pos, const void* vel, const void* aff) {
+    if (n < 0 || n > (int64_t(1) << 31) - 1) throw std::invalid_argument("particle count out of range");
+    if (n > 0 && !pos) throw std::invalid_argument("pos is NULL");
+    alloc_particles(std::max<int64_t>(n, 1));
+    np_ = n;
+    sorted_ = false;
+    if (n == 0) return;
+    T* stage = pdata_[pcur_ ^ 1];  // AoS staging: pos[3n] vel[3n] aff[9n]
+    LHI_CUDA(cudaMemcpyAsync(stage, pos, sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
+    if (vel) LHI_CUDA(cudaMemcpyAsync(stage + 3 * n, vel, sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
+    if (aff) LHI_CUDA(cudaMemcpyAsync(stage + 6 * n, aff, sizeof(T) * 9 * n, cudaMemcpyHostToDevice, stream_));
+    k_aos_to_soa<T><<<blocks_for(n, 256), 256, 0, stream_>>>(stage, pdata_[pcur_], pcap_, pid_[pcur_], n,
+                                                             vel ? 1 : 0, aff ? 1 : 0);
+    LHI_LAUNCH_CHECK();
+    keys_fresh_ = false;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::get_particles(void* pos, void* vel, void* aff) {
+    if (np_ == 0) return;
+    T* stage = pdata_[pcur_ ^ 1];
+    k_soa_to_aos<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pcap_, pid_[pcur_], stage, np_);
+    LHI_LAUNCH_CHECK();
+    if (pos) LHI_CUDA(cudaMemcpyAsync(pos, stage, sizeof(T) * 3 * np_, cudaMemcpyDeviceToHost, stream_));
+    if (vel) LHI_CUDA(cudaMemcpyAsync(vel, stage + 3 * np_, sizeof(T) * 3 * np_, cudaMemcpyDeviceToHost, stream_));
+    if (aff) LHI_CUDA(cudaMemcpyAsync(aff, stage + 6 * np_, sizeof(T) * 9 * np_, cudaMemcpyDeviceToHost, stream_));
+    LHI_CUDA(cudaStreamSynchronize(stream_));
+}
+
+// Stable sort of the particles by cell key, then the per-cell ranges.  The
+// keys of the current positions are already in keys_[0]/vals_[0] (written by
+// set_particles or by the advection kernel).
+template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
+    if (np_ > 0) {
+        if (!keys_fresh_) {
+            k_keys<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, keys_[0],
+                                                                 vals_[0]);
+            LHI_LAUNCH_CHECK();
+        }
+        int kbits = 1;
+        while ((1LL << kbits) < ncell_) ++kbits;
+        int kc = 0;
+        radix_sort_pairs(keys_, vals_, kc, np_, kbits, hist_, scan_tmp_, scan_tmp_bytes_, stream_);
+        k_permute<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_,
+                                                                pid_[pcur_], pid_[pcur_ ^ 1], vals_[kc], np_);
+        LHI_LAUNCH_CHECK();
+        pcur_ ^= 1;
+        if (kc != 0) {  // keep the sorted keys in keys_[0]
+            std::swap(keys_[0], keys_[1]);
+            std::swap(vals_[0], vals_[1]);
+        }
+    }
+    LHI_CUDA(cudaMemsetAsync(cell_count_, 0, sizeof(int32_t) * size_t(ncell_ + 1), stream_));
+    if (np_ > 0) {
+        k_cell_count<<<blocks_for(np_, 256), 256, 0, stream_>>>(keys_[0], np_, cell_count_);
+        LHI_LAUNCH_CHECK();
+    }
+    device_exclusive_scan_i32(cell_count_, cell_start_, ncell_ + 1, scan_tmp_, scan_tmp_bytes_, stream_);
+    LHI_CUDA(cudaMemsetAsync(occ_, 0, size_t(occ_dim_[0]) * occ_dim_[1] * occ_dim_[2], stream_));
+    k_occupancy<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, nx_, ny_, nz_, occ_, occ_dim_[0],
+                                                              occ_dim_[1], occ_dim_[2]);
+    LHI_LAUNCH_CHECK();
+    sorted_ = true;
+    keys_fresh_ = false;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::ensure_sorted() {
+    if (!sorted_) sort_particles();
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::compute_liquid_phi() {
+    if (np_ == 0) return;
+    ensure_sorted();
+    int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
+    if (d0 > 8 || d1 > 8 || d2 > 8) throw std::invalid_argument("particle radius above 8 cells is not supported");
+    k_liquid_phi<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(gridp(*this), cell_start_, occ_, occ_dim_[0],
+                                                                  occ_dim_[1], occ_dim_[2], pdata_[pcur_], pcap_,
+                                                                  radius_, d0, d1, d2, liquid_phi_);
+    LHI_LAUNCH_CHECK();
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
+    ensure_sorted();
+    int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
+    P2GOut<T> out;
+    for (int a = 0; a < 3; ++a) {
+        out.v[a] = v_[a];
+        out.w[a] = w_[a];
+    }
+    size_t smem = sizeof(T) * 2 * (p2g_region(0) + p2g_region(1) + p2g_region(2));
+    LHI_CUDA(cudaFuncSetAttribute(k_p2g<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    dim3 grid(unsigned((nz_ + kTile - 1) / kTile), unsigned((ny_ + kTile - 1) / kTile),
+              unsigned((nx_ + kTile - 1) / kTile));
+    k_p2g<T><<<grid, 256, smem, stream_>>>(gridp(*this), cell_start_, pdata_[pcur_], pcap_, d0, d1, d2, out);
+    LHI_LAUNCH_CHECK();
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::p2g_normalize(bool with_gravity, T gdt) {
+    for (int a = 0; a < 3; ++a) {
+        int fx = nx_ + (a == 0), fy = ny_ + (a == 1), fz = nz_ + (a == 2);
+        k_p2g_normalize<T><<<blocks_for(nface_[a], 256), 256, 0, stream_>>>(
+            v_[a], w_[a], fx, fy, fz, (with_gravity && a == 1) ? 1 : 0, gdt, nx_, ny_, nz_);
+        LHI_LAUNCH_CHECK();
+    }
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::particle_to_grid() {
+    if (np_ == 0) return;
+    p2g_accumulate();
+    p2g_normalize(false, T(0));
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::g2p(bool do_advect, T dt) {
+    if (np_ == 0) return;
+    int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
+    k_g2p<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
+                                                        v_[1], v_[2], 1, do_advect ? 1 : 0, dt, solid_phi_,
+                                                        keys_[0], vals_[0]);
+    LHI_LAUNCH_CHECK();
+    if (do_advect) {
+        sorted_ = false;
+        keys_fresh_ = true;
+    }
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::grid_to_particle() { g2p(false, T(0)); }
+
+template <class T, class TX> void LiquidImpl<T, TX>::advect(double dt) {
+    if (np_ == 0) return;
+    int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
+    k_g2p<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
+                                                        v_[1], v_[2], 0, 1, T(dt), solid_phi_, keys_[0], vals_[0]);
+    LHI_LAUNCH_CHECK();
+    sorted_ = false;
+    keys_fresh_ = true;
+}
+
+template <class T, class TX> double LiquidImpl<T, TX>::cfl() {
+    double vmax = 0.0;
+    if (np_ > 0) {
+        k_vmax<T><<<std::min<unsigned>(blocks_for(np_, 256), 4 * kSMs), 256, 0, stream_>>>(
+            pdata_[pcur_], pcap_, np_, partials_, counter_, &sc_->vmax);
+        LHI_LAUNCH_CHECK();
+        vmax = read_scalar(&sc_->vmax);
+    }
+    // MathUtils::Clamp(dx.x / maxVel, 0.001, 0.1) in Scalar
+    T mv = T(vmax);
+    T r = dx_[0] / mv;
+    T lo = T(0.001), hi = T(0.1);
+    T t = (lo > r) ? lo : r;
+    return double((hi < t) ? hi : t);
+}
+
+template class LiquidImpl<float, float>;
+template class LiquidImpl<float, double>;
+template class LiquidImpl<double, double>;
+
+}  // namespace lhi

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <vector>
 
@@ -264,6 +265,7 @@ template <class S> struct Model {
             S vX = clampS(x_, S(minc[0] + dx[0]), S(maxc[0] - dx[0]));
             S vY = clampS(y_, S(minc[1] + dx[1]), S(maxc[1] - dx[1]));
             S vZ = clampS(z_, S(minc[2] + dx[2]), S(maxc[2] - dx[2]));
+            if (!in_grid(vX, vY, vZ)) return std::numeric_limits<S>::quiet_NaN();  // NaN input
             S g[3];
             solid_gradient(vX, vY, vZ, g);
             return solid_phi_at(vX, vY, vZ) + g[0] * (x_ - vX) + g[1] * (y_ - vY) + g[2] * (z_ - vZ);
@@ -288,6 +290,10 @@ template <class S> struct Model {
             S vX = clampS(x_, S(minc[0] + dx[0]), S(maxc[0] - dx[0]));
             S vY = clampS(y_, S(minc[1] + dx[1]), S(maxc[1] - dx[1]));
             S vZ = clampS(z_, S(minc[2] + dx[2]), S(maxc[2] - dx[2]));
+            if (!in_grid(vX, vY, vZ)) {  // NaN coordinates: the reference recurses without end here
+                g[0] = g[1] = g[2] = std::numeric_limits<S>::quiet_NaN();
+                return;
+            }
             solid_gradient(vX, vY, vZ, g);
             return;
         }
@@ -564,7 +570,9 @@ template <class S> struct Model {
                     div += lwz(xi, yi, zi + 1) * vz(xi, yi, zi + 1) - lwz(xi, yi, zi) * vz(xi, yi, zi);
                     div /= dx[0];
                     divergence += div;
-                    mx = std::max(mx, std::abs(double(div)));
+                    // max-norm only over cells whose six faces the projection updates
+                    if (xi >= 1 && xi <= nx - 3 && yi >= 1 && yi <= ny - 3 && zi >= 1 && zi <= nz - 3)
+                        mx = std::max(mx, std::abs(double(div)));
                 }
         if (mean) *mean = double(divergence / S(count));
         if (max_abs) *max_abs = mx;
@@ -714,8 +722,11 @@ template <class S> struct Model {
                     S dg = Adiag[level](xi, yi, zi);
                     if (is_small(dg)) continue;
                     S term = (r[level](xi, yi, zi) - get_ax(zl, xi, yi, zi, level)) / dg;
-                    zl(xi, yi, zi) =
-                        S((1. - double(smoothFactor)) * double(zl(xi, yi, zi)) + double(S(smoothFactor * term)));
+                    if (sp.smoother == LHI_SMOOTHER_DAMPED_GS)
+                        zl(xi, yi, zi) = zl(xi, yi, zi) + smoothFactor * term;
+                    else
+                        zl(xi, yi, zi) =
+                            S((1. - double(smoothFactor)) * double(zl(xi, yi, zi)) + double(S(smoothFactor * term)));
                 }
     }
 
@@ -798,14 +809,21 @@ template <class S> struct Model {
         return sum;
     }
 
+    // cells where PCG updates x, r and takes p.Ap / ||r||: the fluid cells
+    // of [1, N-2]^3 as the reference (PressureSolver.cpp:874-899), or every
+    // fluid cell with LHI_REGION_FLUID.
+    int lo() const { return sp.update_region == LHI_REGION_FLUID ? 0 : 1; }
+    int hx() const { return sp.update_region == LHI_REGION_FLUID ? nx : nx - 1; }
+    int hy() const { return sp.update_region == LHI_REGION_FLUID ? ny : ny - 1; }
+    int hz() const { return sp.update_region == LHI_REGION_FLUID ? nz : nz - 1; }
     bool interior_fluid(int xi, int yi, int zi) const { return !(liquidPhi(xi, yi, zi) > S(0.0)); }
 
     // ||b - A x|| over interior fluid cells; optionally stores it into r[0].
     S true_residual(bool store) {
         S acc = S(0.0);
-        for (int xi = 1; xi < nx - 1; ++xi)
-            for (int yi = 1; yi < ny - 1; ++yi)
-                for (int zi = 1; zi < nz - 1; ++zi) {
+        for (int xi = lo(); xi < hx(); ++xi)
+            for (int yi = lo(); yi < hy(); ++yi)
+                for (int zi = lo(); zi < hz(); ++zi) {
                     if (!interior_fluid(xi, yi, zi)) continue;
                     S rr = rhs(xi, yi, zi) - get_ax(x, xi, yi, zi, 0);
                     if (store) r[0](xi, yi, zi) = rr;
@@ -835,9 +853,9 @@ template <class S> struct Model {
         for (int iter = 0; iter < sp.max_iterations; ++iter) {
             if (residual < threshold) break;
             S denom = S(0.0);
-            for (int xi = 1; xi < nx - 1; ++xi)
-                for (int yi = 1; yi < ny - 1; ++yi)
-                    for (int zi = 1; zi < nz - 1; ++zi) {
+            for (int xi = lo(); xi < hx(); ++xi)
+                for (int yi = lo(); yi < hy(); ++yi)
+                    for (int zi = lo(); zi < hz(); ++zi) {
                         if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
                         S ap = get_ax(p, xi, yi, zi, 0);
                         if (sp.cg_variant == LHI_CG_FLEXIBLE) Ap(xi, yi, zi) = ap;
@@ -845,9 +863,9 @@ template <class S> struct Model {
                     }
             alpha = oldRZ / denom;
             residual = S(0.0);
-            for (int xi = 1; xi < nx - 1; ++xi)
-                for (int yi = 1; yi < ny - 1; ++yi)
-                    for (int zi = 1; zi < nz - 1; ++zi) {
+            for (int xi = lo(); xi < hx(); ++xi)
+                for (int yi = lo(); yi < hy(); ++yi)
+                    for (int zi = lo(); zi < hz(); ++zi) {
                         if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
                         x(xi, yi, zi) += alpha * p(xi, yi, zi);
                         r[0](xi, yi, zi) -= alpha * get_ax(p, xi, yi, zi, 0);
@@ -861,9 +879,9 @@ template <class S> struct Model {
             if (sp.cg_variant == LHI_CG_FLEXIBLE) {
                 // beta = r_new . (z_new - z_old) / rz_old = -alpha (Ap . z_new) / rz_old
                 S apz = S(0.0);
-                for (int xi = 1; xi < nx - 1; ++xi)
-                    for (int yi = 1; yi < ny - 1; ++yi)
-                        for (int zi = 1; zi < nz - 1; ++zi) {
+                for (int xi = lo(); xi < hx(); ++xi)
+                    for (int yi = lo(); yi < hy(); ++yi)
+                        for (int zi = lo(); zi < hz(); ++zi) {
                             if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
                             apz += Ap(xi, yi, zi) * z[0](xi, yi, zi);
                         }
