@@ -1,0 +1,383 @@
+"""Benchmark of the liquid step: ms/step of the 256^3 dam break on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: the scene lives on the GPU; W untimed steps, then K timed steps
+(PreStep + Step: sort, liquid SDF, P2G, gravity, pressure solve to
+||r||/||b|| <= 1e-6 on the true residual, velocity update, extrapolation, G2P,
+advection) bracketed by a barrier and synchronisation, timed with CUDA events
+on the library's stream, max over ranks.  Under torchrun every rank runs an
+independent replica of the scene (replicas only: the step has no exchange).
+
+e2e: the same step through the public C-ABI with host buffers: every step
+uploads the particle state (position, velocity, affine) from pinned memory,
+steps, and downloads it again.
+
+The reference arm (--impl reference) times the reference's own CPU code
+(oracle/_ref/libref.so, its sources compiled from the reference tree) on
+this workload with all host threads; see reference_step_sample().
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256³ ms/step, solve ms: learned-precond FPCG vs plain MGPCG, 1 B200, rr≤1e-6"
+UNIT = "ms/step"
+
+# The reference's PCG does not converge on this scene (fluid reaches the
+# domain's outer cell layer), so the reference arm runs its
+# solver for the iteration count our MGPCG needs on this workload.
+REFERENCE_PCG_ITERATIONS = 24
+# The reference arm times the full reference step on the same scene at 32^3
+# (1/512 of the cells and particles) and scales the time by 512.  Every
+# reference loop is linear in cells or particles and the small grid is
+# cache-resident, so the extrapolation favours the reference.
+REFERENCE_SAMPLE_N = 32
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scene", default="dam256")
+    ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(
+        os.environ.get("WORLD_SIZE", "1"))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        import statistics
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "", 1).isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if s[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------ peaks
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic bytes per launch of each timed category, per unit (cells of
+# level 0 C, faces F ~ C, particles P) -- the per-unit figures of DESIGN.md.
+def algorithmic_bytes(cat, C_cells, P, scalar=4):
+    s = scalar
+    table = {
+        # one red or black half-sweep on level 0: z, cx, cy, cz, type over all
+        # cells, r and diag of the updated colour, write half of z
+        "smooth_fine": (4 * s + 1 + s / 2 + s / 2 + s / 2) * C_cells,
+        # Ap = A p and p.Ap: p, diag, cx, cy, cz, type read, Ap written
+        "spmv": (5 * s + 1 + s) * C_cells,
+        # P2G accumulation: position, velocity, affine read once per particle,
+        # w and v written once per face of the three components
+        "p2g": 15 * s * P + 6 * s * C_cells,
+        # G2P + advection: position read, velocity/affine/position written,
+        # cell key and index written, face velocities read once
+        "g2p": (3 + 15) * s * P + 8 * P + 3 * s * C_cells,
+    }
+    return table.get(cat)
+
+
+# --------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    from liquidhairinteration_b200 import scenes
+    from liquidhairinteration_b200.model import kernel_launch_count
+
+    spec = scenes.get(args.scene)
+    solver = spec.solver_params()
+    model = scenes.build(spec, args.precision, solver)
+    ps = model.GetParticleSystem()
+    n_particles = ps.NumParticles()
+    stream = torch.cuda.ExternalStream(model.stream_ptr())
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        model.PreStep(spec.dt)
+        model.Step(spec.dt)
+    model.sync()
+
+    # ---- timed region: K steps on device-resident state
+    clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank)
+    iters, solve_ms = [], []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    model.sync()
+    model.profile(True)
+    launches0 = kernel_launch_count()
+    clocks.start()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        model.PreStep(spec.dt)
+        model.Step(spec.dt)
+        st = model.GetSolver().Stats()
+        iters.append(st["iterations"])
+        solve_ms.append(st["solve_ms"])
+    ev1.record(stream)
+    ev1.synchronize()
+    launches = kernel_launch_count() - launches0
+    clock_info = clocks.stop()
+    model.profile(False)
+    prof = model.profile_read()
+    torch.cuda.synchronize()
+    barrier()
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    solve_avg = max_over_ranks(sum(solve_ms) / len(solve_ms))
+
+    # ---- roofline of the dominant kernel category
+    peak, peak_kind = measured_peaks()
+    cells = spec.n ** 3
+    scalar = 8 if args.precision == "fp64" else 4
+    dominant = max((k for k in prof if algorithmic_bytes(k, cells, n_particles, scalar) is not None),
+                   key=lambda k: prof[k][1])
+    n_launch, tot_ms = prof[dominant]
+    algo = algorithmic_bytes(dominant, cells, n_particles, scalar)
+    avg_ms = tot_ms / max(n_launch, 1)
+    achieved = algo / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        traffic = tj.get(args.scene, {}).get(dominant)
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(avg_ms, 5),
+                "launches_timed": n_launch}
+
+    # ---- e2e through the C-ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        dt_np = np.float64 if args.precision == "fp64" else np.float32
+        pos, vel, aff = ps.GetParticles()
+        hp = [torch.from_numpy(a.copy()).pin_memory() for a in (pos, vel, aff)]
+        host = [t.numpy() for t in hp]
+        for _ in range(1):
+            ps.SetParticles(*host)
+            model.PreStep(spec.dt)
+            model.Step(spec.dt)
+            p2, v2, a2 = ps.GetParticles()
+        lib = model  # noqa
+        from liquidhairinteration_b200._lib import call
+        ptrs = [h.ctypes.data_as(C.c_void_p) for h in host]
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            call("lhi_liquid_set_particles", model._h, n_particles, ptrs[0], ptrs[1], ptrs[2])
+            model.PreStep(spec.dt)
+            model.Step(spec.dt)
+            call("lhi_liquid_get_particles", model._h, ptrs[0], ptrs[1], ptrs[2])
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        nbytes = n_particles * 15 * np.dtype(dt_np).itemsize
+        e2e = {"value": round(e2e_ms, 3), "unit": UNIT, "h2d_bytes_per_step": int(nbytes),
+               "d2h_bytes_per_step": int(nbytes)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(spec)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms_step, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else
+            {"fp32": "f32", "fp64": "f64"}[args.precision], "data": "synthetic",
+            "config": {
+                "workload": f"{spec.name}: {spec.n}^3 unit-cube dam break, block [0,0.35]x[0,0.7]x[0,1), two solid "
+                            f"boxes, {n_particles} particles (8 per cell, seed {spec.seed}), dt 1/960, one replica per GPU",
+                "solver": "MGPCG: 5 levels, 2+2 red-black damped Gauss-Seidel (w=1), 20 coarsest sweeps, flexible "
+                          "CG on every fluid cell, FP32 V-cycle, FP64 x/dots/true residual every 10, "
+                          "||r||/||b|| <= 1e-6 on the true residual",
+                "precision": args.precision,
+                "l2": "inputs larger than L2 (grid fields ~1.2 GB, particles ~1.9 GB)",
+                "parallelism": f"replicas x{world}",
+            },
+            "solve_ms": round(solve_avg, 3), "cg_iterations": round(sum(iters) / len(iters), 2),
+            "particles_per_s": round(n_particles / (ms_step * 1e-3), 1),
+            "scenes_per_s": round(world * 1000.0 / ms_step, 3),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clock_info,
+            "kernel_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in prof.items()},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+# --------------------------------------------------------- reference arm
+def reference_model(po, spec_small, iterations):
+    """The reference's LiquidModel<3> on the scene (Scene<3> built from the
+    reference JSON schema), PCG capped at ``iterations``."""
+    from liquidhairinteration_b200 import abi
+    solver = spec_small.solver_params(robust=False, max_iterations=iterations, tolerance=1e-30,
+                                      num_level=5, num_pre_smooth=2, num_post_smooth=2, num_final_smooth=20)
+    ref = po.Reference(spec_small.config_json(solver))
+    ref.set_boundary(spec_small.boundary)
+    return ref
+
+
+def reference_step_sample(po, spec, n_small):
+    """One reference step on the scene's layout at n_small^3; returns
+    (seconds, particles).  Each timed step restarts from the seeded state so
+    the reference's own (non-converging) PCG cannot accumulate NaN."""
+    from liquidhairinteration_b200 import scenes
+    small = scenes.dam256()
+    small.n = n_small
+    small.boundary = [dict(small.boundary[0]), scenes.walls(n_small)] + [dict(b) for b in small.boundary[2:]]
+    pos, vel = scenes.seed(small, "fp32")
+    ref = reference_model(po, small, REFERENCE_PCG_ITERATIONS)
+    import numpy as np
+    dt = np.float32(small.dt)
+
+    def step():
+        ref.set_particles(pos, vel)
+        t = time.perf_counter()
+        ref.pre_step(dt)
+        ref.step(dt)
+        return time.perf_counter() - t
+
+    return step, pos.shape[0]
+
+
+def cpu_baseline(spec, steps=3):
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    from oracle import pyoracle as po
+    if not po.reference_available():
+        return None
+    step, npart = reference_step_sample(po, spec, REFERENCE_SAMPLE_N)
+    step()  # warm-up
+    secs = [step() for _ in range(steps)]
+    scale = (spec.n / REFERENCE_SAMPLE_N) ** 3
+    ms = sum(secs) / len(secs) * 1e3 * scale
+    return {"value": round(ms, 1), "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
+            "sample": f"reference LiquidModel<3>::PreStep+Step (OpenMP, {os.environ['OMP_NUM_THREADS']} threads) on "
+                      f"the same scene at {REFERENCE_SAMPLE_N}^3 ({npart} particles), PCG capped at "
+                      f"{REFERENCE_PCG_ITERATIONS} iterations, {steps} steps, time x{scale:.0f}"}
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    from oracle import pyoracle as po
+    from liquidhairinteration_b200 import scenes
+    if not po.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so was not built"}))
+        return
+    spec = scenes.get(args.scene)
+    step, npart = reference_step_sample(po, spec, REFERENCE_SAMPLE_N)
+    for _ in range(args.warmup):
+        step()
+    secs = [step() for _ in range(args.steps)]
+    scale = (spec.n / REFERENCE_SAMPLE_N) ** 3
+    ms = sum(secs) / len(secs) * 1e3 * scale
+    cores = int(os.environ["OMP_NUM_THREADS"])
+    sample = (f"reference LiquidModel<3>::PreStep+Step (OpenMP, {cores} threads) on the same scene at "
+              f"{REFERENCE_SAMPLE_N}^3 ({npart} particles), PCG capped at {REFERENCE_PCG_ITERATIONS} iterations, "
+              f"time x{scale:.0f}")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(ms, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{spec.name} (reference CPU path, bounded sample)", "parallelism": "OpenMP"},
+        "cpu_baseline": {"value": round(ms, 1), "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": round(ms, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -258,6 +258,34 @@ LHI_API int lhi_liquid_field_size(const lhi_liquid* h, int32_t field, int32_t le
 LHI_API int lhi_liquid_get_field(lhi_liquid* h, int32_t field, int32_t level, void* out);
 LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, const void* in);
 
+/* ------------------------------------------------------- measurement */
+/* The handle's CUDA stream (cudaStream_t), e.g. to record events around
+   calls; all of the handle's device work is ordered on it. */
+LHI_API int lhi_liquid_stream(lhi_liquid* h, void** stream);
+/* Number of kernels this library has launched in the process so far. */
+LHI_API int lhi_kernel_launch_count(int64_t* count);
+/* Kernel categories timed by the optional profiler. */
+#define LHI_KERNEL_SORT 0         /* cell keys, radix sort, permutation, cell ranges */
+#define LHI_KERNEL_LIQUID_PHI 1   /* liquid SDF gather                               */
+#define LHI_KERNEL_P2G 2          /* P2G accumulation + normalisation                */
+#define LHI_KERNEL_G2P 3          /* G2P + advection                                 */
+#define LHI_KERNEL_EXTRAPOLATE 4  /* velocity extrapolation sweeps                    */
+#define LHI_KERNEL_GRID 5         /* clear, gravity, velocity update, RHS, divergence */
+#define LHI_KERNEL_LHS 6          /* per-level matrix assembly                        */
+#define LHI_KERNEL_SMOOTH_FINE 7  /* red-black smoothing on the finest level          */
+#define LHI_KERNEL_SMOOTH_COARSE 8 /* smoothing on the coarser levels                 */
+#define LHI_KERNEL_RESTRICT 9
+#define LHI_KERNEL_PROLONG 10
+#define LHI_KERNEL_SPMV 11        /* Ap and p.Ap                                      */
+#define LHI_KERNEL_CG_VECTOR 12   /* x/r/p updates, dots, true residual, scalars      */
+#define LHI_KERNEL_COUNT 13
+/* enable = 1 starts (and resets) per-category timing with CUDA events on
+   the handle's stream; enable = 0 stops it. */
+LHI_API int lhi_liquid_profile(lhi_liquid* h, int32_t enable);
+/* Launches and total device milliseconds of one category since the last
+   reset (synchronises the handle's stream). */
+LHI_API int lhi_liquid_profile_read(lhi_liquid* h, int32_t category, int64_t* launches, double* total_ms);
+
 /* ------------------------------------------------- seeded scene builder */
 /* RectBoundary / OperatorBoundary::Compute (Boundary.h:38-90) on the host,
    in the given precision (0 float, 2 double), at n points (xyz triples). */

@@ -53,6 +53,10 @@ SIGNATURES = {
     "lhi_liquid_field_size": [_h, C.c_int32, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)],
     "lhi_liquid_get_field": [_h, C.c_int32, C.c_int32, _vp],
     "lhi_liquid_set_field": [_h, C.c_int32, C.c_int32, _vp],
+    "lhi_liquid_stream": [_h, C.POINTER(C.c_void_p)],
+    "lhi_kernel_launch_count": [C.POINTER(C.c_int64)],
+    "lhi_liquid_profile": [_h, C.c_int32],
+    "lhi_liquid_profile_read": [_h, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
     "lhi_boundary_eval": [C.POINTER(abi.BoundaryNode), C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int64, _vp],
     "lhi_scene_seed_particles": [C.POINTER(abi.GridDesc), C.POINTER(abi.BoundaryNode), C.c_int32, C.c_int32,
                                  C.POINTER(abi.FluidPrim), C.c_int32, C.c_uint64, C.c_int32,

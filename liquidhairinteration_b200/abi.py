@@ -81,6 +81,9 @@ FIELD_CELL_KEY = 23
 FIELD_PARTICLE_ID = 24
 FIELD_CELL_START = 25
 
+KERNEL_CATEGORIES = ["sort", "liquid_phi", "p2g", "g2p", "extrapolate", "grid", "lhs", "smooth_fine",
+                     "smooth_coarse", "restrict", "prolong", "spmv", "cg_vector"]
+
 FIELD_NAMES = {
     "vx": FIELD_VX, "vy": FIELD_VY, "vz": FIELD_VZ,
     "wx": FIELD_WX, "wy": FIELD_WY, "wz": FIELD_WZ,

@@ -13,6 +13,10 @@ struct lhi_liquid {
     std::unique_ptr<lhi::LiquidBase> impl;
 };
 
+namespace lhi {
+std::atomic<long long> g_kernel_launches{0};
+}
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -303,6 +307,42 @@ LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, co
     if (!in) return fail(LHI_E_INVALID_ARG, "null argument");
     return guarded([&]() -> int {
         h->impl->set_field(field, level, in);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_stream(lhi_liquid* h, void** stream) {
+    NEED_HANDLE(h);
+    if (!stream) return fail(LHI_E_INVALID_ARG, "null argument");
+    *stream = reinterpret_cast<void*>(h->impl->stream());
+    return LHI_OK;
+}
+
+LHI_API int lhi_kernel_launch_count(int64_t* count) {
+    if (!count) return fail(LHI_E_INVALID_ARG, "null argument");
+    *count = lhi::g_kernel_launches.load();
+    return LHI_OK;
+}
+
+LHI_API int lhi_liquid_profile(lhi_liquid* h, int32_t enable) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        lhi::Profiler& p = h->impl->profiler();
+        if (enable) p.reset();
+        else p.drain();
+        p.on = enable != 0;
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_profile_read(lhi_liquid* h, int32_t category, int64_t* launches, double* total_ms) {
+    NEED_HANDLE(h);
+    if (category < 0 || category >= LHI_KERNEL_COUNT) return fail(LHI_E_INVALID_ARG, "unknown kernel category");
+    return guarded([&]() -> int {
+        lhi::Profiler& p = h->impl->profiler();
+        p.drain();
+        if (launches) *launches = p.launches[category];
+        if (total_ms) *total_ms = p.ms[category];
         return LHI_OK;
     });
 }

@@ -10,12 +10,15 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
 
 namespace lhi {
+
+extern std::atomic<long long> g_kernel_launches;
 
 struct CudaError : std::runtime_error {
     cudaError_t code;
@@ -30,7 +33,13 @@ struct CudaError : std::runtime_error {
                                            __FILE__ + ":" + std::to_string(__LINE__));                     \
     } while (0)
 
-#define LHI_LAUNCH_CHECK() LHI_CUDA(cudaGetLastError())
+// Every kernel launch of the library is followed by this check, which also
+// counts it (lhi_kernel_launch_count).
+#define LHI_LAUNCH_CHECK()                                                          \
+    do {                                                                            \
+        ::lhi::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);           \
+        LHI_CUDA(cudaGetLastError());                                               \
+    } while (0)
 
 constexpr int kSMs = 148;
 

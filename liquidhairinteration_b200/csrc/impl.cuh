@@ -61,6 +61,86 @@ template <class T> struct LevelDev {
     T h[3];                                  // level spacing: factor * dx
 };
 
+// Optional per-category device timing: CUDA events on the handle's stream
+// around every launch of a category while profiling is on.
+struct Profiler {
+    struct Rec {
+        int cat;
+        cudaEvent_t a, b;
+    };
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<Rec> recs;
+    long long launches[LHI_KERNEL_COUNT] = {};
+    double ms[LHI_KERNEL_COUNT] = {};
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        LHI_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    // folds finished records into the totals (synchronises on the last one)
+    void drain() {
+        if (recs.empty()) return;
+        LHI_CUDA(cudaEventSynchronize(recs.back().b));
+        for (const Rec& r : recs) {
+            float t = 0.f;
+            LHI_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+            ms[r.cat] += t;
+            launches[r.cat] += 1;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        recs.clear();
+    }
+    void reset() {
+        drain();
+        for (int i = 0; i < LHI_KERNEL_COUNT; ++i) {
+            launches[i] = 0;
+            ms[i] = 0.0;
+        }
+    }
+    ~Profiler() {
+        for (const Rec& r : recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+};
+
+class ProfScope {
+public:
+    ProfScope(Profiler& p, cudaStream_t s, int cat) : p_(p), s_(s), cat_(cat) {
+        if (p_.on) {
+            a_ = p_.get();
+            LHI_CUDA(cudaEventRecord(a_, s_));
+        }
+    }
+    ~ProfScope() {
+        if (!a_) return;
+        cudaEvent_t b = nullptr;
+        if (cudaEventCreate(&b) != cudaSuccess) return;
+        if (!p_.pool.empty()) {
+            cudaEventDestroy(b);
+            b = p_.pool.back();
+            p_.pool.pop_back();
+        }
+        cudaEventRecord(b, s_);
+        p_.recs.push_back({cat_, a_, b});
+    }
+
+private:
+    Profiler& p_;
+    cudaStream_t s_;
+    int cat_;
+    cudaEvent_t a_ = nullptr;
+};
+
 // Polymorphic front so the C-ABI can hold any precision behind one pointer.
 class LiquidBase {
 public:
@@ -97,6 +177,8 @@ public:
     virtual void get_field(int field, int level, void* out) = 0;
     virtual void set_field(int field, int level, const void* in) = 0;
     virtual void sync() = 0;
+    virtual cudaStream_t stream() const = 0;
+    virtual Profiler& profiler() = 0;
 };
 
 template <class T, class TX> class LiquidImpl : public LiquidBase {
@@ -138,6 +220,9 @@ public:
     void get_field(int field, int level, void* out) override;
     void set_field(int field, int level, const void* in) override;
     void sync() override { LHI_CUDA(cudaStreamSynchronize(stream_)); }
+    cudaStream_t stream() const override { return stream_; }
+    Profiler& profiler() override { return prof_; }
+    ProfScope scope(int cat) { return ProfScope(prof_, stream_, cat); }
 
     // ---- internals shared by the .cu files
     void alloc_particles(int64_t cap);
@@ -157,6 +242,7 @@ public:
     void read_scalars();
 
     int precision_;
+    Profiler prof_;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 

@@ -444,6 +444,7 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
 // ------------------------------------------------------------------ stages
 // Grid<3>::Clear (Grid.cpp:157-169); isValid is left as it is.
 template <class T, class TX> void LiquidImpl<T, TX>::clear() {
+    auto ps_ = scope(LHI_KERNEL_GRID);
     LHI_CUDA(cudaMemsetAsync(pressure_, 0, sizeof(T) * ncell_, stream_));
     k_fill<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(liquid_phi_, ncell_, T(3 * dx_[0]));
     LHI_LAUNCH_CHECK();
@@ -474,6 +475,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::set_solid_phi(const void* h
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::apply_gravity(double dt) {
+    auto ps_ = scope(LHI_KERNEL_GRID);
     T gdt = gravity_ * T(dt);
     k_gravity<T><<<blocks_for(nface_[1], 256), 256, 0, stream_>>>(v_[1], nx_, ny_, nz_, gdt);
     LHI_LAUNCH_CHECK();
@@ -482,6 +484,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::apply_gravity(double dt) {
 template <class T, class TX> void LiquidImpl<T, TX>::velocity_update(double dt) {
     long long n = (long long)std::max(nx_ - 2, 0) * std::max(ny_ - 2, 0) * std::max(nz_ - 2, 0);
     if (n == 0) return;
+    auto ps_ = scope(LHI_KERNEL_GRID);
     k_velocity_update<T><<<blocks_for(n, 256), 256, 0, stream_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], T(dt),
                                                                    density_, liquid_phi_, pressure_, lw_[0], lw_[1],
                                                                    lw_[2], v_[0], v_[1], v_[2]);
@@ -498,6 +501,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::projection(double dt) {
 
 template <class T, class TX> void LiquidImpl<T, TX>::extrapolate() {
     if (np_ == 0) return;
+    auto ps_ = scope(LHI_KERNEL_EXTRAPOLATE);
     for (int a = 0; a < 3; ++a) {
         ExtRange r;
         r.x0 = 1;

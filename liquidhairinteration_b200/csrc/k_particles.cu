@@ -649,6 +649,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::get_particles(void* pos, vo
 // keys of the current positions are already in keys_[0]/vals_[0] (written by
 // set_particles or by the advection kernel).
 template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
+    auto ps_ = scope(LHI_KERNEL_SORT);
     if (np_ > 0) {
         if (!keys_fresh_) {
             k_keys<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, keys_[0],
@@ -691,6 +692,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::compute_liquid_phi() {
     ensure_sorted();
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
     if (d0 > 8 || d1 > 8 || d2 > 8) throw std::invalid_argument("particle radius above 8 cells is not supported");
+    auto ps_ = scope(LHI_KERNEL_LIQUID_PHI);
     k_liquid_phi<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(gridp(*this), cell_start_, occ_, occ_dim_[0],
                                                                   occ_dim_[1], occ_dim_[2], pdata_[pcur_], pcap_,
                                                                   radius_, d0, d1, d2, liquid_phi_);
@@ -699,6 +701,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::compute_liquid_phi() {
 
 template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
     ensure_sorted();
+    auto ps_ = scope(LHI_KERNEL_P2G);
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
     P2GOut<T> out;
     for (int a = 0; a < 3; ++a) {
@@ -714,6 +717,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::p2g_normalize(bool with_gravity, T gdt) {
+    auto ps_ = scope(LHI_KERNEL_P2G);
     for (int a = 0; a < 3; ++a) {
         int fx = nx_ + (a == 0), fy = ny_ + (a == 1), fz = nz_ + (a == 2);
         k_p2g_normalize<T><<<blocks_for(nface_[a], 256), 256, 0, stream_>>>(
@@ -731,6 +735,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::particle_to_grid() {
 template <class T, class TX> void LiquidImpl<T, TX>::g2p(bool do_advect, T dt) {
     if (np_ == 0) return;
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
+    auto ps_ = scope(LHI_KERNEL_G2P);
     k_g2p<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
                                                         v_[1], v_[2], 1, do_advect ? 1 : 0, dt, solid_phi_,
                                                         keys_[0], vals_[0]);
@@ -746,6 +751,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::grid_to_particle() { g2p(fa
 template <class T, class TX> void LiquidImpl<T, TX>::advect(double dt) {
     if (np_ == 0) return;
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
+    auto ps_ = scope(LHI_KERNEL_G2P);
     k_g2p<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
                                                         v_[1], v_[2], 0, 1, T(dt), solid_phi_, keys_[0], vals_[0]);
     LHI_LAUNCH_CHECK();

@@ -473,12 +473,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::solver_init() {
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_rhs() {
+    auto ps_ = scope(LHI_KERNEL_GRID);
     k_build_rhs<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], liquid_phi_,
                                                                  lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_);
     LHI_LAUNCH_CHECK();
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, double dt) {
+    auto ps_ = scope(LHI_KERNEL_LHS);
     for (int l = 0; l < nlev_; ++l) {
         LevelDev<T>& L = lv_[l];
         if (L.n == 0) continue;
@@ -497,13 +499,16 @@ template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweep
     LevelDev<T>& L = lv_[level];
     if (L.n == 0 || sweeps <= 0) return;
     T w = T(sp_.smoothing_factor);
+    const int cat = (level == 0) ? LHI_KERNEL_SMOOTH_FINE : LHI_KERNEL_SMOOTH_COARSE;
     if (L.n <= kBlockSmoothMax) {
+        auto ps_ = scope(cat);
         k_smooth_block<T><<<1, 1024, 0, stream_>>>(lk(L), L.r, L.z, w, sp_.smoother, sweeps);
         LHI_LAUNCH_CHECK();
         return;
     }
     for (int s = 0; s < sweeps; ++s)
         for (int phase = 0; phase < 2; ++phase) {
+            auto ps_ = scope(cat);
             k_smooth<T><<<blocks_for(L.n, 256), 256, 0, stream_>>>(lk(L), L.r, L.z, w, sp_.smoother, phase);
             LHI_LAUNCH_CHECK();
         }
@@ -513,6 +518,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::restrict_to(int level) {
     LevelDev<T>& C = lv_[level];
     LevelDev<T>& F = lv_[level - 1];
     if (C.n == 0) return;
+    auto ps_ = scope(LHI_KERNEL_RESTRICT);
     k_restrict<T><<<blocks_for(C.n, 256), 256, 0, stream_>>>(lk(F), F.r, F.z, C.nx, C.ny, C.nz, C.r, C.z);
     LHI_LAUNCH_CHECK();
 }
@@ -521,6 +527,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::prolong_to(int level) {
     LevelDev<T>& C = lv_[level + 1];
     LevelDev<T>& F = lv_[level];
     if (C.n == 0) return;
+    auto ps_ = scope(LHI_KERNEL_PROLONG);
     k_prolong<T><<<blocks_for(C.n, 256), 256, 0, stream_>>>(C.nx, C.ny, C.nz, C.z, F.ny, F.nz, F.z);
     LHI_LAUNCH_CHECK();
 }
@@ -569,13 +576,19 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     LevelDev<T>& L0 = lv_[0];
     const LevelK<T> K0 = lk(L0);
     const unsigned nb = std::min<unsigned>(blocks_for(ncell_, 256), unsigned(sum_blocks_));
-    k_init_r<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, rhs_, L0.r);
-    LHI_LAUNCH_CHECK();
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_init_r<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, rhs_, L0.r);
+        LHI_LAUNCH_CHECK();
+    }
     apply_preconditioner();
-    k_init_p<T><<<nb, 256, 0, stream_>>>(ncell_, L0.type, L0.r, L0.z, p_, partials_, counter_, sc_);
-    LHI_LAUNCH_CHECK();
-    k_scalars_after_init<<<1, 1, 0, stream_>>>(sc_);
-    LHI_LAUNCH_CHECK();
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_init_p<T><<<nb, 256, 0, stream_>>>(ncell_, L0.type, L0.r, L0.z, p_, partials_, counter_, sc_);
+        LHI_LAUNCH_CHECK();
+        k_scalars_after_init<<<1, 1, 0, stream_>>>(sc_);
+        LHI_LAUNCH_CHECK();
+    }
     read_scalars();
     const double residual0 = std::sqrt(sc_host_->rr_all);
     double residual = residual0;
@@ -590,10 +603,14 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     for (int it = 0; it < sp_.max_iterations; ++it) {
         if (residual < threshold) {
             if (every > 0 && iters > 0) {  // final check on the true residual
-                k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 1, partials_, counter_,
-                                                                &sc_->pad[1]);
-                LHI_LAUNCH_CHECK();
-                k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
+                {
+                    auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+                    k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 1, partials_,
+                                                                    counter_, &sc_->pad[1]);
+                    LHI_LAUNCH_CHECK();
+                    k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
+                    LHI_LAUNCH_CHECK();
+                }
                 read_scalars();
                 residual = std::sqrt(sc_host_->res2);
                 if (residual < threshold) {
@@ -605,33 +622,52 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
                 break;
             }
         }
-        k_spmv_dot<T, TX><<<nb, 256, 0, stream_>>>(K0, region, p_, ap_, partials_, counter_, sc_);
-        LHI_LAUNCH_CHECK();
-        k_scalars_alpha<<<1, 1, 0, stream_>>>(sc_);
-        k_update_xr<T, TX><<<nb, 256, 0, stream_>>>(K0, region, p_, ap_, x_, L0.r, partials_, counter_, sc_);
-        LHI_LAUNCH_CHECK();
-        k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
-        ++iters;
-        if (every > 0 && iters % every == 0) {
-            k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 1, partials_, counter_, &sc_->pad[1]);
+        {
+            auto ps_ = scope(LHI_KERNEL_SPMV);
+            k_spmv_dot<T, TX><<<nb, 256, 0, stream_>>>(K0, region, p_, ap_, partials_, counter_, sc_);
+            LHI_LAUNCH_CHECK();
+        }
+        {
+            auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+            k_scalars_alpha<<<1, 1, 0, stream_>>>(sc_);
+            LHI_LAUNCH_CHECK();
+            k_update_xr<T, TX><<<nb, 256, 0, stream_>>>(K0, region, p_, ap_, x_, L0.r, partials_, counter_, sc_);
             LHI_LAUNCH_CHECK();
             k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
+            LHI_LAUNCH_CHECK();
+        }
+        ++iters;
+        if (every > 0 && iters % every == 0) {
+            auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+            k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 1, partials_, counter_,
+                                                            &sc_->pad[1]);
+            LHI_LAUNCH_CHECK();
+            k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
+            LHI_LAUNCH_CHECK();
         }
         apply_preconditioner();
-        k_dot_rz<T><<<nb, 256, 0, stream_>>>(K0, region, L0.r, L0.z, ap_, partials_, counter_, &sc_->pad[1]);
-        LHI_LAUNCH_CHECK();
-        k_scalars_beta<<<1, 1, 0, stream_>>>(sc_, flexible ? 1 : 0);
-        k_update_p<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, L0.z, p_, sc_);
-        LHI_LAUNCH_CHECK();
+        {
+            auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+            k_dot_rz<T><<<nb, 256, 0, stream_>>>(K0, region, L0.r, L0.z, ap_, partials_, counter_, &sc_->pad[1]);
+            LHI_LAUNCH_CHECK();
+            k_scalars_beta<<<1, 1, 0, stream_>>>(sc_, flexible ? 1 : 0);
+            LHI_LAUNCH_CHECK();
+            k_update_p<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, L0.z, p_, sc_);
+            LHI_LAUNCH_CHECK();
+        }
         read_scalars();
         residual = std::sqrt(sc_host_->res2);
         if (!std::isfinite(residual)) break;
     }
     if (!converged && residual < threshold) converged = true;
-    k_x_to_pressure<T, TX><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, x_, pressure_);
-    LHI_LAUNCH_CHECK();
-    k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 0, partials_, counter_, &sc_->true2);
-    LHI_LAUNCH_CHECK();
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_x_to_pressure<T, TX><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, x_, pressure_);
+        LHI_LAUNCH_CHECK();
+        k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 0, partials_, counter_,
+                                                        &sc_->true2);
+        LHI_LAUNCH_CHECK();
+    }
     LHI_CUDA(cudaEventRecord(ev1_, stream_));
     read_scalars();
     float ms = 0.f;

@@ -413,6 +413,24 @@ class LiquidModel:
     def sync(self):
         call("lhi_liquid_sync", self._h)
 
+    def stream_ptr(self):
+        """cudaStream_t of the handle (all its device work runs on it)."""
+        s = C.c_void_p()
+        call("lhi_liquid_stream", self._h, C.byref(s))
+        return s.value or 0
+
+    def profile(self, enable=True):
+        call("lhi_liquid_profile", self._h, 1 if enable else 0)
+
+    def profile_read(self):
+        """{category: (timed launches, total device ms)} since profile(True)."""
+        out = {}
+        for i, name in enumerate(abi.KERNEL_CATEGORIES):
+            n, ms = C.c_int64(), C.c_double()
+            call("lhi_liquid_profile_read", self._h, i, C.byref(n), C.byref(ms))
+            out[name] = (n.value, ms.value)
+        return out
+
     def set_solid_phi(self, node_phi):
         a = np.ascontiguousarray(node_phi, dtype=self.dtype)
         call("lhi_liquid_set_solid_phi", self._h, _ptr(a))
@@ -483,6 +501,12 @@ class Scene:
 
     def GetGridDimension(self):
         return self.params.gridDimension
+
+
+def kernel_launch_count():
+    n = C.c_int64()
+    call("lhi_kernel_launch_count", C.byref(n))
+    return n.value
 
 
 # --------------------------------------------------------- scene builders

@@ -362,7 +362,10 @@ def test_divergence_after_projection(oracle_mod, lhi):
     g.PreStep(spec.dt)
     g.Particle2Grid()
     g.ApplyGravity(spec.dt)
-    before = g.ComputeDivergenceMax()
     g.Projection(spec.dt)
+    # rhs = -div(u*) per fluid cell; after the update the divergence of the
+    # cells whose faces the update touches is the solver's residual
+    b = np.abs(g.field("rhs")).max()
     after = g.ComputeDivergenceMax()
-    assert after < 1e-2 * before, (before, after)
+    assert b > 0
+    assert after < 1e-4 * b, (b, after)
