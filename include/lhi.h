@@ -286,6 +286,31 @@ LHI_API int lhi_liquid_profile(lhi_liquid* h, int32_t enable);
    reset (synchronises the handle's stream). */
 LHI_API int lhi_liquid_profile_read(lhi_liquid* h, int32_t category, int64_t* launches, double* total_ms);
 
+/* ------------------------------------------- no-allocation divergence */
+/* No counterpart in the reference: an added entry point for callers that
+   cannot allocate device memory -- a host that owns all device memory in its
+   own pool, a frame loop that must not stall on cudaMalloc/cudaFree (which
+   may synchronise the device), or code recording into a stream capture.
+   Computes what lhi_liquid_compute_divergence computes (mean over fluid
+   cells, max-norm over fluid cells of [1, N-3]^3), but from DEVICE pointers
+   the caller already holds, with no handle and no allocation of any kind.
+   Fields are float for LHI_PRECISION_FP32 / MIXED and double for FP64, in
+   the layouts listed at the top of this file; dx is the grid spacing of the
+   x axis; stream is a cudaStream_t (NULL = the legacy default stream).
+   Scratch is a fixed device array inside the library (about 192 KB, held by
+   every GPU that loads the library until the process exits), so grids above
+   LHI_NOALLOC_MAX_CELLS cells are rejected with LHI_E_INVALID_ARG.  The first
+   call on each device looks up that array's device address; make that first
+   call before any stream capture.  Every call shares the one array: calls
+   that overlap on the GPU (other streams, other host threads) race and must
+   be serialised by the caller.  The call synchronises the stream to return
+   the two values. */
+#define LHI_NOALLOC_MAX_CELLS 16777216 /* 256^3 */
+LHI_API int lhi_divergence_noalloc(const int32_t dim[3], double dx, int32_t precision, const void* liquid_phi,
+                                   const void* liquid_wx, const void* liquid_wy, const void* liquid_wz,
+                                   const void* vx, const void* vy, const void* vz, void* stream, double* mean,
+                                   double* max_abs);
+
 /* ------------------------------------------------- seeded scene builder */
 /* RectBoundary / OperatorBoundary::Compute (Boundary.h:38-90) on the host,
    in the given precision (0 float, 2 double), at n points (xyz triples). */

@@ -43,6 +43,8 @@ SIGNATURES = {
     "lhi_liquid_advect_particles": [_h, C.c_double],
     "lhi_liquid_compute_divergence": [_h, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "lhi_liquid_get_cfl": [_h, C.POINTER(C.c_double)],
+    "lhi_divergence_noalloc": [C.POINTER(C.c_int32), C.c_double, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                               C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "lhi_solver_init": [_h],
     "lhi_solver_build_rhs": [_h],
     "lhi_solver_build_lhs": [_h, C.c_double, C.c_double],

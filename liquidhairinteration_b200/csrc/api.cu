@@ -15,6 +15,9 @@ struct lhi_liquid {
 
 namespace lhi {
 std::atomic<long long> g_kernel_launches{0};
+int divergence_noalloc(const int32_t dim[3], double dx, int32_t precision, const void* liquid_phi,
+                       const void* liquid_wx, const void* liquid_wy, const void* liquid_wz, const void* vx,
+                       const void* vy, const void* vz, void* stream, double* mean, double* max_abs);
 }
 
 namespace {
@@ -245,6 +248,16 @@ LHI_API int lhi_liquid_compute_divergence(lhi_liquid* h, double* mean, double* m
     return guarded([&]() -> int {
         h->impl->divergence(mean, max_abs);
         return LHI_OK;
+    });
+}
+
+LHI_API int lhi_divergence_noalloc(const int32_t dim[3], double dx, int32_t precision, const void* liquid_phi,
+                                   const void* liquid_wx, const void* liquid_wy, const void* liquid_wz,
+                                   const void* vx, const void* vy, const void* vz, void* stream, double* mean,
+                                   double* max_abs) {
+    return guarded([&]() -> int {
+        return lhi::divergence_noalloc(dim, dx, precision, liquid_phi, liquid_wx, liquid_wy, liquid_wz, vx, vy,
+                                       vz, stream, mean, max_abs);
     });
 }
 
