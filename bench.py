@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eager", action="store_true", help="host-driven PCG loop instead of the solve graph")
     return ap.parse_args()
 
 
@@ -121,16 +122,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-# Algorithmic bytes per launch of each timed category, per unit (cells of
-# level 0 C, faces F ~ C, particles P) -- the per-unit figures of DESIGN.md.
-def algorithmic_bytes(cat, C_cells, P, scalar=4):
+# Algorithmic bytes per launch of each timed category (the per-unit figures
+# of DESIGN.md): A = active cells of level 0 (active tiles x 2048 cells),
+# C = all cells, P = particles, s = bytes per scalar.
+def algorithmic_bytes(cat, A, C_cells, P, scalar=4):
     s = scalar
     table = {
-        # one red or black half-sweep on level 0: z, cx, cy, cz, type over all
-        # cells, r and diag of the updated colour, write half of z
-        "smooth_fine": (4 * s + 1 + s / 2 + s / 2 + s / 2) * C_cells,
-        # Ap = A p and p.Ap: p, diag, cx, cy, cz, type read, Ap written
-        "spmv": (5 * s + 1 + s) * C_cells,
+        # one red or black half-sweep on level 0 over the active tiles: z of
+        # every cell, r/diag/new z of the updated colour, each face
+        # coefficient once, the type byte
+        "smooth_fine": (s + 3 * s / 2 + 3 * s + 1) * A,
+        # Ap = A p and p.Ap: p, diag, 3 face coefficients, type read, Ap written
+        "spmv": (5 * s + 1 + s) * A,
         # P2G accumulation: position, velocity, affine read once per particle,
         # w and v written once per face of the three components
         "p2g": 15 * s * P + 6 * s * C_cells,
@@ -155,7 +158,7 @@ def run_ours(args):
     from liquidhairinteration_b200.model import kernel_launch_count
 
     spec = scenes.get(args.scene)
-    solver = spec.solver_params()
+    solver = spec.solver_params(eager=1 if args.eager else 0)
     model = scenes.build(spec, args.precision, solver)
     ps = model.GetParticleSystem()
     n_particles = ps.NumParticles()
@@ -177,14 +180,14 @@ def run_ours(args):
         model.Step(spec.dt)
     model.sync()
 
-    # ---- timed region: K steps on device-resident state
+    # ---- timed region: K steps on device-resident state (the solve runs as
+    # one CUDA graph per step; no per-kernel events in here)
     clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank)
     iters, solve_ms = [], []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
     model.sync()
-    model.profile(True)
     launches0 = kernel_launch_count()
     clocks.start()
     ev0.record(stream)
@@ -198,21 +201,32 @@ def run_ours(args):
     ev1.synchronize()
     launches = kernel_launch_count() - launches0
     clock_info = clocks.stop()
-    model.profile(False)
-    prof = model.profile_read()
     torch.cuda.synchronize()
     barrier()
     ms_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     solve_avg = max_over_ranks(sum(solve_ms) / len(solve_ms))
 
+    # ---- per-kernel breakdown: separate profiled steps (CUDA events around
+    # every launch on the library's stream; the PCG loop runs host-driven
+    # here, which changes launch gaps but not kernel durations)
+    prof_steps = max(1, min(3, args.steps))
+    model.profile(True)
+    for _ in range(prof_steps):
+        model.PreStep(spec.dt)
+        model.Step(spec.dt)
+    model.profile(False)
+    prof = model.profile_read()
+    active, total, _ = model.GetSolver().ActiveTiles(0)
+    active_cells = active * 8 * 8 * 32
+
     # ---- roofline of the dominant kernel category
     peak, peak_kind = measured_peaks()
     cells = spec.n ** 3
     scalar = 8 if args.precision == "fp64" else 4
-    dominant = max((k for k in prof if algorithmic_bytes(k, cells, n_particles, scalar) is not None),
+    dominant = max((k for k in prof if algorithmic_bytes(k, active_cells, cells, n_particles, scalar) is not None),
                    key=lambda k: prof[k][1])
     n_launch, tot_ms = prof[dominant]
-    algo = algorithmic_bytes(dominant, cells, n_particles, scalar)
+    algo = algorithmic_bytes(dominant, active_cells, cells, n_particles, scalar)
     avg_ms = tot_ms / max(n_launch, 1)
     achieved = algo / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
     traffic = None
@@ -222,8 +236,8 @@ def run_ours(args):
         traffic = tj.get(args.scene, {}).get(dominant)
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(avg_ms, 5),
-                "launches_timed": n_launch}
+                "algorithmic_bytes_per_launch": int(algo), "avg_launch_ms": round(avg_ms, 5),
+                "launches_profiled": n_launch, "active_tiles_level0": f"{active}/{total}"}
 
     # ---- e2e through the C-ABI with host buffers
     e2e = None
@@ -282,7 +296,7 @@ def run_ours(args):
             "scenes_per_s": round(world * 1000.0 / ms_step, 3),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clock_info,
-            "kernel_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in prof.items()},
+            "kernel_ms_per_step": {k: round(v[1] / prof_steps, 3) for k, v in prof.items()},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -101,7 +101,14 @@ typedef struct lhi_solver_params {   /* SolverParameter<3> (SceneParameter.h:10-
                                         (0 = never)                            */
     int32_t update_region;           /* LHI_REGION_* (0 = reference)           */
     int32_t smoother;                /* LHI_SMOOTHER_* (0 = reference)         */
-    int32_t reserved[3];
+    int32_t coarse_cells;            /* MG levels below the finest with at most
+                                        this many cells are solved together by
+                                        one CTA in shared memory (0 => 4096)   */
+    int32_t eager;                   /* 1: the host drives the PCG loop (one
+                                        synchronisation per iteration); 0: the
+                                        loop runs on the device as a CUDA graph
+                                        with a conditional while node          */
+    int32_t reserved[1];
 } lhi_solver_params;
 
 typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> */
@@ -251,6 +258,12 @@ LHI_API int lhi_solver_get_stats(lhi_liquid* h, lhi_solve_stats* stats);
 /* CGSolver<3>::GetAx (PressureSolver.cpp:700-717) applied to a whole level:
    out = A_level * x (host buffers, ncells(level) host scalars). */
 LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void* out);
+/* Active tiles of one MG level after the last BuildLHS: tiles of 8 x 8 x 32
+   cells (x, y, z) holding a cell with phi <= 0 or covering an active tile of
+   the next finer level; the V-cycle and PCG kernels visit only these.
+   Levels solved by the single-CTA coarse kernel report *coarse = 1. */
+LHI_API int lhi_solver_active_tiles(lhi_liquid* h, int32_t level, int32_t* active, int32_t* total,
+                                    int32_t* coarse);
 
 /* -------------------------------------------------------------- fields */
 LHI_API int lhi_liquid_field_size(const lhi_liquid* h, int32_t field, int32_t level,

@@ -52,6 +52,7 @@ SIGNATURES = {
     "lhi_solver_solve": [_h, C.c_double, C.c_double, C.POINTER(abi.SolveStats)],
     "lhi_solver_get_stats": [_h, C.POINTER(abi.SolveStats)],
     "lhi_solver_get_ax": [_h, C.c_int32, _vp, _vp],
+    "lhi_solver_active_tiles": [_h, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
     "lhi_liquid_field_size": [_h, C.c_int32, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)],
     "lhi_liquid_get_field": [_h, C.c_int32, C.c_int32, _vp],
     "lhi_liquid_set_field": [_h, C.c_int32, C.c_int32, _vp],

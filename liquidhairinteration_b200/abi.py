@@ -108,7 +108,8 @@ class SolverParams(C.Structure):
                 ("num_final_smooth", C.c_int32), ("smoothing_factor", C.c_double),
                 ("tolerance_mode", C.c_int32), ("cg_variant", C.c_int32),
                 ("true_residual_every", C.c_int32), ("update_region", C.c_int32),
-                ("smoother", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("smoother", C.c_int32), ("coarse_cells", C.c_int32), ("eager", C.c_int32),
+                ("reserved", C.c_int32 * 1)]
 
 
 class LiquidParams(C.Structure):
@@ -148,7 +149,8 @@ def make_grid_desc(dim, min_coord, max_coord):
 def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECOND_MULTIGRID,
                        num_level=4, num_pre_smooth=5, num_post_smooth=5, num_final_smooth=20,
                        smoothing_factor=0.5, tolerance_mode=TOL_ABSOLUTE, cg_variant=CG_REFERENCE,
-                       true_residual_every=0, update_region=REGION_INTERIOR, smoother=SMOOTHER_REFERENCE):
+                       true_residual_every=0, update_region=REGION_INTERIOR, smoother=SMOOTHER_REFERENCE,
+                       coarse_cells=0, eager=0):
     s = SolverParams()
     s.max_iterations = int(max_iterations)
     s.tolerance = float(tolerance)
@@ -163,6 +165,8 @@ def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECON
     s.true_residual_every = int(true_residual_every)
     s.update_region = int(update_region)
     s.smoother = int(smoother)
+    s.coarse_cells = int(coarse_cells)
+    s.eager = int(eager)
     return s
 
 

@@ -297,6 +297,16 @@ LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void*
     });
 }
 
+LHI_API int lhi_solver_active_tiles(lhi_liquid* h, int32_t level, int32_t* active, int32_t* total,
+                                    int32_t* coarse) {
+    NEED_HANDLE(h);
+    if (!active || !total || !coarse) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->active_tiles(level, active, total, coarse);
+        return LHI_OK;
+    });
+}
+
 LHI_API int lhi_liquid_field_size(const lhi_liquid* h, int32_t field, int32_t level, int64_t* count,
                                   int32_t* elem_bytes) {
     NEED_HANDLE(h);

@@ -225,4 +225,41 @@ __device__ __forceinline__ void grid_sum_finish(double (&v)[K], double* partials
     if (threadIdx.x == 0) *counter = 0u;
 }
 
+// grid_sum_finish, but the totals go to thread 0 of the last block to
+// finish (the call returns true there, false everywhere else) instead of
+// being stored, so that block can act on them (scalar updates, decisions).
+template <int K>
+__device__ __forceinline__ bool grid_sum_last(double (&v)[K], double* partials, unsigned* counter, double (&tot)[K]) {
+    __shared__ bool last;
+    double part[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[k] = block_sum(v[k]);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) partials[size_t(blockIdx.x) * K + k] = part[k];
+        __threadfence();
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += ((volatile double*)partials)[size_t(b) * K + k];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = block_sum(acc[k]);
+        if (threadIdx.x == 0) tot[k] = s;
+    }
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        return true;
+    }
+    return false;
+}
+
 }  // namespace lhi

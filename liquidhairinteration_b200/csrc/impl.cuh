@@ -31,19 +31,39 @@ struct BoundaryProgram {
     double half[kMaxBoundaryNodes][3];
 };
 
-// Device-resident PCG scalars (one cache line group, read by the kernels).
+// Device-resident PCG state: scalars, control flags and the per-level
+// active-tile counts, read back by the host in one copy.
 struct SolveScalars {
-    double rz_old;   // r.z of the previous iteration
+    double rz_old;    // r.z of the previous iteration
     double rz_new;
-    double denom;    // p.Ap over interior fluid cells
-    double res2;     // sum r^2 over interior fluid cells (recursive residual)
-    double apz;      // Ap.z over interior fluid cells (flexible beta)
-    double rr_all;   // sum r^2 over all cells (initial residual)
-    double true2;    // sum (b - A x)^2 over interior fluid cells
-    double div[3];   // divergence diagnostic: sum, count, max |div|
-    double vmax;     // max |v| over particles (CFL)
-    double pad[5];
+    double denom;     // p.Ap over the update region
+    double res2;      // sum r^2 over the update region (recursive or true residual)
+    double apz;       // Ap.z over the update region (flexible beta)
+    double rr_all;    // sum r^2 over all cells (initial residual)
+    double true2;     // sum (b - A x)^2 over the update region
+    double div[3];    // divergence diagnostic: sum, count, max |div|
+    double vmax;      // max |v| over particles (CFL)
+    double alpha;
+    double beta;
+    double threshold; // stopping threshold on ||r||
+    double residual0; // ||r0|| over all cells
+    double residual;  // last ||r|| the stopping rule saw
+    double red[4];    // spare reduction outputs
+    int iter;         // PCG iterations taken
+    int stop;         // 1 once the loop has ended: every loop kernel returns at once
+    int status;       // LHI_OK / LHI_E_NOT_CONVERGED / LHI_E_NAN
+    int true_now;     // this iteration recomputes r = b - A x
+    int tile_count[kMaxLevels];
+    int pad_i[2];
 };
+
+// Active-tile set of one level: 8 x 8 x 32-cell tiles (x, y, z) holding a
+// cell with phi <= 0 at that level, or covering an active tile of the next
+// finer level; listed in increasing tile index.
+constexpr int kTileX = 8, kTileY = 8, kTileZ = 32;
+constexpr int kTileThreads = 256;  // 8 warps: warp w takes x = x0 + w, lane = z - z0
+constexpr int kDefaultCoarseCells = 4096;  // levels below the finest this small go to one CTA
+constexpr size_t kCoarseSmemBytes = 200 * 1024;  // shared memory of that CTA
 
 struct GridGeom {
     int nx, ny, nz;
@@ -59,6 +79,10 @@ template <class T> struct LevelDev {
     T* r = nullptr;
     T* z = nullptr;
     T h[3];                                  // level spacing: factor * dx
+    int tdim[3] = {0, 0, 0};                 // tiles per axis
+    int ntiles = 0;
+    uint8_t* tile_flag = nullptr;            // ntiles
+    int32_t* tiles = nullptr;                // active tile ids, count in SolveScalars::tile_count
 };
 
 // Optional per-category device timing: CUDA events on the handle's stream
@@ -173,6 +197,7 @@ public:
     virtual int solve(double rho, double dt) = 0;
     virtual lhi_solve_stats stats() const = 0;
     virtual void get_ax(int level, const void* x, void* out) = 0;
+    virtual void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) = 0;
     virtual int field_size(int field, int level, int64_t* count, int32_t* eb) = 0;
     virtual void get_field(int field, int level, void* out) = 0;
     virtual void set_field(int field, int level, const void* in) = 0;
@@ -216,6 +241,7 @@ public:
     int solve(double rho, double dt) override;
     lhi_solve_stats stats() const override { return stats_; }
     void get_ax(int level, const void* x, void* out) override;
+    void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) override;
     int field_size(int field, int level, int64_t* count, int32_t* eb) override;
     void get_field(int field, int level, void* out) override;
     void set_field(int field, int level, const void* in) override;
@@ -234,6 +260,14 @@ public:
     void restrict_to(int level);
     void prolong_to(int level);
     void vcycle();
+    void build_tiles();
+    void setup_coarse();
+    void enqueue_vcycle();
+    void enqueue_precond();
+    void enqueue_init(unsigned long long cond, int use_cond);
+    void enqueue_body(unsigned long long cond, int use_cond);
+    void enqueue_final();
+    void build_solve_graph();
     void spmv(int level, const T* x, T* y);
     void get_acoef(int level, T* host_out);
     void device_sum_launch_prep();
@@ -283,6 +317,12 @@ public:
     lhi_solver_params sp_;
     int nlev_;
     LevelDev<T> lv_[kMaxLevels];
+    int coarse_level_ = 0;   // first level solved by the single-CTA coarse kernel (nlev_ if none)
+    size_t coarse_smem_ = 0; // its dynamic shared memory
+    int tile_grid_ = 0;      // persistent CTAs of the tile kernels
+    cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on
+    cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body
+    cudaGraphExec_t solve_exec_ = nullptr;
     T* rhs_ = nullptr;
     TX* x_ = nullptr;
     T* p_ = nullptr;

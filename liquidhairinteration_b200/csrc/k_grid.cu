@@ -324,6 +324,8 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     nnode_ = (long long)(nx_ + 1) * (ny_ + 1) * (nz_ + 1);
 
     LHI_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    LHI_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    cur_ = stream_;
     LHI_CUDA(cudaEventCreate(&ev0_));
     LHI_CUDA(cudaEventCreate(&ev1_));
     for (int a = 0; a < 3; ++a) {
@@ -373,7 +375,18 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
         LHI_CUDA(cudaMemsetAsync(L.phi, 0, sizeof(T) * n, stream_));
         LHI_CUDA(cudaMemsetAsync(L.r, 0, sizeof(T) * n, stream_));
         LHI_CUDA(cudaMemsetAsync(L.z, 0, sizeof(T) * n, stream_));
+        L.tdim[0] = (L.nx + kTileX - 1) / kTileX;
+        L.tdim[1] = (L.ny + kTileY - 1) / kTileY;
+        L.tdim[2] = (L.nz + kTileZ - 1) / kTileZ;
+        L.ntiles = (L.n > 0) ? L.tdim[0] * L.tdim[1] * L.tdim[2] : 0;
+        size_t nt = size_t(std::max(L.ntiles, 1));
+        LHI_CUDA(cudaMalloc(&L.tile_flag, nt));
+        LHI_CUDA(cudaMalloc(&L.tiles, sizeof(int32_t) * nt));
+        LHI_CUDA(cudaMemsetAsync(L.tile_flag, 0, nt, stream_));
+        LHI_CUDA(cudaMemsetAsync(L.tiles, 0, sizeof(int32_t) * nt, stream_));
     }
+    setup_coarse();
+    tile_grid_ = kSMs * 6;
     LHI_CUDA(cudaMalloc(&rhs_, sizeof(T) * ncell_));
     LHI_CUDA(cudaMalloc(&x_, sizeof(TX) * ncell_));
     LHI_CUDA(cudaMalloc(&p_, sizeof(T) * ncell_));
@@ -427,7 +440,11 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
         F(lv_[l].phi);
         F(lv_[l].r);
         F(lv_[l].z);
+        F(lv_[l].tile_flag);
+        F(lv_[l].tiles);
     }
+    if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+    if (side_) cudaStreamDestroy(side_);
     F(rhs_);
     F(x_);
     F(p_);

@@ -1,6 +1,6 @@
 // k_solver.cu -- CGSolver<3> on the device: per-level ghost-fluid matrix
 // assembly, SpMV, damped red-black Gauss-Seidel, restriction/prolongation,
-// the V-cycle preconditioner and the PCG loop with device-resident scalars.
+// the V-cycle preconditioner and the PCG loop, which runs on the device.
 //
 // Matrix storage: per level, diag plus one coefficient per +x/+y/+z face and
 // a cell type byte (0: phi > 0, 1: phi == 0, 2: phi < 0).  The reference's
@@ -8,6 +8,21 @@
 // neighbour has phi < 0 and 0 otherwise, and rows with phi > 0 are empty; the
 // face term is the same expression seen from both rows, so
 //   A(i, j) = [type_i >= 1] [type_j == 2] * face_coef(i, j).
+//
+// Sparsity: rows with phi > 0 are empty, so every sweep visits only the
+// level's active 8 x 8 x 32 tiles (cells with phi <= 0, plus tiles covering
+// an active finer tile so that restricted residuals are carried down).  Cells
+// outside active tiles are air cells whose values no row ever reads.
+//
+// Levels below the finest with at most coarse_cells cells (default 16^3)
+// are solved by one CTA in one launch, staged in shared memory: their
+// pre-smoothing, restriction, coarsest sweeps, prolongation, post-smoothing.
+//
+// The PCG loop keeps every scalar on the device.  By default one solve is
+// one CUDA graph: the initial V-cycle, then a conditional while node whose
+// body is one PCG iteration; the kernel that applies the stopping rule sets
+// the loop condition.  With eager = 1 the host drives the same kernels and
+// reads the stop flag after every iteration.
 #include <algorithm>
 
 #include "impl.cuh"
@@ -15,6 +30,8 @@
 namespace lhi {
 
 namespace {
+
+constexpr int kGraphIterationCap = 100000;  // hard stop of the device-side loop
 
 template <class T> struct LevelK {
     int nx, ny, nz;
@@ -91,8 +108,10 @@ template <class T> __device__ __forceinline__ T approx_w(const T* __restrict__ w
     return bilerp(b[0], b[sx], b[sy], b[sx + sy], T(0.5), T(0.5));
 }
 
+// Also marks the level's tile of every cell with phi <= 0 as active.
 template <class T>
-__global__ void k_level_phi(LevelGeom g, const T* __restrict__ fine_phi, T* __restrict__ phi, uint8_t* __restrict__ type) {
+__global__ void k_level_phi(LevelGeom g, const T* __restrict__ fine_phi, T* __restrict__ phi, uint8_t* __restrict__ type,
+                            uint8_t* __restrict__ tile_flag, int tdy, int tdz) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)g.nx * g.ny * g.nz;
     if (i >= n) return;
@@ -100,7 +119,9 @@ __global__ void k_level_phi(LevelGeom g, const T* __restrict__ fine_phi, T* __re
     decode(i, g.ny, g.nz, x, y, z);
     T ph = approx_phi(fine_phi, g, x, y, z);
     if (g.level > 0) phi[i] = ph;
-    type[i] = (ph > T(0)) ? 0 : ((ph < T(0)) ? 2 : 1);
+    const uint8_t t = (ph > T(0)) ? 0 : ((ph < T(0)) ? 2 : 1);
+    type[i] = t;
+    if (t != 0) tile_flag[((long long)(x / kTileX) * tdy + y / kTileY) * tdz + z / kTileZ] = 1;
 }
 
 // CGSolver<3>::BuildLHS for one level (PressureSolver.cpp:544-664).
@@ -185,6 +206,88 @@ __global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const T* _
     rhs[i] = b;
 }
 
+// ------------------------------------------------------------ active tiles
+struct TileK {
+    const int32_t* ids;
+    const int* count;
+    int tdy, tdz;
+    int ysplit;  // work units per tile: each takes every ysplit-th row
+};
+
+// Visits every in-grid cell of the active tiles.  A work unit is (tile, row
+// subset); persistent CTAs take units blockIdx.x, blockIdx.x + gridDim.x, ...;
+// warp w takes x = x0 + w and lane l takes z = z0 + l.  Small levels use
+// ysplit = 8 (one row per thread) so their few tiles still fill the GPU.
+template <class F> __device__ __forceinline__ void for_tiles(const TileK& tk, int nx, int ny, int nz, F&& f) {
+    const int units = *tk.count * tk.ysplit;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int t = u / tk.ysplit, sub = u - t * tk.ysplit;
+        const int id = tk.ids[t];
+        const int tz = id % tk.tdz, rest = id / tk.tdz;
+        const int ty = rest % tk.tdy, tx = rest / tk.tdy;
+        const int x = tx * kTileX + w, z = tz * kTileZ + lane;
+        if (x >= nx || z >= nz) continue;
+        const int y0 = ty * kTileY, y1 = min(y0 + kTileY, ny);
+        for (int y = y0 + sub; y < y1; y += tk.ysplit) f(x, y, z, ((long long)x * ny + y) * nz + z);
+    }
+}
+
+struct TileLevels {
+    int nlev;
+    int tdim[kMaxLevels][3];
+    uint8_t* flag[kMaxLevels];
+    int32_t* ids[kMaxLevels];
+};
+
+// One CTA: level l's flags |= its 2x2x2 child tiles' flags at level l - 1
+// (finest first), then each level's active tiles are listed in increasing
+// order (deterministic) with their count in counts[l].
+__global__ void __launch_bounds__(1024) k_tiles_finalize(TileLevels tl, int* __restrict__ counts) {
+    __shared__ int warp_tot[32];
+    __shared__ int base;
+    for (int l = 0; l < tl.nlev; ++l) {
+        const int ax = tl.tdim[l][0], ay = tl.tdim[l][1], az = tl.tdim[l][2];
+        const int n = ax * ay * az;
+        if (l > 0) {
+            const int fx = tl.tdim[l - 1][0], fy = tl.tdim[l - 1][1], fz = tl.tdim[l - 1][2];
+            for (int t = threadIdx.x; t < n; t += blockDim.x) {
+                const int tz = t % az, ty = (t / az) % ay, tx = t / (az * ay);
+                uint8_t f = tl.flag[l][t];
+                for (int c = 0; c < 8 && !f; ++c) {
+                    const int cx = 2 * tx + (c >> 2), cy = 2 * ty + ((c >> 1) & 1), cz = 2 * tz + (c & 1);
+                    if (cx < fx && cy < fy && cz < fz) f |= tl.flag[l - 1][(cx * fy + cy) * fz + cz];
+                }
+                tl.flag[l][t] = f;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) base = 0;
+        __syncthreads();
+        for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+            const int t = c0 + threadIdx.x;
+            const int f = (t < n && tl.flag[l][t]) ? 1 : 0;
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            if (lane == 0) warp_tot[w] = __popc(m);
+            __syncthreads();
+            int off = 0;
+            for (int k = 0; k < w; ++k) off += warp_tot[k];
+            const int rank = base + off + __popc(m & ((1u << lane) - 1u));
+            if (f) tl.ids[l][rank] = t;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int tot = 0;
+                for (int k = 0; k < int(blockDim.x >> 5); ++k) tot += warp_tot[k];
+                base += tot;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) counts[l] = base;
+        __syncthreads();
+    }
+}
+
 // ----------------------------------------------------------- V-cycle
 // CGSolver<3>::Smooth (PressureSolver.cpp:821-837): one colour of damped
 // red-black Gauss-Seidel; (1. - w) * z + w * term evaluated in double.
@@ -199,44 +302,21 @@ __device__ __forceinline__ void smooth_cell(const LevelK<T>& L, const T* __restr
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_smooth(LevelK<T> L, const T* __restrict__ r, T* __restrict__ z, T w,
-                                               int variant, int phase) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long n = (long long)L.nx * L.ny * L.nz;
-    if (i >= n) return;
-    int x, y, zz;
-    decode(i, L.ny, L.nz, x, y, zz);
-    if (((x + y + zz) & 1) != phase) return;
-    smooth_cell(L, r, z, w, variant, i, x, y, zz);
+__global__ void __launch_bounds__(kTileThreads) k_sweep(LevelK<T> L, TileK tk, const T* __restrict__ r, T* __restrict__ z,
+                                                        T w, int variant, int phase, const int* __restrict__ stop) {
+    if (*stop) return;
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
+        if (((x + y + zz) & 1) == phase) smooth_cell(L, r, z, w, variant, i, x, y, zz);
+    });
 }
 
-// All sweeps of a small level inside one CTA (the level is L2-resident).
+// CGSolver<3>::Restrict (PressureSolver.cpp:796-819) at one coarse cell: the
+// coarse residual is accumulated in Scalar with 0.125 * (...) evaluated in
+// double; z_c = 0.
 template <class T>
-__global__ void __launch_bounds__(1024) k_smooth_block(LevelK<T> L, const T* __restrict__ r, T* __restrict__ z, T w,
-                                                       int variant, int sweeps) {
-    long long n = (long long)L.nx * L.ny * L.nz;
-    for (int s = 0; s < sweeps; ++s)
-        for (int phase = 0; phase < 2; ++phase) {
-            for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-                int x, y, zz;
-                decode(i, L.ny, L.nz, x, y, zz);
-                if (((x + y + zz) & 1) != phase) continue;
-                smooth_cell(L, r, z, w, variant, i, x, y, zz);
-            }
-            __syncthreads();
-        }
-}
-
-// CGSolver<3>::Restrict (PressureSolver.cpp:796-819): the coarse residual is
-// accumulated in Scalar with 0.125 * (...) evaluated in double; z_c = 0.
-template <class T>
-__global__ void k_restrict(LevelK<T> F, const T* __restrict__ rf, const T* __restrict__ zf, int cnx, int cny, int cnz,
-                           T* __restrict__ rc, T* __restrict__ zc) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long n = (long long)cnx * cny * cnz;
-    if (i >= n) return;
-    int x, y, z;
-    decode(i, cny, cnz, x, y, z);
+__device__ __forceinline__ void restrict_cell(const LevelK<T>& F, const T* __restrict__ rf, const T* __restrict__ zf,
+                                              int x, int y, int z, long long i, T* __restrict__ rc,
+                                              T* __restrict__ zc) {
     const long long sy = F.nz, sx = (long long)F.ny * F.nz;
     const int bx = x << 1, by = y << 1, bz = z << 1;
     T acc = T(0);
@@ -251,157 +331,341 @@ __global__ void k_restrict(LevelK<T> F, const T* __restrict__ rf, const T* __res
     zc[i] = T(0);
 }
 
-// CGSolver<3>::Prolong (PressureSolver.cpp:774-794): piecewise-constant.
 template <class T>
-__global__ void k_prolong(int cnx, int cny, int cnz, const T* __restrict__ zc, int fny, int fnz, T* __restrict__ zf) {
+__global__ void __launch_bounds__(kTileThreads) k_restrict_t(LevelK<T> F, const T* __restrict__ rf, const T* __restrict__ zf,
+                                                             int cnx, int cny, int cnz, TileK tk, T* __restrict__ rc,
+                                                             T* __restrict__ zc, const int* __restrict__ stop) {
+    if (*stop) return;
+    for_tiles(tk, cnx, cny, cnz, [&](int x, int y, int z, long long i) { restrict_cell(F, rf, zf, x, y, z, i, rc, zc); });
+}
+
+template <class T>
+__global__ void k_restrict_dense(LevelK<T> F, const T* __restrict__ rf, const T* __restrict__ zf, int cnx, int cny,
+                                 int cnz, T* __restrict__ rc, T* __restrict__ zc, const int* __restrict__ stop) {
+    if (*stop) return;
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)cnx * cny * cnz;
     if (i >= n) return;
     int x, y, z;
     decode(i, cny, cnz, x, y, z);
-    const long long sy = fnz, sx = (long long)fny * fnz;
-    const T v = zc[i];
-    const long long b = (long long)(x << 1) * sx + (y << 1) * sy + (z << 1);
+    restrict_cell(F, rf, zf, x, y, z, i, rc, zc);
+}
+
+// CGSolver<3>::Prolong (PressureSolver.cpp:774-794): piecewise-constant,
+// written per fine cell (fine cells beyond 2 * coarse extent get nothing).
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) k_prolong_t(int fnx, int fny, int fnz, TileK tk, const T* __restrict__ zc,
+                                                            int cnx, int cny, int cnz, T* __restrict__ zf,
+                                                            const int* __restrict__ stop) {
+    if (*stop) return;
+    for_tiles(tk, fnx, fny, fnz, [&](int x, int y, int z, long long i) {
+        const int cx = x >> 1, cy = y >> 1, cz = z >> 1;
+        if (cx < cnx && cy < cny && cz < cnz) zf[i] = zf[i] + zc[((long long)cx * cny + cy) * cnz + cz];
+    });
+}
+
+// The coarse levels [first, last] of one V-cycle in a single CTA.
+template <class T> struct CoarseLevels {
+    int first, last;
+    LevelK<T> L[kMaxLevels];
+    T* r[kMaxLevels];
+    T* z[kMaxLevels];
+};
+
+template <class T>
+__device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z, T w, int variant, int sweeps) {
+    const int n = L.nx * L.ny * L.nz;
+    for (int s = 0; s < sweeps; ++s)
+        for (int phase = 0; phase < 2; ++phase) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const int zz = i % L.nz, y = (i / L.nz) % L.ny, x = i / (L.nz * L.ny);
+                if (((x + y + zz) & 1) == phase) smooth_cell(L, r, z, w, variant, i, x, y, zz);
+            }
+            __syncthreads();
+        }
+}
+
+// The whole coarse V-cycle in one CTA with every coarse level staged in
+// shared memory: r, z, diag, cx, cy, cz (Scalar) and type per level.
+template <class T>
+__global__ void __launch_bounds__(1024) k_coarse_cycle(CoarseLevels<T> c, T w, int variant, int pre, int post, int fin,
+                                                        const int* __restrict__ stop) {
+    if (*stop) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    LevelK<T> S[kMaxLevels];
+    T* r[kMaxLevels];
+    T* z[kMaxLevels];
+    size_t off = 0;
+    for (int l = c.first; l <= c.last; ++l) {
+        const LevelK<T>& G = c.L[l];
+        const int n = G.nx * G.ny * G.nz;
+        T* base = reinterpret_cast<T*>(smem + off);
+        r[l] = base;
+        z[l] = base + n;
+        T* d = base + 2 * n;
+        T* ax = base + 3 * n;
+        T* ay = base + 4 * n;
+        T* az = base + 5 * n;
+        off += size_t(6) * n * sizeof(T);
+        uint8_t* ty = smem + off;
+        off += (size_t(n) + 15) & ~size_t(15);
+        S[l] = LevelK<T>{G.nx, G.ny, G.nz, d, ax, ay, az, ty};
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            d[i] = G.diag[i];
+            ax[i] = G.cx[i];
+            ay[i] = G.cy[i];
+            az[i] = G.cz[i];
+            ty[i] = G.type[i];
+            r[l][i] = (l == c.first) ? c.r[l][i] : T(0);
+            z[l][i] = (l == c.first) ? c.z[l][i] : T(0);
+        }
+    }
+    __syncthreads();
+    for (int l = c.first; l < c.last; ++l) {
+        cta_smooth(S[l], r[l], z[l], w, variant, pre);
+        const LevelK<T>& C = S[l + 1];
+        const int n = C.nx * C.ny * C.nz;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int zz = i % C.nz, y = (i / C.nz) % C.ny, x = i / (C.nz * C.ny);
+            restrict_cell(S[l], r[l], z[l], x, y, zz, i, r[l + 1], z[l + 1]);
+        }
+        __syncthreads();
+    }
+    cta_smooth(S[c.last], r[c.last], z[c.last], w, variant, fin);
+    for (int l = c.last - 1; l >= c.first; --l) {
+        const LevelK<T>& C = S[l + 1];
+        const LevelK<T>& F = S[l];
+        const int n = C.nx * C.ny * C.nz;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int zz = i % C.nz, y = (i / C.nz) % C.ny, x = i / (C.nz * C.ny);
+            const T v = z[l + 1][i];
+            const int b = ((x << 1) * F.ny + (y << 1)) * F.nz + (zz << 1);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        long long f = b + ((k >> 2) & 1) * sx + ((k >> 1) & 1) * sy + (k & 1);
-        zf[f] = zf[f] + v;
+            for (int k = 0; k < 8; ++k) {
+                const int f = b + ((k >> 2) & 1) * F.ny * F.nz + ((k >> 1) & 1) * F.nz + (k & 1);
+                z[l][f] = z[l][f] + v;
+            }
+        }
+        __syncthreads();
+        cta_smooth(F, r[l], z[l], w, variant, post);
+    }
+    for (int l = c.first; l <= c.last; ++l) {
+        const int n = S[l].nx * S[l].ny * S[l].nz;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            c.r[l][i] = r[l][i];
+            c.z[l][i] = z[l][i];
+        }
     }
 }
 
-template <class T> __global__ void k_precond_none(long long n, const uint8_t* __restrict__ type, const T* __restrict__ r, T* __restrict__ z) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && type[i] != 0) z[i] = r[i];
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) k_precond_none_t(LevelK<T> L, TileK tk, const T* __restrict__ r,
+                                                                 T* __restrict__ z, const int* __restrict__ stop) {
+    if (*stop) return;
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
+        if (L.type[i] != 0) z[i] = r[i];
+    });
 }
-template <class T> __global__ void k_precond_jacobi(long long n, const T* __restrict__ diag, const T* __restrict__ r, T* __restrict__ z) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T d = diag[i];
-    if (!is_small(d)) z[i] = r[i] / d;
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) k_precond_jacobi_t(LevelK<T> L, TileK tk, const T* __restrict__ r,
+                                                                   T* __restrict__ z, const int* __restrict__ stop) {
+    if (*stop) return;
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
+        T d = L.diag[i];
+        if (!is_small(d)) z[i] = r[i] / d;
+    });
 }
 
 // ---------------------------------------------------------------- PCG
-// r0 = rhs on fluid cells (PressureSolver.cpp:847-856)
-template <class T> __global__ void k_init_r(long long n, const uint8_t* __restrict__ type, const T* __restrict__ rhs, T* __restrict__ r) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && type[i] != 0) r[i] = rhs[i];
+struct CgConf {
+    int region;
+    int maxit;
+    int every;       // true residual every k iterations (0 = never)
+    int flexible;
+    int rel;         // LHI_TOL_RELATIVE
+    double tol;
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+
+// Stopping rule after an update of r (PressureSolver.cpp:889-902): with a
+// true-residual period, every k-th iteration and every apparent convergence
+// is decided on r = b - A x instead (the next kernel computes it).
+__device__ void cg_decide(SolveScalars* sc, double res2, const CgConf& cf, bool after_true) {
+    const double residual = sqrt(res2);
+    sc->residual = residual;
+    if (!after_true) {
+        sc->iter += 1;
+        if (cf.every > 0 && (sc->iter % cf.every == 0 || residual < sc->threshold)) {
+            sc->true_now = 1;
+            return;
+        }
+    } else {
+        sc->true_now = 0;
+    }
+    const bool conv = residual < sc->threshold;
+    const bool bad = !isfinite(residual);
+    const bool stop = conv || bad || sc->iter >= cf.maxit || sc->iter >= kGraphIterationCap;
+    sc->status = bad ? LHI_E_NAN : (conv ? LHI_OK : LHI_E_NOT_CONVERGED);
+    if (stop) sc->stop = 1;
+    if (cf.use_cond) cudaGraphSetConditional(cf.cond, stop ? 0u : 1u);
 }
 
-// p = z on fluid cells; rz_old = r.z, rr_all = r.r over all cells
-// (PressureSolver.cpp:858-868)
+// r0 = rhs on fluid cells (PressureSolver.cpp:847-856)
 template <class T>
-__global__ void k_init_p(long long n, const uint8_t* __restrict__ type, const T* __restrict__ r, const T* __restrict__ z,
-                         T* __restrict__ p, double* __restrict__ partials, unsigned* __restrict__ counter,
-                         SolveScalars* __restrict__ sc) {
+__global__ void __launch_bounds__(kTileThreads) k_cg_init_r(LevelK<T> L, TileK tk, const T* __restrict__ rhs, T* __restrict__ r) {
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int z, long long i) {
+        if (L.type[i] != 0) r[i] = rhs[i];
+    });
+}
+
+// p = z on fluid cells; rz = r.z and rr = r.r over all cells; the stopping
+// threshold from ||r0|| (PressureSolver.cpp:858-871)
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK tk, const T* __restrict__ r,
+                                                            const T* __restrict__ z, T* __restrict__ p,
+                                                            double* __restrict__ partials, unsigned* __restrict__ counter,
+                                                            SolveScalars* __restrict__ sc, CgConf cf) {
     double v[2] = {0.0, 0.0};
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        T zi = z[i], ri = r[i];
-        if (type[i] != 0) p[i] = zi;
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
+        const T zi = z[i], ri = r[i];
+        if (L.type[i] != 0) p[i] = zi;
         v[0] += double(ri) * double(zi);
         v[1] += double(ri) * double(ri);
-    }
-    grid_sum_finish<2>(v, partials, counter, &sc->pad[1]);
+    });
+    double tot[2];
+    if (!grid_sum_last<2>(v, partials, counter, tot)) return;
+    sc->rz_old = tot[0];
+    sc->rr_all = tot[1];
+    const double r0 = sqrt(tot[1]);
+    const T t = T(cf.tol);
+    sc->residual0 = r0;
+    sc->residual = r0;
+    sc->threshold = cf.rel ? double(T(t * T(r0))) : double(t);
+    sc->iter = 0;
+    sc->true_now = 0;
+    const bool conv = r0 < sc->threshold;
+    const bool stop = conv || cf.maxit <= 0;
+    sc->status = conv ? LHI_OK : LHI_E_NOT_CONVERGED;
+    sc->stop = stop ? 1 : 0;
+    if (cf.use_cond) cudaGraphSetConditional(cf.cond, stop ? 0u : 1u);
 }
 
-// Ap = A p; denom = sum p.Ap over interior fluid cells; alpha = rz_old/denom
-// (PressureSolver.cpp:873-883)
-template <class T, class TX>
-__global__ void __launch_bounds__(256) k_spmv_dot(LevelK<T> L, int region, const T* __restrict__ p, T* __restrict__ ap,
-                                                  double* __restrict__ partials, unsigned* __restrict__ counter,
-                                                  SolveScalars* __restrict__ sc) {
+// Ap = A p; p.Ap over the update region; alpha = rz / p.Ap (PressureSolver.cpp:873-888)
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) k_cg_spmv(LevelK<T> L, TileK tk, const T* __restrict__ p, T* __restrict__ ap,
+                                                          double* __restrict__ partials, unsigned* __restrict__ counter,
+                                                          SolveScalars* __restrict__ sc, CgConf cf) {
+    if (sc->stop) return;
     double v[1] = {0.0};
-    long long n = (long long)L.nx * L.ny * L.nz;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(i, L.ny, L.nz, x, y, z);
-        T a = ax_at<T>(L, p, i, x, y, z);
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int z, long long i) {
+        const T a = ax_at<T>(L, p, i, x, y, z);
         ap[i] = a;
-        if (L.type[i] != 0 && in_region(x, y, z, L.nx, L.ny, L.nz, region)) v[0] += double(p[i]) * double(a);
-    }
-    grid_sum_finish<1>(v, partials, counter, &sc->pad[1]);
+        if (L.type[i] != 0 && in_region(x, y, z, L.nx, L.ny, L.nz, cf.region)) v[0] += double(p[i]) * double(a);
+    });
+    double tot[1];
+    if (!grid_sum_last<1>(v, partials, counter, tot)) return;
+    sc->denom = tot[0];
+    sc->alpha = sc->rz_old / tot[0];
 }
 
-// x += alpha p; r -= alpha Ap; res2 = sum r^2 on interior fluid cells
-// (PressureSolver.cpp:889-902)
+// x += alpha p; r -= alpha Ap; ||r||^2 over the update region; then the
+// stopping rule (PressureSolver.cpp:889-902)
 template <class T, class TX>
-__global__ void __launch_bounds__(256) k_update_xr(LevelK<T> L, int region, const T* __restrict__ p, const T* __restrict__ ap,
-                                                   TX* __restrict__ x, T* __restrict__ r, double* __restrict__ partials,
-                                                   unsigned* __restrict__ counter, SolveScalars* __restrict__ sc) {
-    const double alpha = sc->rz_old / sc->denom;
+__global__ void __launch_bounds__(kTileThreads) k_cg_update_xr(LevelK<T> L, TileK tk, const T* __restrict__ p,
+                                                               const T* __restrict__ ap, TX* __restrict__ x,
+                                                               T* __restrict__ r, double* __restrict__ partials,
+                                                               unsigned* __restrict__ counter,
+                                                               SolveScalars* __restrict__ sc, CgConf cf) {
+    if (sc->stop) return;
+    const double alpha = sc->alpha;
     double v[1] = {0.0};
-    long long n = (long long)L.nx * L.ny * L.nz;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int xi, yi, zi;
-        decode(i, L.ny, L.nz, xi, yi, zi);
-        if (L.type[i] == 0 || !in_region(xi, yi, zi, L.nx, L.ny, L.nz, region)) continue;
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zi, long long i) {
+        if (L.type[i] == 0 || !in_region(xi, yi, zi, L.nx, L.ny, L.nz, cf.region)) return;
         x[i] = TX(double(x[i]) + alpha * double(p[i]));
-        T rn = T(double(r[i]) - alpha * double(ap[i]));
+        const T rn = T(double(r[i]) - alpha * double(ap[i]));
         r[i] = rn;
         v[0] += double(rn) * double(rn);
-    }
-    grid_sum_finish<1>(v, partials, counter, &sc->pad[1]);
+    });
+    double tot[1];
+    if (!grid_sum_last<1>(v, partials, counter, tot)) return;
+    sc->res2 = tot[0];
+    cg_decide(sc, tot[0], cf, false);
 }
 
-// r = b - A x on interior fluid cells (optionally stored), sum of squares
+// r = b - A x on the update region (stored when `store`), summed squares.
 template <class T, class TX>
-__global__ void __launch_bounds__(256) k_true_residual(LevelK<T> L, int region, const T* __restrict__ b, const TX* __restrict__ x,
-                                                       T* __restrict__ r, int store, double* __restrict__ partials,
-                                                       unsigned* __restrict__ counter, double* __restrict__ out) {
-    double v[1] = {0.0};
-    long long n = (long long)L.nx * L.ny * L.nz;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int xi, yi, zi;
-        decode(i, L.ny, L.nz, xi, yi, zi);
-        if (L.type[i] == 0 || !in_region(xi, yi, zi, L.nx, L.ny, L.nz, region)) continue;
-        double res = double(b[i]) - ax_at<double>(L, x, i, xi, yi, zi);
+__device__ __forceinline__ void true_residual_sweep(const LevelK<T>& L, const TileK& tk, int region, const T* __restrict__ b,
+                                                    const TX* __restrict__ x, T* __restrict__ r, bool store, double& acc) {
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zi, long long i) {
+        if (L.type[i] == 0 || !in_region(xi, yi, zi, L.nx, L.ny, L.nz, region)) return;
+        const double res = double(b[i]) - ax_at<double>(L, x, i, xi, yi, zi);
         if (store) r[i] = T(res);
-        v[0] += res * res;
-    }
+        acc += res * res;
+    });
+}
+
+template <class T, class TX>
+__global__ void __launch_bounds__(kTileThreads) k_cg_true_residual(LevelK<T> L, TileK tk, const T* __restrict__ b,
+                                                                   const TX* __restrict__ x, T* __restrict__ r,
+                                                                   double* __restrict__ partials,
+                                                                   unsigned* __restrict__ counter,
+                                                                   SolveScalars* __restrict__ sc, CgConf cf) {
+    if (sc->stop || !sc->true_now) return;
+    double v[1] = {0.0};
+    true_residual_sweep(L, tk, cf.region, b, x, r, true, v[0]);
+    double tot[1];
+    if (!grid_sum_last<1>(v, partials, counter, tot)) return;
+    sc->res2 = tot[0];
+    sc->true2 = tot[0];
+    cg_decide(sc, tot[0], cf, true);
+}
+
+// ||b - A x||^2 of the final iterate (not stored)
+template <class T, class TX>
+__global__ void __launch_bounds__(kTileThreads) k_true_residual_final(LevelK<T> L, TileK tk, int region,
+                                                                      const T* __restrict__ b, const TX* __restrict__ x,
+                                                                      double* __restrict__ partials,
+                                                                      unsigned* __restrict__ counter,
+                                                                      double* __restrict__ out) {
+    double v[1] = {0.0};
+    true_residual_sweep<T, TX>(L, tk, region, b, x, nullptr, false, v[0]);
     grid_sum_finish<1>(v, partials, counter, out);
 }
 
-// rz_new = r.z over all cells (Array3::Reduce); apz = Ap.z over interior fluid
+// rz_new = r.z over all cells (Array3::Reduce); Ap.z over the update region;
+// beta (PressureSolver.cpp:905-912): Fletcher-Reeves, or Polak-Ribiere
+// -alpha Ap.z / rz_old when flexible
 template <class T>
-__global__ void __launch_bounds__(256) k_dot_rz(LevelK<T> L, int region, const T* __restrict__ r, const T* __restrict__ z,
-                                                const T* __restrict__ ap, double* __restrict__ partials,
-                                                unsigned* __restrict__ counter, double* __restrict__ out) {
+__global__ void __launch_bounds__(kTileThreads) k_cg_dot_rz(LevelK<T> L, TileK tk, const T* __restrict__ r,
+                                                            const T* __restrict__ z, const T* __restrict__ ap,
+                                                            double* __restrict__ partials, unsigned* __restrict__ counter,
+                                                            SolveScalars* __restrict__ sc, CgConf cf) {
+    if (sc->stop) return;
     double v[2] = {0.0, 0.0};
-    long long n = (long long)L.nx * L.ny * L.nz;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        T zi = z[i];
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zz, long long i) {
+        const T zi = z[i];
         v[0] += double(r[i]) * double(zi);
-        int xi, yi, zz;
-        decode(i, L.ny, L.nz, xi, yi, zz);
-        if (L.type[i] != 0 && in_region(xi, yi, zz, L.nx, L.ny, L.nz, region)) v[1] += double(ap[i]) * double(zi);
-    }
-    grid_sum_finish<2>(v, partials, counter, out);
+        if (L.type[i] != 0 && in_region(xi, yi, zz, L.nx, L.ny, L.nz, cf.region)) v[1] += double(ap[i]) * double(zi);
+    });
+    double tot[2];
+    if (!grid_sum_last<2>(v, partials, counter, tot)) return;
+    const double rz_new = tot[0], apz = tot[1];
+    sc->rz_new = rz_new;
+    sc->apz = apz;
+    sc->beta = cf.flexible ? (-sc->alpha * apz / sc->rz_old) : (rz_new / sc->rz_old);
+    sc->rz_old = rz_new;
 }
 
 // p = z + beta p on fluid cells (PressureSolver.cpp:913-921)
 template <class T>
-__global__ void k_update_p(long long n, const uint8_t* __restrict__ type, const T* __restrict__ z, T* __restrict__ p,
-                           const SolveScalars* __restrict__ sc) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || type[i] == 0) return;
-    const double beta = sc->pad[0];
-    p[i] = T(double(z[i]) + beta * double(p[i]));
-}
-
-// single-thread scalar bookkeeping between kernels
-__global__ void k_scalars_after_init(SolveScalars* sc) {
-    sc->rz_old = sc->pad[1];
-    sc->rr_all = sc->pad[2];
-}
-__global__ void k_scalars_alpha(SolveScalars* sc) { sc->denom = sc->pad[1]; }
-__global__ void k_scalars_res(SolveScalars* sc) { sc->res2 = sc->pad[1]; }
-__global__ void k_scalars_beta(SolveScalars* sc, int flexible) {
-    double rz_new = sc->pad[1], apz = sc->pad[2];
-    double alpha = sc->rz_old / sc->denom;
-    double beta = flexible ? (-alpha * apz / sc->rz_old) : (rz_new / sc->rz_old);
-    sc->rz_new = rz_new;
-    sc->apz = apz;
-    sc->pad[0] = beta;
-    sc->rz_old = rz_new;
+__global__ void __launch_bounds__(kTileThreads) k_cg_update_p(LevelK<T> L, TileK tk, const T* __restrict__ z,
+                                                              T* __restrict__ p, const SolveScalars* __restrict__ sc) {
+    if (sc->stop) return;
+    const double beta = sc->beta;
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
+        if (L.type[i] != 0) p[i] = T(double(z[i]) + beta * double(p[i]));
+    });
 }
 
 template <class T, class TX> __global__ void k_x_to_pressure(long long n, const TX* __restrict__ x, T* __restrict__ pr) {
@@ -439,11 +703,23 @@ template <class T> __global__ void k_expand_acoef(LevelK<T> L, T* __restrict__ o
     for (int k = 0; k < 6; ++k) out[6 * i + k] = c[k];
 }
 
-constexpr long long kBlockSmoothMax = 4096;
-
 }  // namespace
 
 // ------------------------------------------------------------- host side
+static int ysplit_for(int ntiles, int grid) {
+    int s = 1;
+    while (s < kTileY && ntiles * s * 2 <= grid) s *= 2;
+    return s;
+}
+template <class T> static TileK tile_k(const LevelDev<T>& L, const int* count, int grid) {
+    return TileK{L.tiles, count, L.tdim[1], L.tdim[2], ysplit_for(L.ntiles, grid)};
+}
+// persistent CTAs for a tile kernel on level L (0 when the level is empty)
+template <class T> static unsigned tile_blocks(const LevelDev<T>& L, int grid) {
+    const long long units = (long long)L.ntiles * ysplit_for(L.ntiles, grid);
+    return unsigned(std::min<long long>(units, grid));
+}
+
 template <class T, class TX> double LiquidImpl<T, TX>::read_scalar(const double* dptr) {
     double v;
     LHI_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -458,58 +734,73 @@ template <class T, class TX> void LiquidImpl<T, TX>::read_scalars() {
 
 // CGSolver<3>::Init (PressureSolver.cpp:666-680)
 template <class T, class TX> void LiquidImpl<T, TX>::solver_init() {
-    LHI_CUDA(cudaMemsetAsync(p_, 0, sizeof(T) * ncell_, stream_));
-    LHI_CUDA(cudaMemsetAsync(x_, 0, sizeof(TX) * ncell_, stream_));
-    LHI_CUDA(cudaMemsetAsync(rhs_, 0, sizeof(T) * ncell_, stream_));
+    LHI_CUDA(cudaMemsetAsync(p_, 0, sizeof(T) * ncell_, cur_));
+    LHI_CUDA(cudaMemsetAsync(x_, 0, sizeof(TX) * ncell_, cur_));
+    LHI_CUDA(cudaMemsetAsync(rhs_, 0, sizeof(T) * ncell_, cur_));
     for (int l = 0; l < nlev_; ++l) {
         LevelDev<T>& L = lv_[l];
         if (L.n == 0) continue;
-        LHI_CUDA(cudaMemsetAsync(L.r, 0, sizeof(T) * L.n, stream_));
-        LHI_CUDA(cudaMemsetAsync(L.z, 0, sizeof(T) * L.n, stream_));
-        LHI_CUDA(cudaMemsetAsync(L.diag, 0, sizeof(T) * L.n, stream_));
-        for (int a = 0; a < 3; ++a) LHI_CUDA(cudaMemsetAsync(L.cf[a], 0, sizeof(T) * L.n, stream_));
+        LHI_CUDA(cudaMemsetAsync(L.r, 0, sizeof(T) * L.n, cur_));
+        LHI_CUDA(cudaMemsetAsync(L.z, 0, sizeof(T) * L.n, cur_));
+        LHI_CUDA(cudaMemsetAsync(L.diag, 0, sizeof(T) * L.n, cur_));
+        for (int a = 0; a < 3; ++a) LHI_CUDA(cudaMemsetAsync(L.cf[a], 0, sizeof(T) * L.n, cur_));
     }
-    LHI_CUDA(cudaMemsetAsync(sc_, 0, sizeof(SolveScalars), stream_));
+    LHI_CUDA(cudaMemsetAsync(sc_, 0, sizeof(SolveScalars), cur_));
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_rhs() {
     auto ps_ = scope(LHI_KERNEL_GRID);
-    k_build_rhs<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], liquid_phi_,
-                                                                 lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_);
+    k_build_rhs<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], liquid_phi_,
+                                                              lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_);
     LHI_LAUNCH_CHECK();
 }
 
+// CGSolver<3>::BuildLHS (PressureSolver.cpp:544-664) for every level, then
+// the levels' active-tile lists.
 template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, double dt) {
     auto ps_ = scope(LHI_KERNEL_LHS);
     for (int l = 0; l < nlev_; ++l) {
         LevelDev<T>& L = lv_[l];
         if (L.n == 0) continue;
         LevelGeom g{L.nx, L.ny, L.nz, nx_, ny_, nz_, l};
-        k_level_phi<T><<<blocks_for(L.n, 256), 256, 0, stream_>>>(g, liquid_phi_, L.phi, L.type);
+        LHI_CUDA(cudaMemsetAsync(L.tile_flag, 0, size_t(L.ntiles), cur_));
+        k_level_phi<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(g, liquid_phi_, L.phi, L.type, L.tile_flag, L.tdim[1],
+                                                              L.tdim[2]);
         LHI_LAUNCH_CHECK();
         const T* phi = (l == 0) ? liquid_phi_ : L.phi;
-        k_level_matrix<T><<<blocks_for(L.n, 256), 256, 0, stream_>>>(g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1],
-                                                                     L.h[2], T(dt), T(rho), L.diag, L.cf[0],
-                                                                     L.cf[1], L.cf[2]);
+        k_level_matrix<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1],
+                                                                  L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1],
+                                                                  L.cf[2]);
         LHI_LAUNCH_CHECK();
     }
+    build_tiles();
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::build_tiles() {
+    TileLevels tl{};
+    tl.nlev = 0;
+    for (int l = 0; l < nlev_ && lv_[l].n > 0; ++l) {
+        for (int a = 0; a < 3; ++a) tl.tdim[l][a] = lv_[l].tdim[a];
+        tl.flag[l] = lv_[l].tile_flag;
+        tl.ids[l] = lv_[l].tiles;
+        tl.nlev = l + 1;
+    }
+    if (tl.nlev == 0) return;
+    k_tiles_finalize<<<1, 1024, 0, cur_>>>(tl, sc_->tile_count);
+    LHI_LAUNCH_CHECK();
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweeps) {
     LevelDev<T>& L = lv_[level];
-    if (L.n == 0 || sweeps <= 0) return;
-    T w = T(sp_.smoothing_factor);
+    const unsigned G = tile_blocks(L, tile_grid_);
+    if (L.n == 0 || sweeps <= 0 || G == 0) return;
+    const T w = T(sp_.smoothing_factor);
     const int cat = (level == 0) ? LHI_KERNEL_SMOOTH_FINE : LHI_KERNEL_SMOOTH_COARSE;
-    if (L.n <= kBlockSmoothMax) {
-        auto ps_ = scope(cat);
-        k_smooth_block<T><<<1, 1024, 0, stream_>>>(lk(L), L.r, L.z, w, sp_.smoother, sweeps);
-        LHI_LAUNCH_CHECK();
-        return;
-    }
+    const TileK tk = tile_k(L, &sc_->tile_count[level], tile_grid_);
     for (int s = 0; s < sweeps; ++s)
         for (int phase = 0; phase < 2; ++phase) {
             auto ps_ = scope(cat);
-            k_smooth<T><<<blocks_for(L.n, 256), 256, 0, stream_>>>(lk(L), L.r, L.z, w, sp_.smoother, phase);
+            k_sweep<T><<<G, kTileThreads, 0, cur_>>>(lk(L), tk, L.r, L.z, w, sp_.smoother, phase, &sc_->stop);
             LHI_LAUNCH_CHECK();
         }
 }
@@ -519,52 +810,252 @@ template <class T, class TX> void LiquidImpl<T, TX>::restrict_to(int level) {
     LevelDev<T>& F = lv_[level - 1];
     if (C.n == 0) return;
     auto ps_ = scope(LHI_KERNEL_RESTRICT);
-    k_restrict<T><<<blocks_for(C.n, 256), 256, 0, stream_>>>(lk(F), F.r, F.z, C.nx, C.ny, C.nz, C.r, C.z);
+    if (level >= coarse_level_) {
+        k_restrict_dense<T><<<blocks_for(C.n, 256), 256, 0, cur_>>>(lk(F), F.r, F.z, C.nx, C.ny, C.nz, C.r, C.z,
+                                                                     &sc_->stop);
+    } else {
+        const unsigned G = tile_blocks(C, tile_grid_);
+        k_restrict_t<T><<<G, kTileThreads, 0, cur_>>>(lk(F), F.r, F.z, C.nx, C.ny, C.nz,
+                                                      tile_k(C, &sc_->tile_count[level], tile_grid_), C.r, C.z,
+                                                      &sc_->stop);
+    }
     LHI_LAUNCH_CHECK();
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::prolong_to(int level) {
     LevelDev<T>& C = lv_[level + 1];
     LevelDev<T>& F = lv_[level];
-    if (C.n == 0) return;
+    const unsigned G = tile_blocks(F, tile_grid_);
+    if (C.n == 0 || F.n == 0 || G == 0) return;
     auto ps_ = scope(LHI_KERNEL_PROLONG);
-    k_prolong<T><<<blocks_for(C.n, 256), 256, 0, stream_>>>(C.nx, C.ny, C.nz, C.z, F.ny, F.nz, F.z);
+    k_prolong_t<T><<<G, kTileThreads, 0, cur_>>>(F.nx, F.ny, F.nz, tile_k(F, &sc_->tile_count[level], tile_grid_),
+                                                 C.z, C.nx, C.ny, C.nz, F.z, &sc_->stop);
     LHI_LAUNCH_CHECK();
 }
 
-template <class T, class TX> void LiquidImpl<T, TX>::vcycle() {
+// Bytes of shared memory the coarse kernel needs for levels [first, nlev).
+template <class T> static size_t coarse_bytes(const LevelDev<T>* lv, int first, int nlev) {
+    size_t b = 0;
+    for (int l = first; l < nlev; ++l) b += size_t(6) * lv[l].n * sizeof(T) + ((size_t(lv[l].n) + 15) & ~size_t(15));
+    return b;
+}
+
+// Picks the first level (below the finest) whose cell count is at most
+// coarse_cells and whose coarse V-cycle fits in one CTA's shared memory.
+template <class T, class TX> void LiquidImpl<T, TX>::setup_coarse() {
+    const long long cc = sp_.coarse_cells > 0 ? sp_.coarse_cells : kDefaultCoarseCells;
+    coarse_level_ = nlev_;
+    coarse_smem_ = 0;
     for (int l = 1; l < nlev_; ++l) {
-        smooth(l - 1, sp_.num_pre_smooth);
-        restrict_to(l);
+        const size_t b = coarse_bytes(lv_, l, nlev_);
+        if (lv_[l].n <= cc && b <= kCoarseSmemBytes) {
+            coarse_level_ = l;
+            coarse_smem_ = b;
+            break;
+        }
     }
-    smooth(nlev_ - 1, sp_.num_final_smooth);
-    for (int l = nlev_ - 2; l >= 0; --l) {
-        prolong_to(l);
-        smooth(l, sp_.num_post_smooth);
+    LHI_CUDA(cudaFuncSetAttribute(k_coarse_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(kCoarseSmemBytes)));
+}
+
+// CGSolver<3>::ApplyPreconditioner multigrid branch (PressureSolver.cpp:730-771)
+template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle() {
+    const int last = nlev_ - 1;
+    const int Lc = coarse_level_;
+    if (Lc <= last) {
+        for (int l = 0; l < Lc; ++l) {
+            smooth(l, sp_.num_pre_smooth);
+            restrict_to(l + 1);
+        }
+        CoarseLevels<T> c{};
+        c.first = Lc;
+        c.last = last;
+        for (int l = Lc; l <= last; ++l) {
+            c.L[l] = lk(lv_[l]);
+            c.r[l] = lv_[l].r;
+            c.z[l] = lv_[l].z;
+        }
+        {
+            auto ps_ = scope(LHI_KERNEL_SMOOTH_COARSE);
+            k_coarse_cycle<T><<<1, 1024, coarse_smem_, cur_>>>(c, T(sp_.smoothing_factor), sp_.smoother,
+                                                                sp_.num_pre_smooth, sp_.num_post_smooth,
+                                                                sp_.num_final_smooth, &sc_->stop);
+            LHI_LAUNCH_CHECK();
+        }
+        for (int l = Lc - 1; l >= 0; --l) {
+            prolong_to(l);
+            smooth(l, sp_.num_post_smooth);
+        }
+    } else {
+        for (int l = 0; l < last; ++l) {
+            smooth(l, sp_.num_pre_smooth);
+            restrict_to(l + 1);
+        }
+        smooth(last, sp_.num_final_smooth);
+        for (int l = last - 1; l >= 0; --l) {
+            prolong_to(l);
+            smooth(l, sp_.num_post_smooth);
+        }
     }
 }
 
-// CGSolver<3>::ApplyPreconditioner (PressureSolver.cpp:719-772)
-template <class T, class TX> void LiquidImpl<T, TX>::apply_preconditioner() {
+template <class T, class TX> void LiquidImpl<T, TX>::vcycle() { enqueue_vcycle(); }
+
+template <class T, class TX> void LiquidImpl<T, TX>::enqueue_precond() {
     LevelDev<T>& L0 = lv_[0];
+    const unsigned G = tile_blocks(L0, tile_grid_);
     switch (sp_.preconditioner) {
         case LHI_PRECOND_NONE:
-            k_precond_none<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, L0.r, L0.z);
+            if (G == 0) break;
+            k_precond_none_t<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tile_k(L0, &sc_->tile_count[0], tile_grid_),
+                                                              L0.r, L0.z, &sc_->stop);
             LHI_LAUNCH_CHECK();
             break;
         case LHI_PRECOND_JACOBI:
-            k_precond_jacobi<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.diag, L0.r, L0.z);
+            if (G == 0) break;
+            k_precond_jacobi_t<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tile_k(L0, &sc_->tile_count[0], tile_grid_),
+                                                                L0.r, L0.z, &sc_->stop);
             LHI_LAUNCH_CHECK();
             break;
-        default: vcycle();
+        default: enqueue_vcycle();
     }
 }
 
-template <class T, class TX> void LiquidImpl<T, TX>::spmv(int level, const T* x, T* y) {
-    LevelDev<T>& L = lv_[level];
-    if (L.n == 0) return;
-    k_get_ax<T><<<blocks_for(L.n, 256), 256, 0, stream_>>>(lk(L), x, y);
+// CGSolver<3>::ApplyPreconditioner (PressureSolver.cpp:719-772) as a stage
+template <class T, class TX> void LiquidImpl<T, TX>::apply_preconditioner() {
+    LHI_CUDA(cudaMemsetAsync(&sc_->stop, 0, sizeof(int), cur_));
+    enqueue_precond();
+}
+
+static CgConf make_conf(const lhi_solver_params& sp, unsigned long long cond, int use_cond) {
+    CgConf c;
+    c.region = sp.update_region;
+    c.maxit = sp.max_iterations;
+    c.every = sp.true_residual_every;
+    c.flexible = sp.cg_variant == LHI_CG_FLEXIBLE ? 1 : 0;
+    c.rel = sp.tolerance_mode == LHI_TOL_RELATIVE ? 1 : 0;
+    c.tol = sp.tolerance;
+    c.cond = cond;
+    c.use_cond = use_cond;
+    return c;
+}
+
+// r = b; z = M r; p = z; rz; ||r0||; threshold (PressureSolver.cpp:845-871)
+template <class T, class TX> void LiquidImpl<T, TX>::enqueue_init(unsigned long long cond, int use_cond) {
+    LevelDev<T>& L0 = lv_[0];
+    const TileK tk = tile_k(L0, &sc_->tile_count[0], tile_grid_);
+    const unsigned G = std::max(1u, tile_blocks(L0, tile_grid_));
+    const CgConf cf = make_conf(sp_, cond, use_cond);
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_cg_init_r<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, L0.r);
+        LHI_LAUNCH_CHECK();
+    }
+    enqueue_precond();
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_cg_init_p<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, L0.r, L0.z, p_, partials_, counter_, sc_, cf);
+        LHI_LAUNCH_CHECK();
+    }
+}
+
+// One PCG iteration (PressureSolver.cpp:870-922).
+template <class T, class TX> void LiquidImpl<T, TX>::enqueue_body(unsigned long long cond, int use_cond) {
+    LevelDev<T>& L0 = lv_[0];
+    const TileK tk = tile_k(L0, &sc_->tile_count[0], tile_grid_);
+    const unsigned G = std::max(1u, tile_blocks(L0, tile_grid_));
+    const CgConf cf = make_conf(sp_, cond, use_cond);
+    {
+        auto ps_ = scope(LHI_KERNEL_SPMV);
+        k_cg_spmv<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, p_, ap_, partials_, counter_, sc_, cf);
+        LHI_LAUNCH_CHECK();
+    }
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_cg_update_xr<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, p_, ap_, x_, L0.r, partials_, counter_, sc_,
+                                                            cf);
+        LHI_LAUNCH_CHECK();
+        if (sp_.true_residual_every > 0) {
+            k_cg_true_residual<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, x_, L0.r, partials_, counter_,
+                                                                    sc_, cf);
+            LHI_LAUNCH_CHECK();
+        }
+    }
+    enqueue_precond();
+    {
+        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+        k_cg_dot_rz<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, L0.r, L0.z, ap_, partials_, counter_, sc_, cf);
+        LHI_LAUNCH_CHECK();
+        k_cg_update_p<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, L0.z, p_, sc_);
+        LHI_LAUNCH_CHECK();
+    }
+}
+
+// grid.pressure = x (PressureSolver.cpp:933) and the final true residual
+template <class T, class TX> void LiquidImpl<T, TX>::enqueue_final() {
+    LevelDev<T>& L0 = lv_[0];
+    const unsigned G = std::max(1u, tile_blocks(L0, tile_grid_));
+    auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
+    k_x_to_pressure<T, TX><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(ncell_, x_, pressure_);
     LHI_LAUNCH_CHECK();
+    k_true_residual_final<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tile_k(L0, &sc_->tile_count[0], tile_grid_),
+                                                               sp_.update_region, rhs_, x_, partials_, counter_,
+                                                               &sc_->true2);
+    LHI_LAUNCH_CHECK();
+}
+
+// The solve after BuildLHS as one graph: init; while (!stop) { iteration };
+// final.  Pointers and parameters are fixed for the handle's lifetime, so
+// the graph is built on the first solve and replayed after.
+template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
+    cudaGraph_t g = nullptr;
+    LHI_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    try {
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaGraph_t cg = nullptr;
+        LHI_CUDA(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cg, nullptr, nullptr));
+        cudaGraphConditionalHandle h;
+        LHI_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+        enqueue_init(h, 1);
+        LHI_CUDA(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cg, &deps, &nd));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        LHI_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        LHI_CUDA(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+        LHI_CUDA(cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        cur_ = side_;
+        try {
+            enqueue_body(h, 1);
+        } catch (...) {
+            cur_ = stream_;
+            cudaGraph_t b2 = nullptr;
+            cudaStreamEndCapture(side_, &b2);
+            throw;
+        }
+        cur_ = stream_;
+        cudaGraph_t body_out = nullptr;
+        LHI_CUDA(cudaStreamEndCapture(side_, &body_out));
+        enqueue_final();
+        LHI_CUDA(cudaStreamEndCapture(stream_, &g));
+    } catch (...) {
+        cur_ = stream_;
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(stream_, &g2);
+        if (g2) cudaGraphDestroy(g2);
+        throw;
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    LHI_CUDA(e);
+    solve_exec_ = exec;
 }
 
 // CGSolver<3>::Solve (PressureSolver.cpp:839-934)
@@ -573,112 +1064,36 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     solver_init();
     build_rhs();
     build_lhs(rho, dt);
-    LevelDev<T>& L0 = lv_[0];
-    const LevelK<T> K0 = lk(L0);
-    const unsigned nb = std::min<unsigned>(blocks_for(ncell_, 256), unsigned(sum_blocks_));
-    {
-        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-        k_init_r<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, rhs_, L0.r);
-        LHI_LAUNCH_CHECK();
-    }
-    apply_preconditioner();
-    {
-        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-        k_init_p<T><<<nb, 256, 0, stream_>>>(ncell_, L0.type, L0.r, L0.z, p_, partials_, counter_, sc_);
-        LHI_LAUNCH_CHECK();
-        k_scalars_after_init<<<1, 1, 0, stream_>>>(sc_);
-        LHI_LAUNCH_CHECK();
-    }
-    read_scalars();
-    const double residual0 = std::sqrt(sc_host_->rr_all);
-    double residual = residual0;
-    const T tol = T(sp_.tolerance);
-    const double threshold =
-        (sp_.tolerance_mode == LHI_TOL_RELATIVE) ? double(T(tol * T(residual0))) : double(tol);
-    const bool flexible = sp_.cg_variant == LHI_CG_FLEXIBLE;
-    const int region = sp_.update_region;
-    const int every = sp_.true_residual_every;
-    int iters = 0;
-    bool converged = false;
-    for (int it = 0; it < sp_.max_iterations; ++it) {
-        if (residual < threshold) {
-            if (every > 0 && iters > 0) {  // final check on the true residual
-                {
-                    auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-                    k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 1, partials_,
-                                                                    counter_, &sc_->pad[1]);
-                    LHI_LAUNCH_CHECK();
-                    k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
-                    LHI_LAUNCH_CHECK();
-                }
-                read_scalars();
-                residual = std::sqrt(sc_host_->res2);
-                if (residual < threshold) {
-                    converged = true;
-                    break;
-                }
-            } else {
-                converged = true;
-                break;
-            }
+    if (!sp_.eager && !prof_.on) {
+        if (!solve_exec_) build_solve_graph();
+        LHI_CUDA(cudaGraphLaunch(solve_exec_, stream_));
+    } else {
+        enqueue_init(0, 0);
+        for (;;) {
+            read_scalars();
+            if (sc_host_->stop) break;
+            enqueue_body(0, 0);
         }
-        {
-            auto ps_ = scope(LHI_KERNEL_SPMV);
-            k_spmv_dot<T, TX><<<nb, 256, 0, stream_>>>(K0, region, p_, ap_, partials_, counter_, sc_);
-            LHI_LAUNCH_CHECK();
-        }
-        {
-            auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-            k_scalars_alpha<<<1, 1, 0, stream_>>>(sc_);
-            LHI_LAUNCH_CHECK();
-            k_update_xr<T, TX><<<nb, 256, 0, stream_>>>(K0, region, p_, ap_, x_, L0.r, partials_, counter_, sc_);
-            LHI_LAUNCH_CHECK();
-            k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
-            LHI_LAUNCH_CHECK();
-        }
-        ++iters;
-        if (every > 0 && iters % every == 0) {
-            auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-            k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 1, partials_, counter_,
-                                                            &sc_->pad[1]);
-            LHI_LAUNCH_CHECK();
-            k_scalars_res<<<1, 1, 0, stream_>>>(sc_);
-            LHI_LAUNCH_CHECK();
-        }
-        apply_preconditioner();
-        {
-            auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-            k_dot_rz<T><<<nb, 256, 0, stream_>>>(K0, region, L0.r, L0.z, ap_, partials_, counter_, &sc_->pad[1]);
-            LHI_LAUNCH_CHECK();
-            k_scalars_beta<<<1, 1, 0, stream_>>>(sc_, flexible ? 1 : 0);
-            LHI_LAUNCH_CHECK();
-            k_update_p<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, L0.type, L0.z, p_, sc_);
-            LHI_LAUNCH_CHECK();
-        }
-        read_scalars();
-        residual = std::sqrt(sc_host_->res2);
-        if (!std::isfinite(residual)) break;
-    }
-    if (!converged && residual < threshold) converged = true;
-    {
-        auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-        k_x_to_pressure<T, TX><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(ncell_, x_, pressure_);
-        LHI_LAUNCH_CHECK();
-        k_true_residual<T, TX><<<nb, 256, 0, stream_>>>(K0, region, rhs_, x_, L0.r, 0, partials_, counter_,
-                                                        &sc_->true2);
-        LHI_LAUNCH_CHECK();
+        enqueue_final();
     }
     LHI_CUDA(cudaEventRecord(ev1_, stream_));
     read_scalars();
     float ms = 0.f;
     LHI_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
-    stats_.iterations = iters;
-    stats_.initial_residual = residual0;
-    stats_.final_residual = residual;
+    stats_.iterations = sc_host_->iter;
+    stats_.initial_residual = sc_host_->residual0;
+    stats_.final_residual = sc_host_->residual;
     stats_.true_residual = std::sqrt(sc_host_->true2);
     stats_.solve_ms = ms;
-    stats_.status = !std::isfinite(residual) ? LHI_E_NAN : (converged ? LHI_OK : LHI_E_NOT_CONVERGED);
+    stats_.status = sc_host_->status;
     return stats_.status;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::spmv(int level, const T* x, T* y) {
+    LevelDev<T>& L = lv_[level];
+    if (L.n == 0) return;
+    k_get_ax<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(lk(L), x, y);
+    LHI_LAUNCH_CHECK();
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::get_ax(int level, const void* x, void* out) {
@@ -694,6 +1109,15 @@ template <class T, class TX> void LiquidImpl<T, TX>::get_ax(int level, const voi
     LHI_CUDA(cudaStreamSynchronize(stream_));
     cudaFree(dx);
     cudaFree(dy);
+}
+
+template <class T, class TX>
+void LiquidImpl<T, TX>::active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) {
+    if (level < 0 || level >= nlev_) throw std::invalid_argument("bad level");
+    read_scalars();
+    *active = sc_host_->tile_count[level];
+    *total = lv_[level].ntiles;
+    *coarse = (level >= coarse_level_) ? 1 : 0;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::get_acoef(int level, T* host_out) {

@@ -259,6 +259,12 @@ class CGSolver:
         call("lhi_solver_get_ax", self._m._h, int(level), _ptr(x), _ptr(out))
         return out
 
+    def ActiveTiles(self, level=0):
+        """(active tiles, total tiles, solved by the coarse CTA) of a level."""
+        a, t, c = C.c_int32(), C.c_int32(), C.c_int32()
+        call("lhi_solver_active_tiles", self._m._h, int(level), C.byref(a), C.byref(t), C.byref(c))
+        return a.value, t.value, bool(c.value)
+
     def Stats(self):
         st = abi.SolveStats()
         call("lhi_solver_get_stats", self._m._h, C.byref(st))
