@@ -68,6 +68,64 @@ __device__ __forceinline__ C ax_at(const LevelK<T>& L, const V* __restrict__ x, 
     return r;
 }
 
+// The 7-point row of one cell, loaded without data-dependent branches so a
+// thread can put the loads of several cells in flight before any arithmetic.
+// Out-of-range neighbours read the cell itself and are masked by `in`.
+template <class T, class V> struct Cell7 {
+    V zc, zn[6];
+    T d, cf[6];
+    unsigned m;  // bit k: neighbour k exists and has phi < 0
+    uint8_t tc;
+};
+
+template <class T, class V>
+__device__ __forceinline__ void load7(const LevelK<T>& L, const V* __restrict__ x, long long i, int xi, int yi, int zi,
+                                      Cell7<T, V>& s) {
+    const long long sy = L.nz, sx = (long long)L.ny * L.nz;
+    const bool in[6] = {xi + 1 < L.nx, xi > 0, yi + 1 < L.ny, yi > 0, zi + 1 < L.nz, zi > 0};
+    const long long j[6] = {in[0] ? i + sx : i, in[1] ? i - sx : i, in[2] ? i + sy : i,
+                            in[3] ? i - sy : i, in[4] ? i + 1 : i,  in[5] ? i - 1 : i};
+    s.tc = L.type[i];
+    s.d = L.diag[i];
+    s.zc = x[i];
+    uint8_t tn[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        tn[k] = L.type[j[k]];
+        s.zn[k] = x[j[k]];
+    }
+    s.cf[0] = L.cx[i];
+    s.cf[1] = L.cx[j[1]];
+    s.cf[2] = L.cy[i];
+    s.cf[3] = L.cy[j[3]];
+    s.cf[4] = L.cz[i];
+    s.cf[5] = L.cz[j[5]];
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m |= (in[k] && tn[k] == 2) ? (1u << k) : 0u;
+    s.m = m;
+}
+
+// ax_at on a loaded row: same terms in the same order (+x, -x, +y, -y, +z, -z)
+template <class C, class T, class V> __device__ __forceinline__ C ax7(const Cell7<T, V>& s) {
+    if (s.tc == 0) return C(0);
+    C r = C(s.zc) * C(s.d);
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        if (s.m & (1u << k)) r += C(s.zn[k]) * C(s.cf[k]);
+    return r;
+}
+
+// CGSolver<3>::Smooth update of one cell from its loaded row (PressureSolver.cpp:830-834)
+template <class T>
+__device__ __forceinline__ bool smooth7(const Cell7<T, T>& s, T rv, T w, int variant, T& out) {
+    if (is_small(s.d)) return false;
+    const T term = (rv - ax7<T>(s)) / s.d;
+    if (variant == LHI_SMOOTHER_DAMPED_GS) out = s.zc + w * term;
+    else out = T((1.0 - double(w)) * double(s.zc) + double(T(w * term)));
+    return true;
+}
+
 // PCG update region: fluid cells of [1, N-2]^3 (PressureSolver.cpp:874-899)
 // or, with LHI_REGION_FLUID, every fluid cell.
 __device__ __forceinline__ bool in_region(int x, int y, int z, int nx, int ny, int nz, int region) {
@@ -301,13 +359,44 @@ __device__ __forceinline__ void smooth_cell(const LevelK<T>& L, const T* __restr
     else z[i] = T((1.0 - double(w)) * double(z[i]) + double(T(w * term)));
 }
 
+// One colour of one level over its active tiles.  A thread owns (x, z) of a
+// tile and the 4 rows y of that colour; a work unit takes every ysplit-th of
+// them.  All loads of a thread's rows are issued before any update.
 template <class T>
-__global__ void __launch_bounds__(kTileThreads) k_sweep(LevelK<T> L, TileK tk, const T* __restrict__ r, T* __restrict__ z,
+__global__ void __launch_bounds__(kTileThreads, 2) k_sweep(LevelK<T> L, TileK tk, const T* __restrict__ r, T* __restrict__ z,
                                                         T w, int variant, int phase, const int* __restrict__ stop) {
     if (*stop) return;
-    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
-        if (((x + y + zz) & 1) == phase) smooth_cell(L, r, z, w, variant, i, x, y, zz);
-    });
+    const int units = *tk.count * tk.ysplit;
+    const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int t = u / tk.ysplit, sub = u - t * tk.ysplit;
+        const int id = tk.ids[t];
+        const int tz = id % tk.tdz, rest = id / tk.tdz;
+        const int ty = rest % tk.tdy, tx = rest / tk.tdy;
+        const int x = tx * kTileX + wp, zz = tz * kTileZ + lane;
+        if (x >= L.nx || zz >= L.nz) continue;
+        const int y0 = ty * kTileY;
+        const int yf = y0 + ((phase + x + zz + y0) & 1);
+        Cell7<T, T> c[4];
+        T rv[4];
+        bool act[4];
+        long long idx[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = yf + 2 * k;
+            act[k] = (k % tk.ysplit == sub) && y < L.ny;
+            if (act[k]) {
+                idx[k] = ((long long)x * L.ny + y) * L.nz + zz;
+                load7(L, z, idx[k], x, y, zz, c[k]);
+                rv[k] = r[idx[k]];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            T out;
+            if (act[k] && smooth7(c[k], rv[k], w, variant, out)) z[idx[k]] = out;
+        }
+    }
 }
 
 // CGSolver<3>::Restrict (PressureSolver.cpp:796-819) at one coarse cell: the
@@ -331,12 +420,43 @@ __device__ __forceinline__ void restrict_cell(const LevelK<T>& F, const T* __res
     zc[i] = T(0);
 }
 
+// restrict_cell with the 8 children's rows loaded 4 at a time before use;
+// the children are still summed in the reference's order.
 template <class T>
-__global__ void __launch_bounds__(kTileThreads) k_restrict_t(LevelK<T> F, const T* __restrict__ rf, const T* __restrict__ zf,
+__device__ __forceinline__ void restrict_cell_batched(const LevelK<T>& F, const T* __restrict__ rf,
+                                                      const T* __restrict__ zf, int x, int y, int z, long long i,
+                                                      T* __restrict__ rc, T* __restrict__ zc) {
+    const long long sy = F.nz, sx = (long long)F.ny * F.nz;
+    const int bx = x << 1, by = y << 1, bz = z << 1;
+    T acc = T(0);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        Cell7<T, T> c[4];
+        T rv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int a = h, b = (k >> 1) & 1, cc = k & 1;
+            const long long f = (long long)(bx + a) * sx + (by + b) * sy + (bz + cc);
+            load7(F, zf, f, bx + a, by + b, bz + cc, c[k]);
+            rv[k] = rf[f];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const T res = rv[k] - ax7<T>(c[k]);
+            acc = T(double(acc) + 0.125 * double(res));
+        }
+    }
+    rc[i] = acc;
+    zc[i] = T(0);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTileThreads, 2) k_restrict_t(LevelK<T> F, const T* __restrict__ rf, const T* __restrict__ zf,
                                                              int cnx, int cny, int cnz, TileK tk, T* __restrict__ rc,
                                                              T* __restrict__ zc, const int* __restrict__ stop) {
     if (*stop) return;
-    for_tiles(tk, cnx, cny, cnz, [&](int x, int y, int z, long long i) { restrict_cell(F, rf, zf, x, y, z, i, rc, zc); });
+    for_tiles(tk, cnx, cny, cnz,
+              [&](int x, int y, int z, long long i) { restrict_cell_batched(F, rf, zf, x, y, z, i, rc, zc); });
 }
 
 template <class T>
@@ -372,14 +492,49 @@ template <class T> struct CoarseLevels {
     T* z[kMaxLevels];
 };
 
+// Sweeps of one level inside the CTA: thread t owns cells t + k * blockDim
+// (k < 4 per batch of 4 * blockDim cells); coordinates of the first batch are decoded
+// once, and each colour loads all of a thread's cells before updating.
 template <class T>
 __device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z, T w, int variant, int sweeps) {
     const int n = L.nx * L.ny * L.nz;
+    constexpr int kPer = 4;  // cells per thread per batch
+    int ci[kPer], cx[kPer], cy[kPer], cz[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        ci[k] = threadIdx.x + k * blockDim.x;
+        const int i = ci[k] < n ? ci[k] : 0;
+        cz[k] = i % L.nz;
+        cy[k] = (i / L.nz) % L.ny;
+        cx[k] = i / (L.nz * L.ny);
+    }
     for (int s = 0; s < sweeps; ++s)
         for (int phase = 0; phase < 2; ++phase) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const int zz = i % L.nz, y = (i / L.nz) % L.ny, x = i / (L.nz * L.ny);
-                if (((x + y + zz) & 1) == phase) smooth_cell(L, r, z, w, variant, i, x, y, zz);
+            for (int base = 0; base < n; base += kPer * blockDim.x) {
+                Cell7<T, T> c[kPer];
+                T rv[kPer];
+                bool act[kPer];
+                int ii[kPer];
+#pragma unroll
+                for (int k = 0; k < kPer; ++k) {
+                    int i = base + ci[k], x = cx[k], y = cy[k], zz = cz[k];
+                    if (base > 0) {
+                        zz = i % L.nz;
+                        y = (i / L.nz) % L.ny;
+                        x = i / (L.nz * L.ny);
+                    }
+                    ii[k] = i;
+                    act[k] = i < n && ((x + y + zz) & 1) == phase;
+                    if (act[k]) {
+                        load7(L, z, i, x, y, zz, c[k]);
+                        rv[k] = r[i];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kPer; ++k) {
+                    T out;
+                    if (act[k] && smooth7(c[k], rv[k], w, variant, out)) z[ii[k]] = out;
+                }
             }
             __syncthreads();
         }
@@ -388,7 +543,7 @@ __device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z,
 // The whole coarse V-cycle in one CTA with every coarse level staged in
 // shared memory: r, z, diag, cx, cy, cz (Scalar) and type per level.
 template <class T>
-__global__ void __launch_bounds__(1024) k_coarse_cycle(CoarseLevels<T> c, T w, int variant, int pre, int post, int fin,
+__global__ void __launch_bounds__(512) k_coarse_cycle(CoarseLevels<T> c, T w, int variant, int pre, int post, int fin,
                                                         const int* __restrict__ stop) {
     if (*stop) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -551,18 +706,48 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK t
     if (cf.use_cond) cudaGraphSetConditional(cf.cond, stop ? 0u : 1u);
 }
 
-// Ap = A p; p.Ap over the update region; alpha = rz / p.Ap (PressureSolver.cpp:873-888)
+// Ap = A p; p.Ap over the update region; alpha = rz / p.Ap (PressureSolver.cpp:873-888).
+// A thread owns (x, z) of a tile and 8 rows, loaded 4 rows at a time.
 template <class T>
-__global__ void __launch_bounds__(kTileThreads) k_cg_spmv(LevelK<T> L, TileK tk, const T* __restrict__ p, T* __restrict__ ap,
+__global__ void __launch_bounds__(kTileThreads, 2) k_cg_spmv(LevelK<T> L, TileK tk, const T* __restrict__ p, T* __restrict__ ap,
                                                           double* __restrict__ partials, unsigned* __restrict__ counter,
                                                           SolveScalars* __restrict__ sc, CgConf cf) {
     if (sc->stop) return;
     double v[1] = {0.0};
-    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int z, long long i) {
-        const T a = ax_at<T>(L, p, i, x, y, z);
-        ap[i] = a;
-        if (L.type[i] != 0 && in_region(x, y, z, L.nx, L.ny, L.nz, cf.region)) v[0] += double(p[i]) * double(a);
-    });
+    const int units = *tk.count * tk.ysplit;
+    const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int t = u / tk.ysplit, sub = u - t * tk.ysplit;
+        const int id = tk.ids[t];
+        const int tz = id % tk.tdz, rest = id / tk.tdz;
+        const int ty = rest % tk.tdy, tx = rest / tk.tdy;
+        const int x = tx * kTileX + wp, zz = tz * kTileZ + lane;
+        if (x >= L.nx || zz >= L.nz) continue;
+        const int y0 = ty * kTileY;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            Cell7<T, T> c[4];
+            bool act[4];
+            long long idx[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int yy = 4 * h + k, y = y0 + yy;
+                act[k] = (yy % tk.ysplit == sub) && y < L.ny;
+                if (act[k]) {
+                    idx[k] = ((long long)x * L.ny + y) * L.nz + zz;
+                    load7(L, p, idx[k], x, y, zz, c[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!act[k]) continue;
+                const T a = ax7<T>(c[k]);
+                ap[idx[k]] = a;
+                if (c[k].tc != 0 && in_region(x, y0 + 4 * h + k, zz, L.nx, L.ny, L.nz, cf.region))
+                    v[0] += double(c[k].zc) * double(a);
+            }
+        }
+    }
     double tot[1];
     if (!grid_sum_last<1>(v, partials, counter, tot)) return;
     sc->denom = tot[0];
@@ -706,17 +891,19 @@ template <class T> __global__ void k_expand_acoef(LevelK<T> L, T* __restrict__ o
 }  // namespace
 
 // ------------------------------------------------------------- host side
-static int ysplit_for(int ntiles, int grid) {
+// Work units per tile: enough units to fill `grid` CTAs, at most max_split
+// (4 for the colour sweeps, whose threads own 4 rows; 8 otherwise).
+static int ysplit_for(int ntiles, int grid, int max_split = kTileY) {
     int s = 1;
-    while (s < kTileY && ntiles * s * 2 <= grid) s *= 2;
+    while (s < max_split && ntiles * s * 2 <= grid) s *= 2;
     return s;
 }
-template <class T> static TileK tile_k(const LevelDev<T>& L, const int* count, int grid) {
-    return TileK{L.tiles, count, L.tdim[1], L.tdim[2], ysplit_for(L.ntiles, grid)};
+template <class T> static TileK tile_k(const LevelDev<T>& L, const int* count, int grid, int max_split = kTileY) {
+    return TileK{L.tiles, count, L.tdim[1], L.tdim[2], ysplit_for(L.ntiles, grid, max_split)};
 }
 // persistent CTAs for a tile kernel on level L (0 when the level is empty)
-template <class T> static unsigned tile_blocks(const LevelDev<T>& L, int grid) {
-    const long long units = (long long)L.ntiles * ysplit_for(L.ntiles, grid);
+template <class T> static unsigned tile_blocks(const LevelDev<T>& L, int grid, int max_split = kTileY) {
+    const long long units = (long long)L.ntiles * ysplit_for(L.ntiles, grid, max_split);
     return unsigned(std::min<long long>(units, grid));
 }
 
@@ -792,11 +979,11 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_tiles() {
 
 template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweeps) {
     LevelDev<T>& L = lv_[level];
-    const unsigned G = tile_blocks(L, tile_grid_);
+    const unsigned G = tile_blocks(L, tile_grid_, 4);
     if (L.n == 0 || sweeps <= 0 || G == 0) return;
     const T w = T(sp_.smoothing_factor);
     const int cat = (level == 0) ? LHI_KERNEL_SMOOTH_FINE : LHI_KERNEL_SMOOTH_COARSE;
-    const TileK tk = tile_k(L, &sc_->tile_count[level], tile_grid_);
+    const TileK tk = tile_k(L, &sc_->tile_count[level], tile_grid_, 4);
     for (int s = 0; s < sweeps; ++s)
         for (int phase = 0; phase < 2; ++phase) {
             auto ps_ = scope(cat);
@@ -877,7 +1064,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle() {
         }
         {
             auto ps_ = scope(LHI_KERNEL_SMOOTH_COARSE);
-            k_coarse_cycle<T><<<1, 1024, coarse_smem_, cur_>>>(c, T(sp_.smoothing_factor), sp_.smoother,
+            k_coarse_cycle<T><<<1, 512, coarse_smem_, cur_>>>(c, T(sp_.smoothing_factor), sp_.smoother,
                                                                 sp_.num_pre_smooth, sp_.num_post_smooth,
                                                                 sp_.num_final_smooth, &sc_->stop);
             LHI_LAUNCH_CHECK();
