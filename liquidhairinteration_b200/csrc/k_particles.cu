@@ -170,70 +170,140 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
 // ------------------------------------------------------------------ P2G
 constexpr int kTile = 8;
 
-template <class T> struct NodeRange {
-    int lo, hi;
-};
-
 // Per-axis node offsets around the particle's cell for face component a on
 // axis i: the quadratic B-spline is non-zero for offsets [-1, 2] along the
 // face normal and [-1, 1] across it; the reference's window +-d clips it.
 __device__ __forceinline__ int off_lo(int d) { return max(-1, -d); }
 __device__ __forceinline__ int off_hi(int i, int a, int d) { return min(i == a ? 2 : 1, d); }
 
+// LiquidModel<3>::Particle2Grid accumulation (LiquidModel.cpp:614-701).
+// One CTA per 8^3-cell tile.  Thread t owns cells t and t + 256 of the tile;
+// for each face component it walks its cell's sorted particles and sums
+// their weights and APIC values for the cell's fixed window of nodes (4
+// along the component's axis, offsets -1..2; 3 across, offsets -1..1) in
+// registers, then adds each window node once into the tile's shared-memory
+// accumulators.  The lanes of a warp own distinct cells, so at any step they
+// add to distinct nodes.  Finally each touched node goes to global memory
+// with one add.  The per-particle arithmetic is the reference's, rounded the
+// same way; only the order in which particles are summed differs.
+// A particle whose own truncated index (cast<Integer>, LiquidModel.cpp:629)
+// is not the cell it was sorted into (only outside the grid, where the sort
+// key is clamped) adds its window straight to global memory.
 template <class T, int A>
-__device__ __forceinline__ void p2g_particle(const GridP<T>& g, const int d[3], const T q[3], const T g3[3],
-                                             const int ci[3], T vel, const T* Ccol, T* sw, T* sv, int lox, int loy,
-                                             int loz, bool use_smem, T* gw, T* gv) {
-    const int ext_y = kTile + 2 + (A == 1), ext_z = kTile + 2 + (A == 2);
+__device__ void p2g_particle_global(const GridP<T>& g, const int d[3], const T q[3], const T g3[3], T vel, T C0, T C1,
+                                    T C2, T* __restrict__ gw, T* __restrict__ gv) {
     const int hx = g.nx - 1 + (A == 0), hy = g.ny - 1 + (A == 1), hz = g.nz - 1 + (A == 2);
-    T ew[3][4], cc[3][4];
-    bool ok[3][4];
-    int lo[3], hi[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        lo[i] = off_lo(d[i]);
-        hi[i] = off_hi(i, A, d[i]);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            int o = k - 1;
-            int node = ci[i] + o;
-            T c = (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
-            T e = X<T>::sub(g3[i], c);
-            cc[i][k] = c;
-            ok[i][k] = (o >= lo[i] && o <= hi[i] && !(fabs(e) >= T(1.5f)));
-            ew[i][k] = ok[i][k] ? qweight(e) : T(0);
-        }
-    }
-    for (int kx = 0; kx < 4; ++kx) {
-        if (!ok[0][kx]) continue;
-        int xi = ci[0] + kx - 1;
-        if (xi < 0 || xi > hx) continue;
-        for (int ky = 0; ky < 4; ++ky) {
-            if (!ok[1][ky]) continue;
-            int yi = ci[1] + ky - 1;
-            if (yi < 0 || yi > hy) continue;
-            T wxy = X<T>::mul(ew[0][kx], ew[1][ky]);
-            T d0 = X<T>::sub(q[0], X<T>::add(X<T>::mul(cc[0][kx], g.dx[0]), g.mn[0]));
-            T d1 = X<T>::sub(q[1], X<T>::add(X<T>::mul(cc[1][ky], g.dx[1]), g.mn[1]));
-            for (int kz = 0; kz < 4; ++kz) {
-                if (!ok[2][kz]) continue;
-                int zi = ci[2] + kz - 1;
-                if (zi < 0 || zi > hz) continue;
-                T weight = X<T>::mul(wxy, ew[2][kz]);
-                T d2 = X<T>::sub(q[2], X<T>::add(X<T>::mul(cc[2][kz], g.dx[2]), g.mn[2]));
-                T val = X<T>::mul(weight, X<T>::add(vel, dot3(Ccol[0], Ccol[1], Ccol[2], d0, d1, d2)));
-                if (use_smem) {
-                    int idx = ((xi - lox) * ext_y + (yi - loy)) * ext_z + (zi - loz);
-                    atomicAdd(&sw[idx], weight);
-                    atomicAdd(&sv[idx], val);
-                } else {
-                    long long gi = ((long long)xi * (g.ny + (A == 1)) + yi) * (g.nz + (A == 2)) + zi;
-                    atomicAdd(&gw[gi], weight);
-                    atomicAdd(&gv[gi], val);
-                }
+    int ci[3];
+    for (int i = 0; i < 3; ++i) ci[i] = int(g3[i]);
+    for (int ox = max(-1, -d[0]); ox <= min(A == 0 ? 2 : 1, d[0]); ++ox) {
+        const int xi = ci[0] + ox;
+        const T cx = (A == 0) ? T(xi) : X<T>::add(T(xi), T(0.5));
+        const T e0 = X<T>::sub(g3[0], cx);
+        if (xi < 0 || xi > hx || fabs(e0) >= T(1.5f)) continue;
+        for (int oy = max(-1, -d[1]); oy <= min(A == 1 ? 2 : 1, d[1]); ++oy) {
+            const int yi = ci[1] + oy;
+            const T cy = (A == 1) ? T(yi) : X<T>::add(T(yi), T(0.5));
+            const T e1 = X<T>::sub(g3[1], cy);
+            if (yi < 0 || yi > hy || fabs(e1) >= T(1.5f)) continue;
+            const T wxy = X<T>::mul(qweight(e0), qweight(e1));
+            const T t0 = X<T>::mul(C0, X<T>::sub(q[0], X<T>::add(X<T>::mul(cx, g.dx[0]), g.mn[0])));
+            const T t1 = X<T>::mul(C1, X<T>::sub(q[1], X<T>::add(X<T>::mul(cy, g.dx[1]), g.mn[1])));
+            for (int oz = max(-1, -d[2]); oz <= min(A == 2 ? 2 : 1, d[2]); ++oz) {
+                const int zi = ci[2] + oz;
+                const T cz = (A == 2) ? T(zi) : X<T>::add(T(zi), T(0.5));
+                const T e2 = X<T>::sub(g3[2], cz);
+                if (zi < 0 || zi > hz || fabs(e2) >= T(1.5f)) continue;
+                const T weight = X<T>::mul(wxy, qweight(e2));
+                const T t2 = X<T>::mul(C2, X<T>::sub(q[2], X<T>::add(X<T>::mul(cz, g.dx[2]), g.mn[2])));
+                const T val = X<T>::mul(weight, X<T>::add(vel, X<T>::add(t0, X<T>::add(t1, t2))));
+                const long long gi = ((long long)xi * (g.ny + (A == 1)) + yi) * (g.nz + (A == 2)) + zi;
+                atomicAdd(&gw[gi], weight);
+                atomicAdd(&gv[gi], val);
             }
         }
     }
+}
+
+template <class T, int A>
+__device__ __forceinline__ void p2g_cell_component(const GridP<T>& g, const int d[3], const int ci[3], int p0, int p1,
+                                                   const T* __restrict__ pd, long long cap, T* sw, T* sv, int lox,
+                                                   int loy, int loz, T* __restrict__ gw, T* __restrict__ gv) {
+    constexpr int NX = (A == 0) ? 4 : 3, NY = (A == 1) ? 4 : 3, NZ = (A == 2) ? 4 : 3;
+    T aw[NX][NY][NZ], av[NX][NY][NZ];
+#pragma unroll
+    for (int i = 0; i < NX; ++i)
+#pragma unroll
+        for (int j = 0; j < NY; ++j)
+#pragma unroll
+            for (int k = 0; k < NZ; ++k) aw[i][j][k] = av[i][j][k] = T(0);
+    // node coordinate (grid units) of window slot s on axis i, and its validity
+    auto node_c = [&](int i, int s) -> T {
+        const int node = ci[i] + s - 1;
+        return (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
+    };
+    for (int p = p0; p < p1; ++p) {
+        const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
+        const T vel = pd[(3 + A) * cap + p];
+        const T C0 = pd[(6 + 3 * A) * cap + p], C1 = pd[(7 + 3 * A) * cap + p], C2 = pd[(8 + 3 * A) * cap + p];
+        T g3[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g3[i] = X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]);  // cwiseQuotient
+        if (int(g3[0]) != ci[0] || int(g3[1]) != ci[1] || int(g3[2]) != ci[2]) {
+            p2g_particle_global<T, A>(g, d, q, g3, vel, C0, C1, C2, gw, gv);
+            continue;
+        }
+        // per-axis weights and C_a . (x_p - x_node) terms (Eigen dot order a0 + (a1 + a2))
+        T wx[NX], wy[NY], wz[NZ], ex[NX], ey[NY], ez[NZ];
+#pragma unroll
+        for (int s2 = 0; s2 < NX; ++s2) {
+            const T c = node_c(0, s2), e = X<T>::sub(g3[0], c);
+            const int o = s2 - 1;
+            const bool ok = o >= max(-1, -d[0]) && o <= min(A == 0 ? 2 : 1, d[0]) && !(fabs(e) >= T(1.5f));
+            wx[s2] = ok ? qweight(e) : T(0);
+            ex[s2] = X<T>::mul(C0, X<T>::sub(q[0], X<T>::add(X<T>::mul(c, g.dx[0]), g.mn[0])));
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < NY; ++s2) {
+            const T c = node_c(1, s2), e = X<T>::sub(g3[1], c);
+            const int o = s2 - 1;
+            const bool ok = o >= max(-1, -d[1]) && o <= min(A == 1 ? 2 : 1, d[1]) && !(fabs(e) >= T(1.5f));
+            wy[s2] = ok ? qweight(e) : T(0);
+            ey[s2] = X<T>::mul(C1, X<T>::sub(q[1], X<T>::add(X<T>::mul(c, g.dx[1]), g.mn[1])));
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < NZ; ++s2) {
+            const T c = node_c(2, s2), e = X<T>::sub(g3[2], c);
+            const int o = s2 - 1;
+            const bool ok = o >= max(-1, -d[2]) && o <= min(A == 2 ? 2 : 1, d[2]) && !(fabs(e) >= T(1.5f));
+            wz[s2] = ok ? qweight(e) : T(0);
+            ez[s2] = X<T>::mul(C2, X<T>::sub(q[2], X<T>::add(X<T>::mul(c, g.dx[2]), g.mn[2])));
+        }
+#pragma unroll
+        for (int i = 0; i < NX; ++i)
+#pragma unroll
+            for (int j = 0; j < NY; ++j) {
+                const T wxy = X<T>::mul(wx[i], wy[j]);
+#pragma unroll
+                for (int k = 0; k < NZ; ++k) {
+                    const T weight = X<T>::mul(wxy, wz[k]);
+                    const T val = X<T>::mul(weight, X<T>::add(vel, X<T>::add(ex[i], X<T>::add(ey[j], ez[k]))));
+                    aw[i][j][k] = aw[i][j][k] + weight;
+                    av[i][j][k] = av[i][j][k] + val;
+                }
+            }
+    }
+    if (p1 == p0) return;
+    const int ext_y = kTile + 2 + (A == 1), ext_z = kTile + 2 + (A == 2);
+#pragma unroll
+    for (int i = 0; i < NX; ++i)
+#pragma unroll
+        for (int j = 0; j < NY; ++j)
+#pragma unroll
+            for (int k = 0; k < NZ; ++k) {
+                const int idx = ((ci[0] + i - 1 - lox) * ext_y + (ci[1] + j - 1 - loy)) * ext_z + (ci[2] + k - 1 - loz);
+                atomicAdd(&sw[idx], aw[i][j][k]);
+                atomicAdd(&sv[idx], av[i][j][k]);
+            }
 }
 
 template <class T> struct P2GOut {
@@ -245,38 +315,36 @@ __host__ __device__ constexpr int p2g_region(int a) {
     return (kTile + 2 + (a == 0)) * (kTile + 2 + (a == 1)) * (kTile + 2 + (a == 2));
 }
 
-// LiquidModel<3>::Particle2Grid accumulation (LiquidModel.cpp:614-701):
-// one CTA per 8^3-cell tile; its particles are the sorted runs of the tile's
-// 64 (x, y) rows.  Contributions are summed in shared memory, then each
-// touched node is added to global memory once.
 template <class T>
 __global__ void __launch_bounds__(256) k_p2g(GridP<T> g, const int32_t* __restrict__ cs, const T* __restrict__ pd,
                                              long long cap, int d0, int d1, int d2, P2GOut<T> out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
-    __shared__ int row_start[kTile * kTile];
-    __shared__ int row_pre[kTile * kTile + 1];
+    __shared__ int any;
     const int x0 = blockIdx.z * kTile, y0 = blockIdx.y * kTile, z0 = blockIdx.x * kTile;
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int r = 0; r < kTile * kTile; ++r) {
-            int x = x0 + r / kTile, y = y0 + r % kTile;
-            int cnt = 0, st = 0;
-            if (x < g.nx && y < g.ny) {
-                long long c0 = ((long long)x * g.ny + y) * g.nz + z0;
-                long long c1 = ((long long)x * g.ny + y) * g.nz + min(z0 + kTile, g.nz);
-                st = cs[c0];
-                cnt = cs[c1] - st;
-            }
-            row_start[r] = st;
-            row_pre[r] = run;
-            run += cnt;
+    // the tile's two cells of this thread and their particle ranges
+    int cnt[2], beg[2], cc[2][3];
+    int mine = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int t = threadIdx.x + h * 256;
+        cc[h][0] = x0 + (t >> 6);
+        cc[h][1] = y0 + ((t >> 3) & 7);
+        cc[h][2] = z0 + (t & 7);
+        beg[h] = 0;
+        cnt[h] = 0;
+        if (cc[h][0] < g.nx && cc[h][1] < g.ny && cc[h][2] < g.nz) {
+            const long long c = ((long long)cc[h][0] * g.ny + cc[h][1]) * g.nz + cc[h][2];
+            beg[h] = cs[c];
+            cnt[h] = cs[c + 1] - beg[h];
         }
-        row_pre[kTile * kTile] = run;
+        mine += cnt[h];
     }
+    if (threadIdx.x == 0) any = 0;
     __syncthreads();
-    const int total = row_pre[kTile * kTile];
-    if (total == 0) return;
+    if (mine) any = 1;
+    __syncthreads();
+    if (!any) return;
     const int R0 = p2g_region(0), R1 = p2g_region(1), R2 = p2g_region(2);
     const int ntot = 2 * (R0 + R1 + R2);
     for (int i = threadIdx.x; i < ntot; i += blockDim.x) acc[i] = T(0);
@@ -284,34 +352,15 @@ __global__ void __launch_bounds__(256) k_p2g(GridP<T> g, const int32_t* __restri
     T* sw[3] = {acc, acc + 2 * R0, acc + 2 * (R0 + R1)};
     T* sv[3] = {acc + R0, acc + 2 * R0 + R1, acc + 2 * (R0 + R1) + R2};
     const int d[3] = {d0, d1, d2};
-    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        int lo = 0, hi = kTile * kTile;  // find row: row_pre[r] <= k < row_pre[r+1]
-        while (hi - lo > 1) {
-            int mid = (lo + hi) >> 1;
-            if (row_pre[mid] <= k) lo = mid;
-            else hi = mid;
-        }
-        long long p = (long long)row_start[lo] + (k - row_pre[lo]);
-        T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
-        T vel[3] = {pd[3 * cap + p], pd[4 * cap + p], pd[5 * cap + p]};
-        T C[9];
-#pragma unroll
-        for (int c = 0; c < 9; ++c) C[c] = pd[(6 + c) * cap + p];
-        T g3[3];
-        int ci[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            g3[i] = X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]);  // cwiseQuotient
-            ci[i] = int(g3[i]);                                      // cast<Integer>
-        }
-        bool in_tile = ci[0] >= x0 && ci[0] < x0 + kTile && ci[1] >= y0 && ci[1] < y0 + kTile && ci[2] >= z0 &&
-                       ci[2] < z0 + kTile;
-        p2g_particle<T, 0>(g, d, q, g3, ci, vel[0], &C[0], sw[0], sv[0], x0 - 1, y0 - 1, z0 - 1, in_tile, out.w[0],
-                           out.v[0]);
-        p2g_particle<T, 1>(g, d, q, g3, ci, vel[1], &C[3], sw[1], sv[1], x0 - 1, y0 - 1, z0 - 1, in_tile, out.w[1],
-                           out.v[1]);
-        p2g_particle<T, 2>(g, d, q, g3, ci, vel[2], &C[6], sw[2], sv[2], x0 - 1, y0 - 1, z0 - 1, in_tile, out.w[2],
-                           out.v[2]);
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        const int p0 = beg[h], p1 = beg[h] + cnt[h];
+        p2g_cell_component<T, 0>(g, d, cc[h], p0, p1, pd, cap, sw[0], sv[0], x0 - 1, y0 - 1, z0 - 1, out.w[0],
+                                   out.v[0]);
+        p2g_cell_component<T, 1>(g, d, cc[h], p0, p1, pd, cap, sw[1], sv[1], x0 - 1, y0 - 1, z0 - 1, out.w[1],
+                                   out.v[1]);
+        p2g_cell_component<T, 2>(g, d, cc[h], p0, p1, pd, cap, sw[2], sv[2], x0 - 1, y0 - 1, z0 - 1, out.w[2],
+                                   out.v[2]);
     }
     __syncthreads();
     // flush: one global add per touched node
