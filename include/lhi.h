@@ -299,6 +299,37 @@ LHI_API int lhi_liquid_profile(lhi_liquid* h, int32_t enable);
    reset (synchronises the handle's stream). */
 LHI_API int lhi_liquid_profile_read(lhi_liquid* h, int32_t category, int64_t* launches, double* total_ms);
 
+/* ------------------------------------------- learned preconditioner */
+/* No counterpart in the reference: the network M(r, masks) -> search
+   direction used by LHI_PRECOND_LEARNED inside flexible PCG.  Three-level 3D
+   convolutional network, 3x3x3 kernels, 16/32/64 channels (about 140k
+   parameters), BF16 activations and weights with FP32 accumulation on the
+   tensor cores.  Parameters cross the ABI as FP32 in packed order: per layer
+   l = 0..5, W[27][cout_l][cin_l] then b[cout_l], with (cin, cout) =
+   (4,16) (16,32) (32,64) (64,32) (32,16) (16,1) and tap = (dx+1)*9 +
+   (dy+1)*3 + (dz+1). */
+typedef struct lhi_net lhi_net;
+LHI_API int lhi_net_create(uint64_t seed, lhi_net** out);
+LHI_API int lhi_net_destroy(lhi_net* net);
+LHI_API int lhi_net_num_params(int64_t* count);
+LHI_API int lhi_net_get_params(lhi_net* net, float* out);
+LHI_API int lhi_net_set_params(lhi_net* net, const float* in);
+/* z = M(r) on an n0 x n1 x n2 grid from host buffers: r (float per cell),
+   type (uint8 per cell: 0 phi > 0, 1 phi == 0, 2 phi < 0), solid (uint8
+   per cell, 1 = solid cell, may be NULL); scale > 0 fixes s, 0 uses the RMS
+   of r over cells with type != 0. */
+LHI_API int lhi_net_forward_host(lhi_net* net, const int32_t dims[3], const float* r, const uint8_t* type,
+                                 const uint8_t* solid, double scale, float* z);
+/* Self-check of the tensor-core path: one CTA computes D = A B^T (A 128 x K,
+   B N x K as BF16 bit patterns, row-major; D 128 x N float) with the same
+   tcgen05 descriptors as the network; *stage reports the last step reached
+   (1 TMEM allocated, 2 MMAs issued, 3 commit arrived, 4 result read). */
+LHI_API int lhi_net_tensor_core_selftest(int32_t n, int32_t k, const uint16_t* a, const uint16_t* b, float* d,
+                                         int32_t* stage);
+/* Gradient of sum(dz * M(r)) with respect to the packed parameters. */
+LHI_API int lhi_net_backward_host(lhi_net* net, const int32_t dims[3], const float* r, const uint8_t* type,
+                                  const uint8_t* solid, double scale, const float* dz, float* grad);
+
 /* ------------------------------------------- no-allocation divergence */
 /* No counterpart in the reference: an added entry point for callers that
    cannot allocate device memory -- a host that owns all device memory in its

@@ -43,6 +43,14 @@ SIGNATURES = {
     "lhi_liquid_advect_particles": [_h, C.c_double],
     "lhi_liquid_compute_divergence": [_h, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "lhi_liquid_get_cfl": [_h, C.POINTER(C.c_double)],
+    "lhi_net_create": [C.c_uint64, C.POINTER(C.c_void_p)],
+    "lhi_net_destroy": [C.c_void_p],
+    "lhi_net_num_params": [C.POINTER(C.c_int64)],
+    "lhi_net_get_params": [C.c_void_p, _vp],
+    "lhi_net_set_params": [C.c_void_p, _vp],
+    "lhi_net_tensor_core_selftest": [C.c_int32, C.c_int32, _vp, _vp, _vp, C.POINTER(C.c_int32)],
+    "lhi_net_forward_host": [C.c_void_p, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp],
+    "lhi_net_backward_host": [C.c_void_p, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp, _vp],
     "lhi_divergence_noalloc": [C.POINTER(C.c_int32), C.c_double, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "lhi_solver_init": [_h],

@@ -8,9 +8,19 @@
 
 #include "impl.cuh"
 #include "lhi.h"
+#include "net.cuh"
 
 struct lhi_liquid {
     std::unique_ptr<lhi::LiquidBase> impl;
+};
+
+struct lhi_net {
+    std::unique_ptr<lhi::LearnedNet> impl;
+    cudaStream_t stream = nullptr;
+    ~lhi_net() {
+        impl.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 namespace lhi {
@@ -258,6 +268,136 @@ LHI_API int lhi_divergence_noalloc(const int32_t dim[3], double dx, int32_t prec
     return guarded([&]() -> int {
         return lhi::divergence_noalloc(dim, dx, precision, liquid_phi, liquid_wx, liquid_wy, liquid_wz, vx, vy,
                                        vz, stream, mean, max_abs);
+    });
+}
+
+// ------------------------------------------------------------ network
+LHI_API int lhi_net_create(uint64_t seed, lhi_net** out) {
+    if (!out) return fail(LHI_E_INVALID_ARG, "null argument");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        std::unique_ptr<lhi_net> n(new lhi_net());
+        LHI_CUDA(cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking));
+        n->impl.reset(new lhi::LearnedNet(seed));
+        *out = n.release();
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_net_destroy(lhi_net* net) {
+    if (!net) return LHI_OK;
+    return guarded([&]() -> int {
+        delete net;
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_net_num_params(int64_t* count) {
+    if (!count) return fail(LHI_E_INVALID_ARG, "null argument");
+    *count = lhi::net_param_count();
+    return LHI_OK;
+}
+
+LHI_API int lhi_net_get_params(lhi_net* net, float* out) {
+    if (!net || !out) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        net->impl->get_params(out);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_net_set_params(lhi_net* net, const float* in) {
+    if (!net || !in) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        net->impl->set_params(in);
+        return LHI_OK;
+    });
+}
+
+namespace {
+// device copies of host inputs for the host-buffer network entry points
+struct NetHostArgs {
+    float* r = nullptr;
+    uint8_t* type = nullptr;
+    uint8_t* solid = nullptr;
+    float* z = nullptr;
+    float* dz = nullptr;
+    ~NetHostArgs() {
+        cudaFree(r);
+        cudaFree(type);
+        cudaFree(solid);
+        cudaFree(z);
+        cudaFree(dz);
+    }
+};
+
+long long net_dims_check(const int32_t dims[3]) {
+    if (!dims) throw std::invalid_argument("null dims");
+    for (int a = 0; a < 3; ++a)
+        if (dims[a] < 4 || dims[a] > 4096) throw std::invalid_argument("network grid axes must be in [4, 4096]");
+    return (long long)dims[0] * dims[1] * dims[2];
+}
+
+void net_upload(NetHostArgs& d, long long n, const float* r, const uint8_t* type, const uint8_t* solid, cudaStream_t s) {
+    LHI_CUDA(cudaMalloc(&d.r, sizeof(float) * n));
+    LHI_CUDA(cudaMalloc(&d.type, size_t(n)));
+    LHI_CUDA(cudaMalloc(&d.z, sizeof(float) * n));
+    LHI_CUDA(cudaMemcpyAsync(d.r, r, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    LHI_CUDA(cudaMemcpyAsync(d.type, type, size_t(n), cudaMemcpyHostToDevice, s));
+    if (solid) {
+        LHI_CUDA(cudaMalloc(&d.solid, size_t(n)));
+        LHI_CUDA(cudaMemcpyAsync(d.solid, solid, size_t(n), cudaMemcpyHostToDevice, s));
+    }
+}
+}  // namespace
+
+LHI_API int lhi_net_tensor_core_selftest(int32_t n, int32_t k, const uint16_t* a, const uint16_t* b, float* d,
+                                         int32_t* stage) {
+    if (!a || !b || !d || !stage) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        int st = 0;
+        const int rc = lhi::umma_selftest(a, b, n, k, d, &st);
+        *stage = st;
+        return rc == LHI_OK ? LHI_OK : fail(rc, "tensor-core self-test timed out at stage " + std::to_string(st));
+    });
+}
+
+LHI_API int lhi_net_forward_host(lhi_net* net, const int32_t dims[3], const float* r, const uint8_t* type,
+                                 const uint8_t* solid, double scale, float* z) {
+    if (!net || !r || !type || !z) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        const long long n = net_dims_check(dims);
+        NetHostArgs d;
+        net_upload(d, n, r, type, solid, net->stream);
+        const int dd[3] = {dims[0], dims[1], dims[2]};
+        net->impl->forward(dd, d.r, d.type, d.solid, d.z, scale, net->stream);
+        LHI_CUDA(cudaMemcpyAsync(z, d.z, sizeof(float) * n, cudaMemcpyDeviceToHost, net->stream));
+        LHI_CUDA(cudaStreamSynchronize(net->stream));
+        const int st = net->impl->check_status(net->stream);
+        if (st != LHI_OK)
+            return fail(st, "tensor-core pipeline wait timed out (kernel " + std::to_string(net->impl->last_timeout_[0]) +
+                                ", step " + std::to_string(net->impl->last_timeout_[1]) + ", block " +
+                                std::to_string(net->impl->last_timeout_[2]) + ")");
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_net_backward_host(lhi_net* net, const int32_t dims[3], const float* r, const uint8_t* type,
+                                  const uint8_t* solid, double scale, const float* dz, float* grad) {
+    if (!net || !r || !type || !dz || !grad) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        const long long n = net_dims_check(dims);
+        NetHostArgs d;
+        net_upload(d, n, r, type, solid, net->stream);
+        LHI_CUDA(cudaMalloc(&d.dz, sizeof(float) * n));
+        LHI_CUDA(cudaMemcpyAsync(d.dz, dz, sizeof(float) * n, cudaMemcpyHostToDevice, net->stream));
+        const int dd[3] = {dims[0], dims[1], dims[2]};
+        net->impl->zero_grad(net->stream);
+        net->impl->forward(dd, d.r, d.type, d.solid, d.z, scale, net->stream);
+        net->impl->backward(d.dz, net->stream);
+        net->impl->get_grads(grad, net->stream);
+        const int st = net->impl->check_status(net->stream);
+        return st == LHI_OK ? LHI_OK : fail(st, "tensor-core pipeline wait timed out");
     });
 }
 

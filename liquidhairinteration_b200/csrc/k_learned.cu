@@ -1,0 +1,949 @@
+// k_learned.cu -- the learned preconditioner's kernels on sm_100a.
+//
+// Convolutions are implicit GEMMs on the 5th-generation tensor cores:
+//   forward / input gradient: D[voxel][cout] += A[voxel][cin] * B[cout][cin]
+//     per tap; M = 128 voxels per CTA, N = cout (16/32/64), K = 27 taps x cin.
+//     A rows are gathered (zero padding at the grid edge) from channels-last
+//     BF16 activations into shared memory in the UMMA K-major core-matrix
+//     layout; B is the tap's pre-formatted weight tile.
+//   weight gradient: D[cout][cin] += A[cout][voxel] * B[cin][voxel] per tap
+//     with K = voxels; both operands are MN-major, which is what
+//     channels-last activations already are, so each voxel's channels are
+//     one 16-byte shared-memory store.
+// One thread issues tcgen05.mma into a TMEM accumulator; tcgen05.commit
+// arrives on an mbarrier per shared-memory stage (two stages, so loading tap
+// t + 1 overlaps the MMAs of tap t); the epilogue reads TMEM with tcgen05.ld.
+// Every mbarrier wait is bounded: on timeout the kernel records it in
+// NetStatus, waits (bounded) for its last commit, frees TMEM and returns.
+#include <algorithm>
+#include <cmath>
+#include <random>
+
+#include "net.cuh"
+#include "lhi.h"
+
+namespace lhi {
+
+namespace {
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the completion of the barrier phase with this parity:
+// non-blocking test_wait polled against a 200 ms deadline.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    const uint32_t addr = smem_u32(bar);
+    const uint64_t deadline = global_ns() + 200000000ull;
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (global_ns() > deadline) return false;
+    }
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// warp-wide
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// UMMA shared-memory descriptor, no swizzle (canonical INTERLEAVE layout):
+// start address, leading (K-direction) and stride (M/N-direction) byte
+// offsets between 8 x 16-byte core matrices, version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFFu);
+    d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+    d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+    d |= uint64_t(1) << 46;
+    return d;
+}
+
+// Instruction descriptor of kind::f16: BF16 x BF16 -> F32, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(a_mn) << 15) | (uint32_t(b_mn) << 16) |
+           (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        :
+        : "r"(d_tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// warp-collective: callers reconverge the warp first (__syncwarp)
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tap_offset(int tap, int& dx, int& dy, int& dz) {
+    dx = tap / 9 - 1;
+    dy = (tap / 3) % 3 - 1;
+    dz = tap % 3 - 1;
+}
+
+// ------------------------------------------------------------ convolution
+constexpr int kConvM = 128;  // voxels per CTA
+
+struct ConvParams {
+    const uint16_t* in;   // channels-last BF16, cin channels
+    int cin;              // padded: 16, 32 or 64
+    const uint16_t* w;    // 27 formatted B tiles [cout][cin]
+    int cout;             // padded: 16, 32 or 64
+    const float* bias;    // cout_real entries or null
+    int cout_real;
+    int nx, ny, nz;
+    long long nvox;
+    int mode;             // 0: BF16 out (+bias +skip, relu); 1: FP32 out, all channels; 2: FP32 channel 0 + bias
+    const uint16_t* skip; // BF16, cout channels (mode 0), or null
+    int relu;
+    uint16_t* out_b;
+    float* out_f;
+    NetStatus* status;
+};
+
+// out[v][n] = sum_tap sum_k in[v + off(tap)][k] * w[tap][n][k]
+__global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int abytes = kConvM * P.cin * 2;
+    const int bbytes = P.cout * P.cin * 2;
+    uint8_t* A[2] = {sm, sm + abytes};
+    uint8_t* B[2] = {sm + 2 * abytes, sm + 2 * abytes + bbytes};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * abytes + 2 * bbytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = P.cout < 32 ? 32u : uint32_t(P.cout);
+    if (tid == 0) {
+        abort_flag = 0;
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(tslot, ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    const long long v = (long long)blockIdx.x * kConvM + tid;
+    const bool valid = v < P.nvox;
+    int x = 0, y = 0, z = 0;
+    if (valid) {
+        z = int(v % P.nz);
+        const long long t = v / P.nz;
+        y = int(t % P.ny);
+        x = int(t / P.ny);
+    }
+    const int kc = P.cin / 8;             // 16-byte chunks per A/B row
+    const uint32_t sbo = uint32_t(kc) * 128;
+    const uint32_t idesc = idesc_bf16(kConvM, P.cout, 0, 0);
+    int last_tap = -1;
+    for (int tap = 0; tap < kNetTaps; ++tap) {
+        const int s = tap & 1;
+        if (tap >= 2 && !mbar_wait(&bar[s], unsigned((tap - 2) >> 1) & 1u)) abort_flag = 1;
+        int dx, dy, dz;
+        tap_offset(tap, dx, dy, dz);
+        const int xx = x + dx, yy = y + dy, zz = z + dz;
+        const bool in = valid && xx >= 0 && xx < P.nx && yy >= 0 && yy < P.ny && zz >= 0 && zz < P.nz;
+        const uint4* src = reinterpret_cast<const uint4*>(P.in + (((long long)xx * P.ny + yy) * P.nz + zz) * P.cin);
+        uint8_t* arow = A[s] + (tid >> 3) * sbo + (tid & 7) * 16;
+        for (int c = 0; c < kc; ++c) {
+            const uint4 val = in ? src[c] : make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(arow + c * 128) = val;
+        }
+        const uint4* wsrc = reinterpret_cast<const uint4*>(P.w + (long long)tap * P.cout * P.cin);
+        for (int i = tid; i < bbytes / 16; i += kConvM) reinterpret_cast<uint4*>(B[s])[i] = wsrc[i];
+        fence_async_smem();
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(A[s]), b0 = smem_u32(B[s]);
+            for (int k = 0; k < P.cin / 16; ++k)
+                umma_bf16(tmem, sdesc(a0 + k * 256, 128, sbo), sdesc(b0 + k * 256, 128, sbo), idesc,
+                          (tap > 0 || k > 0) ? 1u : 0u);
+            umma_commit(&bar[s]);
+        }
+        last_tap = tap;
+    }
+    bool ok = !abort_flag;
+    if (last_tap >= 0 && !mbar_wait(&bar[last_tap & 1], unsigned(last_tap >> 1) & 1u)) ok = false;
+    tc_fence_after();
+    __syncwarp();
+    // tcgen05.ld is warp-collective: every lane loads, only valid rows store
+    if (ok) {
+        const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+        if (P.mode == 2) {
+            float a[8];
+            tmem_ld8(trow, a);
+            if (valid) P.out_f[v] = a[0] + (P.bias ? P.bias[0] : 0.f);
+        } else {
+            for (int c0 = 0; c0 < P.cout; c0 += 8) {
+                float a[8];
+                tmem_ld8(trow + c0, a);
+                if (!valid) continue;
+                if (P.mode == 1) {
+                    float4* o = reinterpret_cast<float4*>(P.out_f + v * P.cout + c0);
+                    o[0] = make_float4(a[0], a[1], a[2], a[3]);
+                    o[1] = make_float4(a[4], a[5], a[6], a[7]);
+                } else {
+                    uint16_t sk[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    if (P.skip) *reinterpret_cast<uint4*>(sk) = *reinterpret_cast<const uint4*>(P.skip + v * P.cout + c0);
+                    uint16_t o[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int c = c0 + k;
+                        float val = a[k];
+                        if (P.bias && c < P.cout_real) val += P.bias[c];
+                        if (P.skip) val += bf16_float(sk[k]);
+                        if (P.relu) val = fmaxf(val, 0.f);
+                        o[k] = (c < P.cout_real) ? bf16_bits(val) : uint16_t(0);
+                    }
+                    *reinterpret_cast<uint4*>(P.out_b + v * P.cout + c0) = *reinterpret_cast<uint4*>(o);
+                }
+            }
+        }
+    } else if (!ok && valid) {
+        // keep the tensor well defined after a timeout
+        if (P.mode == 2) P.out_f[v] = 0.f;
+    }
+    if (!ok && tid == 0 && atomicExch(&P.status->timeout, 1) == 0) {
+        P.status->pad[0] = 1;  // kernel: convolution
+        P.status->pad[1] = last_tap;
+        P.status->pad[2] = int(blockIdx.x);
+    }
+    tc_fence_before();
+    __syncthreads();
+    __syncwarp();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ------------------------------------------------------- weight gradient
+constexpr int kWgChunk = 128;        // voxels per MMA batch (K)
+constexpr int kWgChunksPerCta = 16;
+
+struct WgradParams {
+    const uint16_t* g;   // BF16 gradient at the layer output, cout channels (padded)
+    int cout;            // padded
+    int cout_real;
+    const uint16_t* in;  // BF16 layer input, cin channels (padded)
+    int cin;             // padded
+    int cin_real;
+    int nx, ny, nz;
+    long long nvox;
+    float* grad_w;       // packed W[27][cout_real][cin_real] of the layer
+    NetStatus* status;
+};
+
+// D[co][ci] = sum_v g[v][co] * in[v + off(tap)][ci] for tap = blockIdx.y over
+// kWgChunksPerCta chunks of 128 voxels; A rows co >= cout stay zero.
+__global__ void __launch_bounds__(128) k_wgrad(WgradParams P) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    constexpr int abytes = 128 * kWgChunk * 2;  // M = 128 rows (cout padded to 128 with zeros)
+    const int bbytes = P.cin * kWgChunk * 2;
+    uint8_t* A[2] = {sm, sm + abytes};
+    uint8_t* B[2] = {sm + 2 * abytes, sm + 2 * abytes + bbytes};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * abytes + 2 * bbytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = P.cin < 32 ? 32u : uint32_t(P.cin);
+    // zero both A stages once (rows >= cout are never written again)
+    for (int i = tid; i < 2 * abytes / 16; i += 128) reinterpret_cast<uint4*>(sm)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) {
+        abort_flag = 0;
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(tslot, ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const int tap = blockIdx.y;
+    int dx, dy, dz;
+    tap_offset(tap, dx, dy, dz);
+    // MN-major layout: element (m, k) at (m / 8) * SBO + (k / 8) * 128 + (k % 8) * 16 + (m % 8) * 2
+    constexpr uint32_t sbo = (kWgChunk / 8) * 128;
+    const uint32_t idesc = idesc_bf16(128, P.cin, 1, 1);
+    int issued = 0;
+    const long long vbase = (long long)blockIdx.x * kWgChunksPerCta * kWgChunk;
+    for (int ch = 0; ch < kWgChunksPerCta; ++ch) {
+        const long long v0 = vbase + (long long)ch * kWgChunk;
+        if (v0 >= P.nvox) break;
+        const int s = ch & 1;
+        if (ch >= 2 && !mbar_wait(&bar[s], unsigned((ch - 2) >> 1) & 1u)) abort_flag = 1;
+        const long long v = v0 + tid;  // voxel k = tid of this chunk
+        bool vin = v < P.nvox, src_in = false;
+        long long src = 0;
+        if (vin) {
+            const int z = int(v % P.nz);
+            const long long t = v / P.nz;
+            const int y = int(t % P.ny), x = int(t / P.ny);
+            const int xx = x + dx, yy = y + dy, zz = z + dz;
+            src_in = xx >= 0 && xx < P.nx && yy >= 0 && yy < P.ny && zz >= 0 && zz < P.nz;
+            src = ((long long)xx * P.ny + yy) * P.nz + zz;
+        }
+        const uint32_t koff = (tid >> 3) * 128 + (tid & 7) * 16;
+        for (int c = 0; c < P.cout / 8; ++c) {
+            const uint4 val = vin ? reinterpret_cast<const uint4*>(P.g + v * P.cout)[c] : make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(A[s] + c * sbo + koff) = val;
+        }
+        for (int c = 0; c < P.cin / 8; ++c) {
+            const uint4 val = src_in ? reinterpret_cast<const uint4*>(P.in + src * P.cin)[c] : make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(B[s] + c * sbo + koff) = val;
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(A[s]), b0 = smem_u32(B[s]);
+            for (int k = 0; k < kWgChunk / 16; ++k)
+                umma_bf16(tmem, sdesc(a0 + k * 256, 128, sbo), sdesc(b0 + k * 256, 128, sbo), idesc,
+                          (issued > 0 || k > 0) ? 1u : 0u);
+            umma_commit(&bar[s]);
+        }
+        issued = ch + 1;
+    }
+    bool ok = !abort_flag;
+    if (issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], unsigned((issued - 1) >> 1) & 1u)) ok = false;
+    tc_fence_after();
+    __syncwarp();
+    if (ok && issued > 0) {
+        const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+        const int co = tid;  // TMEM lane = row of D
+        for (int c0 = 0; c0 < P.cin; c0 += 8) {
+            float a[8];
+            tmem_ld8(trow + c0, a);
+            if (co < P.cout_real)
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (c0 + k < P.cin_real)
+                        atomicAdd(&P.grad_w[((long long)tap * P.cout_real + co) * P.cin_real + c0 + k], a[k]);
+        }
+    }
+    if (!ok && tid == 0 && atomicExch(&P.status->timeout, 1) == 0) {
+        P.status->pad[0] = 2;  // kernel: weight gradient
+        P.status->pad[1] = issued;
+        P.status->pad[2] = int(blockIdx.x);
+    }
+    tc_fence_before();
+    __syncthreads();
+    __syncwarp();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// One CTA, one 128 x N x K bf16 GEMM through the same descriptors and
+// pipeline pieces as the convolutions: D[m][n] = sum_k A[m][k] B[n][k], A and
+// B given row-major in global memory (K-major).  Records in status how far
+// it got: pad[3] = 1 after TMEM allocation, 2 after the MMAs were issued, 3
+// after their commit arrived, 4 after the TMEM read.
+__global__ void __launch_bounds__(128) k_umma_selftest(const uint16_t* __restrict__ a, const uint16_t* __restrict__ b,
+                                                       int N, int K, float* __restrict__ d, NetStatus* status) {
+    __shared__ __align__(1024) uint8_t As[128 * 64 * 2];
+    __shared__ __align__(1024) uint8_t Bs[64 * 64 * 2];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tslot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int kc = K / 8;
+    const uint32_t sbo = uint32_t(kc) * 128;
+    for (int c = 0; c < kc; ++c)
+        *reinterpret_cast<uint4*>(As + (tid >> 3) * sbo + (tid & 7) * 16 + c * 128) =
+            reinterpret_cast<const uint4*>(a + (long long)tid * K)[c];
+    if (tid < N)
+        for (int c = 0; c < kc; ++c)
+            *reinterpret_cast<uint4*>(Bs + (tid >> 3) * sbo + (tid & 7) * 16 + c * 128) =
+                reinterpret_cast<const uint4*>(b + (long long)tid * K)[c];
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tmem_alloc(&tslot, 64);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tslot;
+    if (tid == 0) {
+        status->pad[3] = 1;
+        const uint32_t idesc = idesc_bf16(128, N, 0, 0);
+        for (int k = 0; k < K / 16; ++k)
+            umma_bf16(tmem, sdesc(smem_u32(As) + k * 256, 128, sbo), sdesc(smem_u32(Bs) + k * 256, 128, sbo), idesc,
+                      k > 0 ? 1u : 0u);
+        umma_commit(&bar);
+        status->pad[3] = 2;
+    }
+    const bool ok = mbar_wait(&bar, 0);
+    if (tid == 0 && ok) status->pad[3] = 3;
+    tc_fence_after();
+    __syncwarp();
+    if (ok) {
+        for (int c0 = 0; c0 < N; c0 += 8) {
+            float v[8];
+            tmem_ld8(tmem + (uint32_t(warp * 32) << 16) + c0, v);
+            for (int k = 0; k < 8; ++k) d[(long long)tid * N + c0 + k] = v[k];
+        }
+        if (tid == 0) status->pad[3] = 4;
+    } else if (tid == 0) {
+        atomicExch(&status->timeout, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 64);
+}
+
+// db[c] += sum_v g[v][c]
+__global__ void k_bias_grad(const uint16_t* __restrict__ g, int cpad, int creal, long long nvox, float* __restrict__ db) {
+    __shared__ float part[64];
+    if (threadIdx.x < 64) part[threadIdx.x] = 0.f;
+    __syncthreads();
+    const int c = threadIdx.x % cpad;
+    const int lanes = blockDim.x / cpad;
+    float acc = 0.f;
+    for (long long v = (long long)blockIdx.x * lanes + threadIdx.x / cpad; v < nvox; v += (long long)gridDim.x * lanes)
+        acc += bf16_float(g[v * cpad + c]);
+    atomicAdd(&part[c], acc);
+    __syncthreads();
+    if (threadIdx.x < creal) atomicAdd(&db[threadIdx.x], part[threadIdx.x]);
+}
+
+// ------------------------------------------------------------ elementwise
+__device__ __forceinline__ void dec3(long long v, int ny, int nz, int& x, int& y, int& z) {
+    z = int(v % nz);
+    const long long t = v / nz;
+    y = int(t % ny);
+    x = int(t / ny);
+}
+
+// sum r^2 and count over fluid cells -> s = sqrt(sum / count) (1 if empty)
+__global__ void k_net_scale(const float* __restrict__ r, const uint8_t* __restrict__ type, long long n,
+                            double* __restrict__ partials, unsigned* __restrict__ counter, float* __restrict__ scale) {
+    double v[2] = {0.0, 0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (type[i] != 0) {
+            v[0] += double(r[i]) * double(r[i]);
+            v[1] += 1.0;
+        }
+    double tot[2];
+    if (!grid_sum_last<2>(v, partials, counter, tot)) return;
+    const double s = (tot[1] > 0 && tot[0] > 0) ? sqrt(tot[0] / tot[1]) : 1.0;
+    *scale = float(s);
+}
+
+__global__ void k_net_input(const float* __restrict__ r, const uint8_t* __restrict__ type,
+                            const uint8_t* __restrict__ solid, long long n, const float* __restrict__ scale,
+                            uint16_t* __restrict__ a0) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const bool fl = type[v] != 0;
+    const bool so = !fl && solid && solid[v];
+    uint16_t o[16] = {};
+    o[0] = bf16_bits(fl ? r[v] / *scale : 0.f);
+    o[1] = bf16_bits(fl ? 1.f : 0.f);
+    o[2] = bf16_bits(so ? 1.f : 0.f);
+    o[3] = bf16_bits((!fl && !so) ? 1.f : 0.f);
+    uint4* dst = reinterpret_cast<uint4*>(a0 + v * 16);
+    dst[0] = reinterpret_cast<uint4*>(o)[0];
+    dst[1] = reinterpret_cast<uint4*>(o)[1];
+}
+
+// coarse[v][c] = bf16(0.125 * sum of the 8 children), children in (x, y, z) order
+__global__ void k_pool(const uint16_t* __restrict__ fine, int fny, int fnz, uint16_t* __restrict__ coarse, int cnx,
+                       int cny, int cnz, int C) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)cnx * cny * cnz * C;
+    if (i >= n) return;
+    const int c = int(i % C);
+    const long long v = i / C;
+    int x, y, z;
+    dec3(v, cny, cnz, x, y, z);
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const long long f = ((long long)(2 * x + (k >> 2)) * fny + (2 * y + ((k >> 1) & 1))) * fnz + (2 * z + (k & 1));
+        acc += bf16_float(fine[f * C + c]);
+    }
+    coarse[i] = bf16_bits(acc * 0.125f);
+}
+
+// fine[v][c] = coarse[parent(v)][c] (0 beyond 2 * coarse extent)
+__global__ void k_upsample(const uint16_t* __restrict__ coarse, int cnx, int cny, int cnz, uint16_t* __restrict__ fine,
+                           int fnx, int fny, int fnz, int C) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)fnx * fny * fnz * C;
+    if (i >= n) return;
+    const int c = int(i % C);
+    const long long v = i / C;
+    int x, y, z;
+    dec3(v, fny, fnz, x, y, z);
+    const int px = x >> 1, py = y >> 1, pz = z >> 1;
+    fine[i] = (px < cnx && py < cny && pz < cnz) ? coarse[(((long long)px * cny + py) * cnz + pz) * C + c] : uint16_t(0);
+}
+
+// dcoarse[v][c] = sum of the 8 children's dfine (FP32, children in order)
+__global__ void k_sum_children(const float* __restrict__ fine, int fny, int fnz, float* __restrict__ coarse, int cnx,
+                               int cny, int cnz, int C) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)cnx * cny * cnz * C;
+    if (i >= n) return;
+    const int c = int(i % C);
+    const long long v = i / C;
+    int x, y, z;
+    dec3(v, cny, cnz, x, y, z);
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const long long f = ((long long)(2 * x + (k >> 2)) * fny + (2 * y + ((k >> 1) & 1))) * fnz + (2 * z + (k & 1));
+        acc += fine[f * C + c];
+    }
+    coarse[i] = acc;
+}
+
+// g = bf16(d * relu'(u))
+__global__ void k_relu_grad(const float* __restrict__ d, const uint16_t* __restrict__ u, long long n,
+                            uint16_t* __restrict__ g) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    g[i] = bf16_bits(bf16_float(u[i]) > 0.f ? d[i] : 0.f);
+}
+
+// g = bf16((skip + 0.125 * dcoarse[parent]) * relu'(u)) at a fine level
+__global__ void k_relu_grad_unpool(const uint16_t* __restrict__ skip, const float* __restrict__ dcoarse, int cnx, int cny,
+                                   int cnz, const uint16_t* __restrict__ u, int fnx, int fny, int fnz, int C,
+                                   uint16_t* __restrict__ g) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)fnx * fny * fnz * C;
+    if (i >= n) return;
+    const int c = int(i % C);
+    const long long v = i / C;
+    int x, y, z;
+    dec3(v, fny, fnz, x, y, z);
+    const int px = x >> 1, py = y >> 1, pz = z >> 1;
+    float d = bf16_float(skip[i]);
+    if (px < cnx && py < cny && pz < cnz) d += 0.125f * dcoarse[(((long long)px * cny + py) * cnz + pz) * C + c];
+    g[i] = bf16_bits(bf16_float(u[i]) > 0.f ? d : 0.f);
+}
+
+// z = s * y on fluid cells
+__global__ void k_net_output(const float* __restrict__ y, const uint8_t* __restrict__ type, long long n,
+                             const float* __restrict__ scale, float* __restrict__ z) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    z[v] = (type[v] != 0) ? y[v] * *scale : 0.f;
+}
+
+// g5[v] = [bf16(s * dz * fluid), 0, ..., 0]
+__global__ void k_net_dy(const float* __restrict__ dz, const uint8_t* __restrict__ type, long long n,
+                         const float* __restrict__ scale, uint16_t* __restrict__ g5) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    uint16_t o[16] = {};
+    o[0] = bf16_bits(type[v] != 0 ? dz[v] * *scale : 0.f);
+    uint4* dst = reinterpret_cast<uint4*>(g5 + v * 16);
+    dst[0] = reinterpret_cast<uint4*>(o)[0];
+    dst[1] = reinterpret_cast<uint4*>(o)[1];
+}
+
+// B tiles of one layer: forward [tap][n = cout_pad][k = cin_pad] holding
+// W[tap][n][k]; backward [tap][n = cin_pad][k = cout_pad] holding
+// W[26 - tap][k][n].  K-major core-matrix layout, zero padding.
+__global__ void k_format_weights(const float* __restrict__ w, int cout, int cin, uint16_t* __restrict__ fwd,
+                                 uint16_t* __restrict__ bwd) {
+    const int cop = pad16(cout), cip = pad16(cin);
+    const long long per_tap = (long long)cop * cip;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= per_tap * kNetTaps) return;
+    const int tap = int(i / per_tap);
+    const int rem = int(i % per_tap);
+    {  // forward element (n, k)
+        const int n = rem / cip, k = rem % cip;
+        const float val = (n < cout && k < cin) ? w[((long long)tap * cout + n) * cin + k] : 0.f;
+        const long long off = (long long)(n / 8) * (cip / 8) * 64 + (k / 8) * 64 + (n % 8) * 8 + (k % 8);
+        fwd[tap * per_tap + off] = bf16_bits(val);
+    }
+    if (bwd) {  // backward element (n = ci, k = co)
+        const int n = rem / cop, k = rem % cop;
+        const float val = (n < cin && k < cout) ? w[((long long)(kNetTaps - 1 - tap) * cout + k) * cin + n] : 0.f;
+        const long long off = (long long)(n / 8) * (cop / 8) * 64 + (k / 8) * 64 + (n % 8) * 8 + (k % 8);
+        bwd[tap * per_tap + off] = bf16_bits(val);
+    }
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+unsigned nb(long long n, int t = 256) { return unsigned(std::max<long long>(1, (n + t - 1) / t)); }
+
+}  // namespace
+
+// ------------------------------------------------------------- host side
+LearnedNet::LearnedNet(uint64_t seed) {
+    const long long np = net_param_count();
+    std::vector<float> w(size_t(np), 0.f);
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < kNetLayers; ++l) {
+        const long long off = net_param_offset(l);
+        const int fan_in = kNetTaps * kNetCin[l];
+        const double sd = std::sqrt(2.0 / fan_in) * (l == kNetLayers - 1 ? 0.5 : 1.0);
+        std::normal_distribution<double> nd(0.0, sd);
+        const long long nw = (long long)kNetTaps * kNetCout[l] * kNetCin[l];
+        for (long long i = 0; i < nw; ++i) w[size_t(off + i)] = float(nd(rng));
+    }
+    LHI_CUDA(cudaMalloc(&w32_, sizeof(float) * np));
+    LHI_CUDA(cudaMalloc(&grad_, sizeof(float) * np));
+    LHI_CUDA(cudaMalloc(&adam_m_, sizeof(float) * np));
+    LHI_CUDA(cudaMalloc(&adam_v_, sizeof(float) * np));
+    LHI_CUDA(cudaMemcpy(w32_, w.data(), sizeof(float) * np, cudaMemcpyHostToDevice));
+    LHI_CUDA(cudaMemset(grad_, 0, sizeof(float) * np));
+    LHI_CUDA(cudaMemset(adam_m_, 0, sizeof(float) * np));
+    LHI_CUDA(cudaMemset(adam_v_, 0, sizeof(float) * np));
+    long long f = 0;
+    for (int l = 0; l < kNetLayers; ++l) {
+        wfwd_off_[l] = f;
+        wbwd_off_[l] = f;
+        f += (long long)kNetTaps * pad16(kNetCout[l]) * pad16(kNetCin[l]);
+    }
+    LHI_CUDA(cudaMalloc(&wfwd_, sizeof(uint16_t) * f));
+    LHI_CUDA(cudaMalloc(&wbwd_, sizeof(uint16_t) * f));
+    LHI_CUDA(cudaMalloc(&status_, sizeof(NetStatus)));
+    LHI_CUDA(cudaMemset(status_, 0, sizeof(NetStatus)));
+    LHI_CUDA(cudaMalloc(&scale_, sizeof(float)));
+    LHI_CUDA(cudaMalloc(&red_, sizeof(double) * 2 * 1024));
+    LHI_CUDA(cudaMalloc(&counter_, sizeof(unsigned) * 4));
+    LHI_CUDA(cudaMemset(counter_, 0, sizeof(unsigned) * 4));
+    LHI_CUDA(cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    LHI_CUDA(cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+}
+
+static void free_buffers(NetBuffers& b) {
+    auto F = [](void* p) {
+        if (p) cudaFree(p);
+    };
+    F(b.a0), F(b.h0), F(b.p0), F(b.h1), F(b.p1), F(b.h2), F(b.q1), F(b.u1), F(b.q0), F(b.u0), F(b.y), F(b.dx), F(b.acc);
+    for (int l = 0; l < kNetLayers; ++l) F(b.g[l]);
+    b = NetBuffers();
+}
+
+LearnedNet::~LearnedNet() {
+    free_buffers(b_);
+    auto F = [](void* p) {
+        if (p) cudaFree(p);
+    };
+    F(w32_), F(grad_), F(adam_m_), F(adam_v_), F(wfwd_), F(wbwd_), F(status_), F(scale_), F(red_), F(counter_);
+}
+
+void LearnedNet::set_params(const float* host) {
+    LHI_CUDA(cudaMemcpy(w32_, host, sizeof(float) * net_param_count(), cudaMemcpyHostToDevice));
+    wfmt_stale_ = true;
+}
+void LearnedNet::get_params(float* host) {
+    LHI_CUDA(cudaMemcpy(host, w32_, sizeof(float) * net_param_count(), cudaMemcpyDeviceToHost));
+}
+void LearnedNet::get_grads(float* host, cudaStream_t s) {
+    LHI_CUDA(cudaMemcpyAsync(host, grad_, sizeof(float) * net_param_count(), cudaMemcpyDeviceToHost, s));
+    LHI_CUDA(cudaStreamSynchronize(s));
+}
+void LearnedNet::zero_grad(cudaStream_t s) {
+    LHI_CUDA(cudaMemsetAsync(grad_, 0, sizeof(float) * net_param_count(), s));
+}
+int LearnedNet::check_status(cudaStream_t s) {
+    NetStatus h{};
+    LHI_CUDA(cudaMemcpyAsync(&h, status_, sizeof(h), cudaMemcpyDeviceToHost, s));
+    LHI_CUDA(cudaStreamSynchronize(s));
+    if (h.timeout) {
+        last_timeout_[0] = h.pad[0];
+        last_timeout_[1] = h.pad[1];
+        last_timeout_[2] = h.pad[2];
+    }
+    return h.timeout ? LHI_E_TIMEOUT : LHI_OK;
+}
+
+void LearnedNet::ensure(const int dims[3]) {
+    int d1[3], d2[3];
+    for (int a = 0; a < 3; ++a) {
+        d1[a] = dims[a] / 2;
+        d2[a] = d1[a] / 2;
+        if (dims[a] < 4) throw std::invalid_argument("learned preconditioner: grid below 4 cells on an axis");
+    }
+    const long long v0 = (long long)dims[0] * dims[1] * dims[2];
+    bool same = true;
+    for (int a = 0; a < 3; ++a) same = same && b_.dims[0][a] == dims[a];
+    if (same && b_.cap_vox0 == v0) return;
+    free_buffers(b_);
+    for (int a = 0; a < 3; ++a) {
+        b_.dims[0][a] = dims[a];
+        b_.dims[1][a] = d1[a];
+        b_.dims[2][a] = d2[a];
+    }
+    b_.vox[0] = v0;
+    b_.vox[1] = (long long)d1[0] * d1[1] * d1[2];
+    b_.vox[2] = (long long)d2[0] * d2[1] * d2[2];
+    b_.cap_vox0 = v0;
+    const long long V0 = b_.vox[0], V1 = std::max(1LL, b_.vox[1]), V2 = std::max(1LL, b_.vox[2]);
+    auto A16 = [](uint16_t** p, long long n) { LHI_CUDA(cudaMalloc(p, sizeof(uint16_t) * size_t(n))); };
+    A16(&b_.a0, V0 * 16);
+    A16(&b_.h0, V0 * 16);
+    A16(&b_.p0, V1 * 16);
+    A16(&b_.h1, V1 * 32);
+    A16(&b_.p1, V2 * 32);
+    A16(&b_.h2, V2 * 64);
+    A16(&b_.q1, V1 * 64);
+    A16(&b_.u1, V1 * 32);
+    A16(&b_.q0, V0 * 32);
+    A16(&b_.u0, V0 * 16);
+    LHI_CUDA(cudaMalloc(&b_.y, sizeof(float) * V0));
+    const long long gsz[kNetLayers] = {V0 * 16, V1 * 32, V2 * 64, V1 * 32, V0 * 16, V0 * 16};
+    for (int l = 0; l < kNetLayers; ++l) A16(&b_.g[l], gsz[l]);
+    LHI_CUDA(cudaMalloc(&b_.dx, sizeof(float) * std::max(V0 * 32, V1 * 64)));
+    LHI_CUDA(cudaMalloc(&b_.acc, sizeof(float) * std::max(V1 * 32, V2 * 64)));
+}
+
+void LearnedNet::format_weights(cudaStream_t s) {
+    for (int l = 0; l < kNetLayers; ++l) {
+        const long long n = (long long)kNetTaps * pad16(kNetCout[l]) * pad16(kNetCin[l]);
+        k_format_weights<<<nb(n), 256, 0, s>>>(w32_ + net_param_offset(l), kNetCout[l], kNetCin[l], wfwd_ + wfwd_off_[l],
+                                               l == 0 ? nullptr : wbwd_ + wbwd_off_[l]);
+        LHI_LAUNCH_CHECK();
+    }
+    wfmt_stale_ = false;
+}
+
+namespace {
+void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const float* bias, int cout_real,
+                 const int* d, int mode, const uint16_t* skip, int relu, uint16_t* out_b, float* out_f, NetStatus* st,
+                 cudaStream_t s) {
+    ConvParams P;
+    P.in = in;
+    P.cin = cin;
+    P.w = w;
+    P.cout = cout;
+    P.bias = bias;
+    P.cout_real = cout_real;
+    P.nx = d[0];
+    P.ny = d[1];
+    P.nz = d[2];
+    P.nvox = (long long)d[0] * d[1] * d[2];
+    P.mode = mode;
+    P.skip = skip;
+    P.relu = relu;
+    P.out_b = out_b;
+    P.out_f = out_f;
+    P.status = st;
+    if (P.nvox == 0) return;
+    const size_t smem = size_t(2) * kConvM * cin * 2 + size_t(2) * cout * cin * 2 + 32;
+    k_conv<<<unsigned((P.nvox + kConvM - 1) / kConvM), kConvM, smem, s>>>(P);
+    LHI_LAUNCH_CHECK();
+}
+
+void launch_wgrad(const uint16_t* g, int cout, int cout_real, const uint16_t* in, int cin, int cin_real, const int* d,
+                  float* grad_w, NetStatus* st, cudaStream_t s) {
+    WgradParams P;
+    P.g = g;
+    P.cout = cout;
+    P.cout_real = cout_real;
+    P.in = in;
+    P.cin = cin;
+    P.cin_real = cin_real;
+    P.nx = d[0];
+    P.ny = d[1];
+    P.nz = d[2];
+    P.nvox = (long long)d[0] * d[1] * d[2];
+    P.grad_w = grad_w;
+    P.status = st;
+    if (P.nvox == 0) return;
+    const size_t smem = size_t(2) * 128 * kWgChunk * 2 + size_t(2) * cin * kWgChunk * 2 + 32;
+    dim3 grid(unsigned((P.nvox + kWgChunk * kWgChunksPerCta - 1) / (kWgChunk * kWgChunksPerCta)), kNetTaps);
+    k_wgrad<<<grid, 128, smem, s>>>(P);
+    LHI_LAUNCH_CHECK();
+}
+}  // namespace
+
+void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type, const uint8_t* solid, float* z,
+                         double scale_fixed, cudaStream_t s) {
+    ensure(dims);
+    if (wfmt_stale_) format_weights(s);
+    last_type_ = type;
+    const int* d0 = b_.dims[0];
+    const int* d1 = b_.dims[1];
+    const int* d2 = b_.dims[2];
+    const long long V0 = b_.vox[0];
+    if (scale_fixed > 0) {
+        const float sf = float(scale_fixed);
+        LHI_CUDA(cudaMemcpyAsync(scale_, &sf, sizeof(float), cudaMemcpyHostToDevice, s));
+    } else {
+        k_net_scale<<<std::min<unsigned>(nb(V0), 1024), 256, 0, s>>>(r, type, V0, red_, counter_, scale_);
+        LHI_LAUNCH_CHECK();
+    }
+    k_net_input<<<nb(V0), 256, 0, s>>>(r, type, solid, V0, scale_, b_.a0);
+    LHI_LAUNCH_CHECK();
+    auto W = [&](int l) { return wfwd_ + wfwd_off_[l]; };
+    auto Bv = [&](int l) { return w32_ + net_param_offset(l) + (long long)kNetTaps * kNetCout[l] * kNetCin[l]; };
+    launch_conv(b_.a0, 16, W(0), 16, Bv(0), 16, d0, 0, nullptr, 1, b_.h0, nullptr, status_, s);
+    k_pool<<<nb(b_.vox[1] * 16), 256, 0, s>>>(b_.h0, d0[1], d0[2], b_.p0, d1[0], d1[1], d1[2], 16);
+    LHI_LAUNCH_CHECK();
+    launch_conv(b_.p0, 16, W(1), 32, Bv(1), 32, d1, 0, nullptr, 1, b_.h1, nullptr, status_, s);
+    k_pool<<<nb(b_.vox[2] * 32), 256, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[0], d2[1], d2[2], 32);
+    LHI_LAUNCH_CHECK();
+    launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, 1, b_.h2, nullptr, status_, s);
+    k_upsample<<<nb(b_.vox[1] * 64), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
+    LHI_LAUNCH_CHECK();
+    launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, 1, b_.u1, nullptr, status_, s);
+    k_upsample<<<nb(V0 * 32), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
+    LHI_LAUNCH_CHECK();
+    launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, 1, b_.u0, nullptr, status_, s);
+    launch_conv(b_.u0, 16, W(5), 16, Bv(5), 1, d0, 2, nullptr, 0, nullptr, b_.y, status_, s);
+    k_net_output<<<nb(V0), 256, 0, s>>>(b_.y, type, V0, scale_, z);
+    LHI_LAUNCH_CHECK();
+}
+
+void LearnedNet::backward(const float* dz, cudaStream_t s) {
+    const int* d0 = b_.dims[0];
+    const int* d1 = b_.dims[1];
+    const int* d2 = b_.dims[2];
+    const long long V0 = b_.vox[0], V1 = b_.vox[1], V2 = b_.vox[2];
+    auto WB = [&](int l) { return wbwd_ + wbwd_off_[l]; };
+    auto GW = [&](int l) { return grad_ + net_param_offset(l); };
+    auto GB = [&](int l) { return grad_ + net_param_offset(l) + (long long)kNetTaps * kNetCout[l] * kNetCin[l]; };
+    auto bias_grad = [&](const uint16_t* g, int cpad, int creal, long long nv, float* db) {
+        if (nv == 0) return;
+        k_bias_grad<<<std::min<unsigned>(nb(nv * cpad), 512), 256, 0, s>>>(g, cpad, creal, nv, db);
+        LHI_LAUNCH_CHECK();
+    };
+    // layer 5
+    k_net_dy<<<nb(V0), 256, 0, s>>>(dz, last_type_, V0, scale_, b_.g[5]);
+    LHI_LAUNCH_CHECK();
+    launch_wgrad(b_.g[5], 16, 1, b_.u0, 16, 16, d0, GW(5), status_, s);
+    bias_grad(b_.g[5], 16, 1, V0, GB(5));
+    launch_conv(b_.g[5], 16, WB(5), 16, nullptr, 16, d0, 1, nullptr, 0, nullptr, b_.dx, status_, s);
+    // layer 4
+    k_relu_grad<<<nb(V0 * 16), 256, 0, s>>>(b_.dx, b_.u0, V0 * 16, b_.g[4]);
+    LHI_LAUNCH_CHECK();
+    launch_wgrad(b_.g[4], 16, 16, b_.q0, 32, 32, d0, GW(4), status_, s);
+    bias_grad(b_.g[4], 16, 16, V0, GB(4));
+    launch_conv(b_.g[4], 16, WB(4), 32, nullptr, 32, d0, 1, nullptr, 0, nullptr, b_.dx, status_, s);
+    k_sum_children<<<nb(V1 * 32), 256, 0, s>>>(b_.dx, d0[1], d0[2], b_.acc, d1[0], d1[1], d1[2], 32);
+    LHI_LAUNCH_CHECK();
+    // layer 3
+    k_relu_grad<<<nb(V1 * 32), 256, 0, s>>>(b_.acc, b_.u1, V1 * 32, b_.g[3]);
+    LHI_LAUNCH_CHECK();
+    launch_wgrad(b_.g[3], 32, 32, b_.q1, 64, 64, d1, GW(3), status_, s);
+    bias_grad(b_.g[3], 32, 32, V1, GB(3));
+    launch_conv(b_.g[3], 32, WB(3), 64, nullptr, 64, d1, 1, nullptr, 0, nullptr, b_.dx, status_, s);
+    k_sum_children<<<nb(V2 * 64), 256, 0, s>>>(b_.dx, d1[1], d1[2], b_.acc, d2[0], d2[1], d2[2], 64);
+    LHI_LAUNCH_CHECK();
+    // layer 2
+    k_relu_grad<<<nb(V2 * 64), 256, 0, s>>>(b_.acc, b_.h2, V2 * 64, b_.g[2]);
+    LHI_LAUNCH_CHECK();
+    launch_wgrad(b_.g[2], 64, 64, b_.p1, 32, 32, d2, GW(2), status_, s);
+    bias_grad(b_.g[2], 64, 64, V2, GB(2));
+    launch_conv(b_.g[2], 64, WB(2), 32, nullptr, 32, d2, 1, nullptr, 0, nullptr, b_.dx, status_, s);
+    // layer 1: dh1 = g3 (skip) + unpool(dp1) / 8
+    k_relu_grad_unpool<<<nb(V1 * 32), 256, 0, s>>>(b_.g[3], b_.dx, d2[0], d2[1], d2[2], b_.h1, d1[0], d1[1], d1[2], 32,
+                                                    b_.g[1]);
+    LHI_LAUNCH_CHECK();
+    launch_wgrad(b_.g[1], 32, 32, b_.p0, 16, 16, d1, GW(1), status_, s);
+    bias_grad(b_.g[1], 32, 32, V1, GB(1));
+    launch_conv(b_.g[1], 32, WB(1), 16, nullptr, 16, d1, 1, nullptr, 0, nullptr, b_.dx, status_, s);
+    // layer 0: dh0 = g4 (skip) + unpool(dp0) / 8
+    k_relu_grad_unpool<<<nb(V0 * 16), 256, 0, s>>>(b_.g[4], b_.dx, d1[0], d1[1], d1[2], b_.h0, d0[0], d0[1], d0[2], 16,
+                                                    b_.g[0]);
+    LHI_LAUNCH_CHECK();
+    launch_wgrad(b_.g[0], 16, 16, b_.a0, 16, 4, d0, GW(0), status_, s);
+    bias_grad(b_.g[0], 16, 16, V0, GB(0));
+}
+
+int umma_selftest(const uint16_t* a_host, const uint16_t* b_host, int N, int K, float* d_host, int* stage) {
+    if (N < 16 || N > 64 || N % 16 || K < 16 || K > 64 || K % 16) throw std::invalid_argument("selftest: N, K in {16, 32, 48, 64}");
+    uint16_t *a = nullptr, *b = nullptr;
+    float* d = nullptr;
+    NetStatus* st = nullptr;
+    LHI_CUDA(cudaMalloc(&a, 2 * 128 * K));
+    LHI_CUDA(cudaMalloc(&b, 2 * N * K));
+    LHI_CUDA(cudaMalloc(&d, 4 * 128 * N));
+    LHI_CUDA(cudaMalloc(&st, sizeof(NetStatus)));
+    LHI_CUDA(cudaMemset(st, 0, sizeof(NetStatus)));
+    LHI_CUDA(cudaMemset(d, 0, 4 * 128 * N));
+    LHI_CUDA(cudaMemcpy(a, a_host, 2 * 128 * K, cudaMemcpyHostToDevice));
+    LHI_CUDA(cudaMemcpy(b, b_host, 2 * N * K, cudaMemcpyHostToDevice));
+    k_umma_selftest<<<1, 128>>>(a, b, N, K, d, st);
+    LHI_LAUNCH_CHECK();
+    LHI_CUDA(cudaDeviceSynchronize());
+    NetStatus h{};
+    LHI_CUDA(cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost));
+    LHI_CUDA(cudaMemcpy(d_host, d, 4 * 128 * N, cudaMemcpyDeviceToHost));
+    cudaFree(a);
+    cudaFree(b);
+    cudaFree(d);
+    cudaFree(st);
+    *stage = h.pad[3];
+    return h.timeout ? LHI_E_TIMEOUT : LHI_OK;
+}
+
+void LearnedNet::adam_step(double lr, double beta1, double beta2, double eps, cudaStream_t s) {
+    ++adam_t_;
+    const double c1 = 1.0 - std::pow(beta1, double(adam_t_));
+    const double c2 = 1.0 - std::pow(beta2, double(adam_t_));
+    const long long n = net_param_count();
+    k_adam<<<nb(n), 256, 0, s>>>(w32_, grad_, adam_m_, adam_v_, n, float(lr), float(beta1), float(beta2), float(eps),
+                                 float(c1), float(c2));
+    LHI_LAUNCH_CHECK();
+    wfmt_stale_ = true;
+}
+
+}  // namespace lhi

@@ -472,3 +472,46 @@ class Reference:
         out = np.empty_like(x)
         self.lib.ref_solver_get_ax(self.h, level, _ptr(x), _ptr(out))
         return out
+
+
+# ---------------------------------------------------------- network oracle
+def _net_lib():
+    lib = oracle_lib()
+    if not getattr(lib, "_net_ready", False):
+        lib.lho_net_num_params.restype = C.c_longlong
+        lib.lho_net_forward.argtypes = [_vp, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp]
+        lib.lho_net_backward.argtypes = [_vp, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp, _vp]
+        lib._net_ready = True
+    return lib
+
+
+def net_num_params():
+    return int(_net_lib().lho_net_num_params())
+
+
+def net_forward(params, r, type_, solid=None, scale=0.0):
+    """z = M(r) of the learned preconditioner's network (double sums, BF16
+    storage points as on the GPU); r, type_, solid are 3D arrays."""
+    lib = _net_lib()
+    dims = (C.c_int32 * 3)(*r.shape)
+    p = np.ascontiguousarray(params, np.float32)
+    rr = np.ascontiguousarray(r, np.float32)
+    tt = np.ascontiguousarray(type_, np.uint8)
+    ss = None if solid is None else np.ascontiguousarray(solid, np.uint8)
+    z = np.empty(r.shape, np.float32)
+    lib.lho_net_forward(_ptr(p), dims, _ptr(rr), _ptr(tt), _ptr(ss), float(scale), _ptr(z))
+    return z
+
+
+def net_backward(params, r, type_, solid, dz, scale=0.0):
+    """Gradient of sum(dz * M(r)) with respect to the packed parameters."""
+    lib = _net_lib()
+    dims = (C.c_int32 * 3)(*r.shape)
+    p = np.ascontiguousarray(params, np.float32)
+    rr = np.ascontiguousarray(r, np.float32)
+    tt = np.ascontiguousarray(type_, np.uint8)
+    ss = None if solid is None else np.ascontiguousarray(solid, np.uint8)
+    d = np.ascontiguousarray(dz, np.float32)
+    g = np.empty(p.size, np.float32)
+    lib.lho_net_backward(_ptr(p), dims, _ptr(rr), _ptr(tt), _ptr(ss), float(scale), _ptr(d), _ptr(g))
+    return g
