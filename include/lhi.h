@@ -60,6 +60,9 @@ extern "C" {
 #define LHI_PRECOND_NONE 0
 #define LHI_PRECOND_JACOBI 1
 #define LHI_PRECOND_MULTIGRID 2
+#define LHI_PRECOND_LEARNED 3 /* no counterpart in the reference: the network of
+                                 lhi_solver_set_network inside flexible PCG, with
+                                 the V-cycle as fallback (FP32 / MIXED handles) */
 
 /* stopping rule */
 #define LHI_TOL_ABSOLUTE 0 /* ||r|| < tol, as PressureSolver.cpp:871      */
@@ -320,6 +323,31 @@ LHI_API int lhi_net_set_params(lhi_net* net, const float* in);
    of r over cells with type != 0. */
 LHI_API int lhi_net_forward_host(lhi_net* net, const int32_t dims[3], const float* r, const uint8_t* type,
                                  const uint8_t* solid, double scale, float* z);
+/* Attaches a network to a handle created with LHI_PRECOND_LEARNED (the
+   handle does not own it; keep it alive while the handle solves).  The
+   solve applies the network as the preconditioner until an iteration
+   reduces ||r|| by less than 5% or the iteration count exceeds
+   fallback_iterations (0 = the solver's max_iterations); from then on it
+   applies the multigrid V-cycle of the handle's solver parameters.  The
+   loop is host-driven (one synchronisation per iteration). */
+LHI_API int lhi_solver_set_network(lhi_liquid* h, lhi_net* net, int32_t fallback_iterations);
+/* Iterations of the last solve that used the network, and the iteration
+   at which the fallback started (-1 if it did not). */
+LHI_API int lhi_solver_learned_stats(lhi_liquid* h, int32_t* network_iterations, int32_t* fallback_iteration);
+/* Keeps the PCG residual handed to the preconditioner at each iteration of
+   the following solves (up to max_snapshots, FP32, device memory; 0 stops
+   recording and frees them).  Recording solves run host-driven. */
+LHI_API int lhi_solver_record_residuals(lhi_liquid* h, int32_t max_snapshots);
+LHI_API int lhi_solver_num_snapshots(lhi_liquid* h, int32_t* count);
+/* Adam training of the network on the handle's recorded residuals with the
+   handle's level-0 matrix A (from its last BuildLHS): each step draws
+   `batch` snapshots r (seeded), accumulates the gradient of
+   ||A M(r) - r||^2 / ||r||^2 / batch and takes one Adam step (beta1 0.9,
+   beta2 0.999, eps 1e-8).  Returns the mean loss of the first and of the
+   last step. */
+LHI_API int lhi_net_train(lhi_net* net, lhi_liquid* h, int32_t steps, int32_t batch, double lr, uint64_t seed,
+                          double* first_loss, double* last_loss);
+
 /* Self-check of the tensor-core path: one CTA computes D = A B^T (A 128 x K,
    B N x K as BF16 bit patterns, row-major; D 128 x N float) with the same
    tcgen05 descriptors as the network; *stage reports the last step reached

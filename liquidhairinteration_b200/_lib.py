@@ -48,6 +48,12 @@ SIGNATURES = {
     "lhi_net_num_params": [C.POINTER(C.c_int64)],
     "lhi_net_get_params": [C.c_void_p, _vp],
     "lhi_net_set_params": [C.c_void_p, _vp],
+    "lhi_solver_set_network": [_h, C.c_void_p, C.c_int32],
+    "lhi_solver_learned_stats": [_h, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+    "lhi_solver_record_residuals": [_h, C.c_int32],
+    "lhi_solver_num_snapshots": [_h, C.POINTER(C.c_int32)],
+    "lhi_net_train": [C.c_void_p, _h, C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.POINTER(C.c_double),
+                      C.POINTER(C.c_double)],
     "lhi_net_tensor_core_selftest": [C.c_int32, C.c_int32, _vp, _vp, _vp, C.POINTER(C.c_int32)],
     "lhi_net_forward_host": [C.c_void_p, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp],
     "lhi_net_backward_host": [C.c_void_p, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp, _vp],

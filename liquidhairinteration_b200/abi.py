@@ -31,6 +31,7 @@ PRECISION_FP64 = 2
 PRECOND_NONE = 0
 PRECOND_JACOBI = 1
 PRECOND_MULTIGRID = 2
+PRECOND_LEARNED = 3
 
 TOL_ABSOLUTE = 0
 TOL_RELATIVE = 1

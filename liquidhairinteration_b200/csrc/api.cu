@@ -351,6 +351,47 @@ void net_upload(NetHostArgs& d, long long n, const float* r, const uint8_t* type
 }
 }  // namespace
 
+LHI_API int lhi_solver_set_network(lhi_liquid* h, lhi_net* net, int32_t fallback_iterations) {
+    NEED_HANDLE(h);
+    if (!net) return fail(LHI_E_INVALID_ARG, "null network");
+    return guarded([&]() -> int {
+        h->impl->set_network(net->impl.get(), fallback_iterations);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_solver_learned_stats(lhi_liquid* h, int32_t* network_iterations, int32_t* fallback_iteration) {
+    NEED_HANDLE(h);
+    if (!network_iterations || !fallback_iteration) return fail(LHI_E_INVALID_ARG, "null argument");
+    h->impl->learned_stats(network_iterations, fallback_iteration);
+    return LHI_OK;
+}
+
+LHI_API int lhi_solver_record_residuals(lhi_liquid* h, int32_t max_snapshots) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        h->impl->record_residuals(max_snapshots);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_solver_num_snapshots(lhi_liquid* h, int32_t* count) {
+    NEED_HANDLE(h);
+    if (!count) return fail(LHI_E_INVALID_ARG, "null argument");
+    *count = h->impl->num_snapshots();
+    return LHI_OK;
+}
+
+LHI_API int lhi_net_train(lhi_net* net, lhi_liquid* h, int32_t steps, int32_t batch, double lr, uint64_t seed,
+                          double* first_loss, double* last_loss) {
+    NEED_HANDLE(h);
+    if (!net || !first_loss || !last_loss) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->train(net->impl.get(), steps, batch, lr, seed, first_loss, last_loss);
+        return LHI_OK;
+    });
+}
+
 LHI_API int lhi_net_tensor_core_selftest(int32_t n, int32_t k, const uint16_t* a, const uint16_t* b, float* d,
                                          int32_t* stage) {
     if (!a || !b || !d || !stage) return fail(LHI_E_INVALID_ARG, "null argument");

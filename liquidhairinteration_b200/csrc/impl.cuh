@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "lhi.h"
+#include "net.cuh"
 
 namespace lhi {
 
@@ -198,6 +199,12 @@ public:
     virtual lhi_solve_stats stats() const = 0;
     virtual void get_ax(int level, const void* x, void* out) = 0;
     virtual void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) = 0;
+    virtual void set_network(LearnedNet* net, int fallback_iterations) = 0;
+    virtual void learned_stats(int32_t* net_iters, int32_t* fallback_at) = 0;
+    virtual void record_residuals(int max_snapshots) = 0;
+    virtual int num_snapshots() const = 0;
+    virtual void train(LearnedNet* net, int steps, int batch, double lr, uint64_t seed, double* first,
+                       double* last) = 0;
     virtual int field_size(int field, int level, int64_t* count, int32_t* eb) = 0;
     virtual void get_field(int field, int level, void* out) = 0;
     virtual void set_field(int field, int level, const void* in) = 0;
@@ -242,6 +249,17 @@ public:
     lhi_solve_stats stats() const override { return stats_; }
     void get_ax(int level, const void* x, void* out) override;
     void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) override;
+    void set_network(LearnedNet* net, int fallback_iterations) override;
+    void learned_stats(int32_t* net_iters, int32_t* fallback_at) override {
+        *net_iters = learned_iters_;
+        *fallback_at = fallback_at_;
+    }
+    void record_residuals(int max_snapshots) override;
+    int num_snapshots() const override { return snap_count_; }
+    void train(LearnedNet* net, int steps, int batch, double lr, uint64_t seed, double* first, double* last) override;
+    void ensure_solid_cells();
+    void ensure_net_type();
+    void record_snapshot();
     int field_size(int field, int level, int64_t* count, int32_t* eb) override;
     void get_field(int field, int level, void* out) override;
     void set_field(int field, int level, const void* in) override;
@@ -323,6 +341,22 @@ public:
     cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on
     cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body
     cudaGraphExec_t solve_exec_ = nullptr;
+    // learned preconditioner
+    LearnedNet* net_ = nullptr;
+    int fallback_iters_ = 0;
+    bool use_fallback_ = false;  // this solve switched to the V-cycle
+    int learned_iters_ = 0;
+    int fallback_at_ = -1;
+    uint8_t* solid_cell_ = nullptr;  // cell-centre solid flag (mean of the 8 node SDFs < 0)
+    bool solid_cell_fresh_ = false;
+    uint8_t* net_type_ = nullptr;    // level-0 type with skipped rows (small diagonal) as 0
+    bool net_type_fresh_ = false;
+    float* snaps_ = nullptr;         // recorded residuals [snap_cap_][ncell_]
+    int snap_cap_ = 0, snap_count_ = 0, snap_next_ = 0;
+    float* train_z_ = nullptr;
+    float* train_dz_ = nullptr;
+    float* train_e_ = nullptr;
+    double* train_red_ = nullptr;    // [0] sum e^2, [1] sum r^2, [2] loss accumulator
     T* rhs_ = nullptr;
     TX* x_ = nullptr;
     T* p_ = nullptr;

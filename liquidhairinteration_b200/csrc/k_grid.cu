@@ -303,7 +303,7 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     sp_ = sp;
     if (sp.max_iterations < 0 || sp.num_pre_smooth < 0 || sp.num_post_smooth < 0 || sp.num_final_smooth < 0)
         throw std::invalid_argument("negative solver parameter");
-    if (sp.preconditioner < LHI_PRECOND_NONE || sp.preconditioner > LHI_PRECOND_MULTIGRID)
+    if (sp.preconditioner < LHI_PRECOND_NONE || sp.preconditioner > LHI_PRECOND_LEARNED)
         throw std::invalid_argument("unknown preconditioner");
     if (sp.update_region != LHI_REGION_INTERIOR && sp.update_region != LHI_REGION_FLUID)
         throw std::invalid_argument("unknown update_region");
@@ -314,7 +314,9 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     if (sp.cg_variant != LHI_CG_REFERENCE && sp.cg_variant != LHI_CG_FLEXIBLE)
         throw std::invalid_argument("unknown cg_variant");
     nlev_ = std::max(1, sp.num_level);
-    if (sp.preconditioner != LHI_PRECOND_MULTIGRID) nlev_ = 1;
+    if (sp.preconditioner != LHI_PRECOND_MULTIGRID && sp.preconditioner != LHI_PRECOND_LEARNED) nlev_ = 1;
+    if (sp.preconditioner == LHI_PRECOND_LEARNED && precision == LHI_PRECISION_FP64)
+        throw std::invalid_argument("the learned preconditioner needs an FP32 or MIXED handle");
     if (nlev_ > kMaxLevels) throw std::invalid_argument("num_level above 10 is not supported");
 
     ncell_ = (long long)nx_ * ny_ * nz_;
@@ -444,6 +446,13 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
         F(lv_[l].tiles);
     }
     if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+    F(solid_cell_);
+    F(net_type_);
+    F(snaps_);
+    F(train_z_);
+    F(train_dz_);
+    F(train_e_);
+    F(train_red_);
     if (side_) cudaStreamDestroy(side_);
     F(rhs_);
     F(x_);
@@ -473,6 +482,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::clear() {
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::set_boundary(const BoundaryProgram& prog) {
+    solid_cell_fresh_ = false;
     G3<T> g{nx_, ny_, nz_, {min_[0], min_[1], min_[2]}, {dx_[0], dx_[1], dx_[2]}};
     k_boundary<T><<<blocks_for(nnode_, 256), 256, 0, stream_>>>(prog, g, solid_phi_);
     LHI_LAUNCH_CHECK();
@@ -483,6 +493,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::set_boundary(const Boundary
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::set_solid_phi(const void* host) {
+    solid_cell_fresh_ = false;
     LHI_CUDA(cudaMemcpyAsync(solid_phi_, host, sizeof(T) * nnode_, cudaMemcpyHostToDevice, stream_));
     for (int a = 0; a < 3; ++a) {
         k_face_fractions<T><<<blocks_for(nface_[a], 256), 256, 0, stream_>>>(solid_phi_, nx_, ny_, nz_, a, lw_[a]);

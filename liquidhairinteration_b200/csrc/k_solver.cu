@@ -24,6 +24,7 @@
 // the loop condition.  With eager = 1 the host drives the same kernels and
 // reads the stop flag after every iteration.
 #include <algorithm>
+#include <random>
 
 #include "impl.cuh"
 
@@ -888,6 +889,74 @@ template <class T> __global__ void k_expand_acoef(LevelK<T> L, T* __restrict__ o
     for (int k = 0; k < 6; ++k) out[6 * i + k] = c[k];
 }
 
+// --------------------------------------------------- learned preconditioner
+// Cell-centre solid flag: mean of the cell's 8 node SDF values < 0.
+template <class T>
+__global__ void k_solid_cells(const T* __restrict__ sp, int nx, int ny, int nz, uint8_t* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)nx * ny * nz;
+    if (i >= n) return;
+    int x, y, z;
+    decode(i, ny, nz, x, y, z);
+    const long long sy = nz + 1, sx = (long long)(ny + 1) * (nz + 1);
+    const T* b = sp + x * sx + y * sy + z;
+    const double m = double(b[0]) + b[1] + b[sy] + b[sy + 1] + b[sx] + b[sx + 1] + b[sx + sy] + b[sx + sy + 1];
+    out[i] = m < 0.0 ? 1 : 0;
+}
+
+// The network's cell classes: the level-0 type, with rows that the solver
+// skips (diagonal below EPSILON: cells cut off by solid walls) marked 0.
+template <class T>
+__global__ void k_net_type(const uint8_t* __restrict__ type, const T* __restrict__ diag, long long n,
+                           uint8_t* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = is_small(diag[i]) ? 0 : type[i];
+}
+
+// e = A z - r; sums of e^2 and r^2 over all cells
+template <class T>
+__global__ void k_loss_residual(LevelK<T> L, const float* __restrict__ z, const T* __restrict__ r, float* __restrict__ e,
+                                double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ out) {
+    double v[2] = {0.0, 0.0};
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int x, y, zz;
+        decode(i, L.ny, L.nz, x, y, zz);
+        const double ei = ax_at<double>(L, z, i, x, y, zz) - double(r[i]);
+        e[i] = float(ei);
+        v[0] += ei * ei;
+        v[1] += double(r[i]) * double(r[i]);
+    }
+    grid_sum_finish<2>(v, partials, counter, out);
+}
+
+// dz = 2 A^T e / (sum r^2 * batch); the loss sum e^2 / sum r^2 / batch is added to out[2]
+template <class T>
+__global__ void k_loss_grad(LevelK<T> L, const float* __restrict__ e, int batch, float* __restrict__ dz,
+                            double* __restrict__ red) {
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    const double rr = red[1] > 0 ? red[1] : 1.0;
+    const double scale = 2.0 / (rr * batch);
+    const long long sy = L.nz, sx = (long long)L.ny * L.nz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(i, L.ny, L.nz, x, y, z);
+        const uint8_t ti = L.type[i];
+        double acc = 0.0;
+        if (ti != 0) acc = double(L.diag[i]) * e[i];
+        if (ti == 2) {  // A(j, i) = [t_j >= 1][t_i == 2] c_ij
+            if (x + 1 < L.nx && L.type[i + sx] != 0) acc += double(L.cx[i]) * e[i + sx];
+            if (x > 0 && L.type[i - sx] != 0) acc += double(L.cx[i - sx]) * e[i - sx];
+            if (y + 1 < L.ny && L.type[i + sy] != 0) acc += double(L.cy[i]) * e[i + sy];
+            if (y > 0 && L.type[i - sy] != 0) acc += double(L.cy[i - sy]) * e[i - sy];
+            if (z + 1 < L.nz && L.type[i + 1] != 0) acc += double(L.cz[i]) * e[i + 1];
+            if (z > 0 && L.type[i - 1] != 0) acc += double(L.cz[i - 1]) * e[i - 1];
+        }
+        dz[i] = float(scale * acc);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) red[2] += red[0] / rr / batch;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- host side
@@ -961,6 +1030,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
         LHI_LAUNCH_CHECK();
     }
     build_tiles();
+    net_type_fresh_ = false;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_tiles() {
@@ -1104,6 +1174,17 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_precond() {
                                                                 L0.r, L0.z, &sc_->stop);
             LHI_LAUNCH_CHECK();
             break;
+        case LHI_PRECOND_LEARNED:
+            if (net_ && !use_fallback_) {
+                ensure_solid_cells();
+                ensure_net_type();
+                const int dims[3] = {nx_, ny_, nz_};
+                net_->forward(dims, reinterpret_cast<const float*>(L0.r), net_type_, solid_cell_,
+                              reinterpret_cast<float*>(L0.z), 0.0, cur_);
+                break;
+            }
+            enqueue_vcycle();
+            break;
         default: enqueue_vcycle();
     }
 }
@@ -1138,6 +1219,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_init(unsigned long 
         k_cg_init_r<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, L0.r);
         LHI_LAUNCH_CHECK();
     }
+    record_snapshot();
     enqueue_precond();
     {
         auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
@@ -1168,6 +1250,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_body(unsigned long 
             LHI_LAUNCH_CHECK();
         }
     }
+    record_snapshot();
     enqueue_precond();
     {
         auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
@@ -1251,14 +1334,44 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     solver_init();
     build_rhs();
     build_lhs(rho, dt);
-    if (!sp_.eager && !prof_.on) {
+    const bool learned = sp_.preconditioner == LHI_PRECOND_LEARNED;
+    if (learned && !net_) throw std::invalid_argument("LHI_PRECOND_LEARNED without a network (lhi_solver_set_network)");
+    use_fallback_ = false;
+    learned_iters_ = 0;
+    fallback_at_ = -1;
+    if (!sp_.eager && !prof_.on && !learned && snap_cap_ == 0) {
         if (!solve_exec_) build_solve_graph();
         LHI_CUDA(cudaGraphLaunch(solve_exec_, stream_));
     } else {
+        // host-driven loop; with the learned preconditioner the host also
+        // applies the fallback rule between iterations
+        const int cap = fallback_iters_ > 0 ? fallback_iters_ : sp_.max_iterations;
         enqueue_init(0, 0);
+        if (learned) {
+            learned_iters_ = 1;
+            read_scalars();
+            if (!(sc_host_->rz_old > 0.0) && !sc_host_->stop) {
+                // r.M(r) <= 0: the network gives no descent direction; start over with the V-cycle
+                use_fallback_ = true;
+                fallback_at_ = 0;
+                learned_iters_ = 0;
+                enqueue_init(0, 0);
+            }
+        }
+        double prev = -1.0;
         for (;;) {
             read_scalars();
             if (sc_host_->stop) break;
+            if (learned && !use_fallback_) {
+                const double res = sc_host_->residual;
+                const bool slow = prev > 0 && res > 0.95 * prev;
+                if (slow || sc_host_->iter >= cap) {
+                    use_fallback_ = true;
+                    fallback_at_ = sc_host_->iter;
+                }
+                prev = res;
+            }
+            if (learned && !use_fallback_) ++learned_iters_;
             enqueue_body(0, 0);
         }
         enqueue_final();
@@ -1305,6 +1418,99 @@ void LiquidImpl<T, TX>::active_tiles(int level, int32_t* active, int32_t* total,
     *active = sc_host_->tile_count[level];
     *total = lv_[level].ntiles;
     *coarse = (level >= coarse_level_) ? 1 : 0;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::set_network(LearnedNet* net, int fallback_iterations) {
+    if (sp_.preconditioner != LHI_PRECOND_LEARNED)
+        throw std::invalid_argument("lhi_solver_set_network needs a handle created with LHI_PRECOND_LEARNED");
+    if (fallback_iterations < 0) throw std::invalid_argument("fallback_iterations must be >= 0");
+    net_ = net;
+    fallback_iters_ = fallback_iterations;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::ensure_solid_cells() {
+    if (!solid_cell_) LHI_CUDA(cudaMalloc(&solid_cell_, size_t(ncell_)));
+    if (solid_cell_fresh_) return;
+    k_solid_cells<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(solid_phi_, nx_, ny_, nz_, solid_cell_);
+    LHI_LAUNCH_CHECK();
+    solid_cell_fresh_ = true;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::ensure_net_type() {
+    if (!net_type_) LHI_CUDA(cudaMalloc(&net_type_, size_t(ncell_)));
+    if (net_type_fresh_) return;
+    k_net_type<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(lv_[0].type, lv_[0].diag, ncell_, net_type_);
+    LHI_LAUNCH_CHECK();
+    net_type_fresh_ = true;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::record_residuals(int max_snapshots) {
+    if (max_snapshots < 0 || max_snapshots > 100000) throw std::invalid_argument("max_snapshots out of range");
+    if (snaps_) cudaFree(snaps_);
+    snaps_ = nullptr;
+    snap_cap_ = max_snapshots;
+    snap_count_ = snap_next_ = 0;
+    if (max_snapshots > 0) LHI_CUDA(cudaMalloc(&snaps_, sizeof(float) * size_t(ncell_) * size_t(max_snapshots)));
+}
+
+// Copy of level-0 r (as FP32) into the next snapshot slot (ring buffer).
+template <class T, class TX> void LiquidImpl<T, TX>::record_snapshot() {
+    if (snap_cap_ == 0) return;
+    float* dst = snaps_ + size_t(snap_next_) * size_t(ncell_);
+    if (sizeof(T) == sizeof(float)) {
+        LHI_CUDA(cudaMemcpyAsync(dst, lv_[0].r, sizeof(float) * ncell_, cudaMemcpyDeviceToDevice, cur_));
+    } else {
+        throw std::invalid_argument("residual recording needs an FP32 or MIXED handle");
+    }
+    snap_next_ = (snap_next_ + 1) % snap_cap_;
+    snap_count_ = std::min(snap_count_ + 1, snap_cap_);
+}
+
+template <class T, class TX>
+void LiquidImpl<T, TX>::train(LearnedNet* net, int steps, int batch, double lr, uint64_t seed, double* first,
+                              double* last) {
+    if (sizeof(T) != sizeof(float)) throw std::invalid_argument("training needs an FP32 or MIXED handle");
+    if (snap_count_ == 0) throw std::invalid_argument("no recorded residuals (lhi_solver_record_residuals + solve)");
+    if (steps < 1 || batch < 1) throw std::invalid_argument("steps and batch must be >= 1");
+    if (!train_z_) {
+        LHI_CUDA(cudaMalloc(&train_z_, sizeof(float) * ncell_));
+        LHI_CUDA(cudaMalloc(&train_dz_, sizeof(float) * ncell_));
+        LHI_CUDA(cudaMalloc(&train_e_, sizeof(float) * ncell_));
+        LHI_CUDA(cudaMalloc(&train_red_, sizeof(double) * 4));
+    }
+    ensure_solid_cells();
+    ensure_net_type();
+    LevelDev<T>& L0 = lv_[0];
+    const int dims[3] = {nx_, ny_, nz_};
+    const unsigned nbk = std::min<unsigned>(blocks_for(ncell_, 256), unsigned(sum_blocks_));
+    std::mt19937_64 rng(seed);
+    double first_loss = 0.0, last_loss = 0.0;
+    for (int st = 0; st < steps; ++st) {
+        net->zero_grad(cur_);
+        LHI_CUDA(cudaMemsetAsync(train_red_ + 2, 0, sizeof(double), cur_));
+        for (int b = 0; b < batch; ++b) {
+            const int k = int(rng() % uint64_t(snap_count_));
+            const float* r = snaps_ + size_t(k) * size_t(ncell_);
+            net->forward(dims, r, net_type_, solid_cell_, train_z_, 0.0, cur_);
+            k_loss_residual<T><<<nbk, 256, 0, cur_>>>(lk(L0), train_z_, reinterpret_cast<const T*>(r), train_e_,
+                                                      partials_, counter_, train_red_);
+            LHI_LAUNCH_CHECK();
+            k_loss_grad<T><<<nbk, 256, 0, cur_>>>(lk(L0), train_e_, batch, train_dz_, train_red_);
+            LHI_LAUNCH_CHECK();
+            net->backward(train_dz_, cur_);
+        }
+        net->adam_step(lr, 0.9, 0.999, 1e-8, cur_);
+        if (st == 0 || st == steps - 1) {
+            double loss = 0.0;
+            LHI_CUDA(cudaMemcpyAsync(&loss, train_red_ + 2, sizeof(double), cudaMemcpyDeviceToHost, cur_));
+            LHI_CUDA(cudaStreamSynchronize(cur_));
+            if (st == 0) first_loss = loss;
+            last_loss = loss;
+        }
+    }
+    if (net->check_status(cur_) != LHI_OK) throw CudaError(cudaErrorLaunchTimeout, "tensor-core pipeline wait timed out");
+    *first = first_loss;
+    *last = last_loss;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::get_acoef(int level, T* host_out) {

@@ -34,7 +34,8 @@ class SolverParameter:
     toleranceMode ("absolute" | "relative"), cgVariant ("reference" |
     "flexible") and trueResidualEvery (int)."""
 
-    _PRE = {"None": abi.PRECOND_NONE, "Jacobi": abi.PRECOND_JACOBI, "Multigrid": abi.PRECOND_MULTIGRID}
+    _PRE = {"None": abi.PRECOND_NONE, "Jacobi": abi.PRECOND_JACOBI, "Multigrid": abi.PRECOND_MULTIGRID,
+            "Learned": abi.PRECOND_LEARNED}
 
     def __init__(self, cfg):
         s = cfg["SolverParameter"]
@@ -258,6 +259,27 @@ class CGSolver:
         out = np.empty_like(x)
         call("lhi_solver_get_ax", self._m._h, int(level), _ptr(x), _ptr(out))
         return out
+
+    def SetNetwork(self, net, fallbackIterations=0):
+        """The learned preconditioner's network (handle created with
+        preconditionerType "Learned"); the handle keeps a reference."""
+        call("lhi_solver_set_network", self._m._h, net._h, int(fallbackIterations))
+        self._net = net
+
+    def LearnedStats(self):
+        """(iterations that used the network, iteration where the V-cycle
+        fallback started or -1) of the last solve."""
+        a, b = C.c_int32(), C.c_int32()
+        call("lhi_solver_learned_stats", self._m._h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def RecordResiduals(self, maxSnapshots):
+        call("lhi_solver_record_residuals", self._m._h, int(maxSnapshots))
+
+    def NumSnapshots(self):
+        n = C.c_int32()
+        call("lhi_solver_num_snapshots", self._m._h, C.byref(n))
+        return n.value
 
     def ActiveTiles(self, level=0):
         """(active tiles, total tiles, solved by the coarse CTA) of a level."""

@@ -87,3 +87,12 @@ class LearnedNet:
         call("lhi_net_backward_host", self._h, (C.c_int32 * 3)(*rr.shape), _p(rr), _p(tt), _p(ss), float(scale),
              _p(d), _p(g))
         return g
+
+    def train(self, model, steps, batch=16, lr=1e-3, seed=0):
+        """Adam steps on the residuals ``model`` recorded (its solver's
+        RecordResiduals + Solve) with its level-0 matrix; returns the mean
+        loss ||A M(r) - r||^2 / ||r||^2 of the first and the last step."""
+        a, b = C.c_double(), C.c_double()
+        call("lhi_net_train", self._h, model._h, int(steps), int(batch), float(lr), int(seed), C.byref(a), C.byref(b))
+        return a.value, b.value
+
