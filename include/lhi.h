@@ -316,7 +316,14 @@ LHI_API int lhi_net_create(uint64_t seed, lhi_net** out);
 LHI_API int lhi_net_destroy(lhi_net* net);
 LHI_API int lhi_net_num_params(int64_t* count);
 LHI_API int lhi_net_get_params(lhi_net* net, float* out);
+/* Parameters to / from a file: 8-byte tag "LHINET01", int64 count, then the
+   packed FP32 parameters (little-endian). */
+LHI_API int lhi_net_save(lhi_net* net, const char* path);
+LHI_API int lhi_net_load(lhi_net* net, const char* path);
 LHI_API int lhi_net_set_params(lhi_net* net, const float* in);
+/* Activation between layers: 0 = identity (default: a linear multilevel
+   operator, a fixed preconditioner for each geometry), 1 = ReLU. */
+LHI_API int lhi_net_set_relu(lhi_net* net, int32_t relu);
 /* z = M(r) on an n0 x n1 x n2 grid from host buffers: r (float per cell),
    type (uint8 per cell: 0 phi > 0, 1 phi == 0, 2 phi < 0), solid (uint8
    per cell, 1 = solid cell, may be NULL); scale > 0 fixes s, 0 uses the RMS
@@ -328,7 +335,8 @@ LHI_API int lhi_net_forward_host(lhi_net* net, const int32_t dims[3], const floa
    solve applies the network as the preconditioner until an iteration
    reduces ||r|| by less than 5% or the iteration count exceeds
    fallback_iterations (0 = the solver's max_iterations); from then on it
-   applies the multigrid V-cycle of the handle's solver parameters.  The
+   applies the multigrid V-cycle of the handle's solver parameters.
+   fallback_iterations = -1 turns the fallback off (network only).  The
    loop is host-driven (one synchronisation per iteration). */
 LHI_API int lhi_solver_set_network(lhi_liquid* h, lhi_net* net, int32_t fallback_iterations);
 /* Iterations of the last solve that used the network, and the iteration

@@ -1,8 +1,10 @@
 // api.cu -- the C-ABI of include/lhi.h: argument checking, error reporting
 // (thread-local last error, int status codes) and dispatch to the handle's
 // precision-specific implementation.  No exception crosses the boundary.
+#include <cstdio>
 #include <cstring>
 #include <memory>
+#include <vector>
 #include <new>
 #include <string>
 
@@ -302,6 +304,46 @@ LHI_API int lhi_net_get_params(lhi_net* net, float* out) {
     if (!net || !out) return fail(LHI_E_INVALID_ARG, "null argument");
     return guarded([&]() -> int {
         net->impl->get_params(out);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_net_set_relu(lhi_net* net, int32_t relu) {
+    if (!net) return fail(LHI_E_INVALID_ARG, "null argument");
+    net->impl->relu_ = relu != 0;
+    return LHI_OK;
+}
+
+LHI_API int lhi_net_save(lhi_net* net, const char* path) {
+    if (!net || !path) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        const long long n = lhi::net_param_count();
+        std::vector<float> p(static_cast<size_t>(n));
+        net->impl->get_params(p.data());
+        FILE* f = std::fopen(path, "wb");
+        if (!f) return fail(LHI_E_INVALID_ARG, std::string("cannot open ") + path);
+        const int64_t cnt = n;
+        bool ok = std::fwrite("LHINET01", 1, 8, f) == 8 && std::fwrite(&cnt, 8, 1, f) == 1 &&
+                  std::fwrite(p.data(), 4, size_t(n), f) == size_t(n);
+        ok = (std::fclose(f) == 0) && ok;
+        return ok ? LHI_OK : fail(LHI_E_INVALID_ARG, std::string("write failed: ") + path);
+    });
+}
+
+LHI_API int lhi_net_load(lhi_net* net, const char* path) {
+    if (!net || !path) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        FILE* f = std::fopen(path, "rb");
+        if (!f) return fail(LHI_E_INVALID_ARG, std::string("cannot open ") + path);
+        char tag[8];
+        int64_t cnt = 0;
+        const long long n = lhi::net_param_count();
+        std::vector<float> p(static_cast<size_t>(n));
+        bool ok = std::fread(tag, 1, 8, f) == 8 && std::memcmp(tag, "LHINET01", 8) == 0 && std::fread(&cnt, 8, 1, f) == 1 &&
+                  cnt == n && std::fread(p.data(), 4, size_t(n), f) == size_t(n);
+        std::fclose(f);
+        if (!ok) return fail(LHI_E_INVALID_ARG, std::string("not a network parameter file of this layout: ") + path);
+        net->impl->set_params(p.data());
         return LHI_OK;
     });
 }

@@ -477,18 +477,40 @@ __global__ void k_net_scale(const float* __restrict__ r, const uint8_t* __restri
     *scale = float(s);
 }
 
+// Input channels, all linear in r so that M(a r) = a M(r) for a > 0 and
+// M(0) = 0: [r/s, r/s on cells next to air, r/s on cells next to a solid
+// (or the domain edge), 0], on cells with type != 0.
 __global__ void k_net_input(const float* __restrict__ r, const uint8_t* __restrict__ type,
-                            const uint8_t* __restrict__ solid, long long n, const float* __restrict__ scale,
+                            const uint8_t* __restrict__ solid, int nx, int ny, int nz, const float* __restrict__ scale,
                             uint16_t* __restrict__ a0) {
+    const long long n = (long long)nx * ny * nz;
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     const bool fl = type[v] != 0;
-    const bool so = !fl && solid && solid[v];
+    bool air = false, sol = false;
+    if (fl) {
+        int x, y, z;
+        z = int(v % nz);
+        const long long t = v / nz;
+        y = int(t % ny);
+        x = int(t / ny);
+        const int dx[6] = {1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, 1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, 1, -1};
+        for (int k = 0; k < 6; ++k) {
+            const int xx = x + dx[k], yy = y + dy[k], zz = z + dz[k];
+            if (xx < 0 || xx >= nx || yy < 0 || yy >= ny || zz < 0 || zz >= nz) {
+                sol = true;
+                continue;
+            }
+            const long long u = ((long long)xx * ny + yy) * nz + zz;
+            if (solid && solid[u]) sol = true;
+            else if (type[u] == 0) air = true;
+        }
+    }
+    const float rh = fl ? r[v] / *scale : 0.f;
     uint16_t o[16] = {};
-    o[0] = bf16_bits(fl ? r[v] / *scale : 0.f);
-    o[1] = bf16_bits(fl ? 1.f : 0.f);
-    o[2] = bf16_bits(so ? 1.f : 0.f);
-    o[3] = bf16_bits((!fl && !so) ? 1.f : 0.f);
+    o[0] = bf16_bits(rh);
+    o[1] = bf16_bits(air ? rh : 0.f);
+    o[2] = bf16_bits(sol ? rh : 0.f);
     uint4* dst = reinterpret_cast<uint4*>(a0 + v * 16);
     dst[0] = reinterpret_cast<uint4*>(o)[0];
     dst[1] = reinterpret_cast<uint4*>(o)[1];
@@ -546,18 +568,18 @@ __global__ void k_sum_children(const float* __restrict__ fine, int fny, int fnz,
     coarse[i] = acc;
 }
 
-// g = bf16(d * relu'(u))
-__global__ void k_relu_grad(const float* __restrict__ d, const uint16_t* __restrict__ u, long long n,
+// g = bf16(d * relu'(u)), or bf16(d) for the linear network
+__global__ void k_relu_grad(const float* __restrict__ d, const uint16_t* __restrict__ u, long long n, int relu,
                             uint16_t* __restrict__ g) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    g[i] = bf16_bits(bf16_float(u[i]) > 0.f ? d[i] : 0.f);
+    g[i] = bf16_bits((!relu || bf16_float(u[i]) > 0.f) ? d[i] : 0.f);
 }
 
 // g = bf16((skip + 0.125 * dcoarse[parent]) * relu'(u)) at a fine level
 __global__ void k_relu_grad_unpool(const uint16_t* __restrict__ skip, const float* __restrict__ dcoarse, int cnx, int cny,
                                    int cnz, const uint16_t* __restrict__ u, int fnx, int fny, int fnz, int C,
-                                   uint16_t* __restrict__ g) {
+                                   int relu, uint16_t* __restrict__ g) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long n = (long long)fnx * fny * fnz * C;
     if (i >= n) return;
@@ -568,7 +590,7 @@ __global__ void k_relu_grad_unpool(const uint16_t* __restrict__ skip, const floa
     const int px = x >> 1, py = y >> 1, pz = z >> 1;
     float d = bf16_float(skip[i]);
     if (px < cnx && py < cny && pz < cnz) d += 0.125f * dcoarse[(((long long)px * cny + py) * cnz + pz) * C + c];
-    g[i] = bf16_bits(bf16_float(u[i]) > 0.f ? d : 0.f);
+    g[i] = bf16_bits((!relu || bf16_float(u[i]) > 0.f) ? d : 0.f);
 }
 
 // z = s * y on fluid cells
@@ -830,23 +852,28 @@ void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type,
         k_net_scale<<<std::min<unsigned>(nb(V0), 1024), 256, 0, s>>>(r, type, V0, red_, counter_, scale_);
         LHI_LAUNCH_CHECK();
     }
-    k_net_input<<<nb(V0), 256, 0, s>>>(r, type, solid, V0, scale_, b_.a0);
+    k_net_input<<<nb(V0), 256, 0, s>>>(r, type, solid, d0[0], d0[1], d0[2], scale_, b_.a0);
     LHI_LAUNCH_CHECK();
     auto W = [&](int l) { return wfwd_ + wfwd_off_[l]; };
-    auto Bv = [&](int l) { return w32_ + net_param_offset(l) + (long long)kNetTaps * kNetCout[l] * kNetCin[l]; };
-    launch_conv(b_.a0, 16, W(0), 16, Bv(0), 16, d0, 0, nullptr, 1, b_.h0, nullptr, status_, s);
+    // bias-free: M(0) = 0 (the packed bias entries are kept and ignored)
+    auto Bv = [&](int l) -> const float* {
+        (void)l;
+        return nullptr;
+    };
+    const int act = relu_ ? 1 : 0;
+    launch_conv(b_.a0, 16, W(0), 16, Bv(0), 16, d0, 0, nullptr, act, b_.h0, nullptr, status_, s);
     k_pool<<<nb(b_.vox[1] * 16), 256, 0, s>>>(b_.h0, d0[1], d0[2], b_.p0, d1[0], d1[1], d1[2], 16);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.p0, 16, W(1), 32, Bv(1), 32, d1, 0, nullptr, 1, b_.h1, nullptr, status_, s);
+    launch_conv(b_.p0, 16, W(1), 32, Bv(1), 32, d1, 0, nullptr, act, b_.h1, nullptr, status_, s);
     k_pool<<<nb(b_.vox[2] * 32), 256, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[0], d2[1], d2[2], 32);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, 1, b_.h2, nullptr, status_, s);
+    launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, act, b_.h2, nullptr, status_, s);
     k_upsample<<<nb(b_.vox[1] * 64), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, 1, b_.u1, nullptr, status_, s);
+    launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, act, b_.u1, nullptr, status_, s);
     k_upsample<<<nb(V0 * 32), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, 1, b_.u0, nullptr, status_, s);
+    launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, act, b_.u0, nullptr, status_, s);
     launch_conv(b_.u0, 16, W(5), 16, Bv(5), 1, d0, 2, nullptr, 0, nullptr, b_.y, status_, s);
     k_net_output<<<nb(V0), 256, 0, s>>>(b_.y, type, V0, scale_, z);
     LHI_LAUNCH_CHECK();
@@ -861,6 +888,8 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     auto GW = [&](int l) { return grad_ + net_param_offset(l); };
     auto GB = [&](int l) { return grad_ + net_param_offset(l) + (long long)kNetTaps * kNetCout[l] * kNetCin[l]; };
     auto bias_grad = [&](const uint16_t* g, int cpad, int creal, long long nv, float* db) {
+        (void)g, (void)cpad, (void)creal, (void)db;
+        return;  // bias-free network: the bias entries keep zero gradient
         if (nv == 0) return;
         k_bias_grad<<<std::min<unsigned>(nb(nv * cpad), 512), 256, 0, s>>>(g, cpad, creal, nv, db);
         LHI_LAUNCH_CHECK();
@@ -872,7 +901,7 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     bias_grad(b_.g[5], 16, 1, V0, GB(5));
     launch_conv(b_.g[5], 16, WB(5), 16, nullptr, 16, d0, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     // layer 4
-    k_relu_grad<<<nb(V0 * 16), 256, 0, s>>>(b_.dx, b_.u0, V0 * 16, b_.g[4]);
+    k_relu_grad<<<nb(V0 * 16), 256, 0, s>>>(b_.dx, b_.u0, V0 * 16, relu_ ? 1 : 0, b_.g[4]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[4], 16, 16, b_.q0, 32, 32, d0, GW(4), status_, s);
     bias_grad(b_.g[4], 16, 16, V0, GB(4));
@@ -880,7 +909,7 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     k_sum_children<<<nb(V1 * 32), 256, 0, s>>>(b_.dx, d0[1], d0[2], b_.acc, d1[0], d1[1], d1[2], 32);
     LHI_LAUNCH_CHECK();
     // layer 3
-    k_relu_grad<<<nb(V1 * 32), 256, 0, s>>>(b_.acc, b_.u1, V1 * 32, b_.g[3]);
+    k_relu_grad<<<nb(V1 * 32), 256, 0, s>>>(b_.acc, b_.u1, V1 * 32, relu_ ? 1 : 0, b_.g[3]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[3], 32, 32, b_.q1, 64, 64, d1, GW(3), status_, s);
     bias_grad(b_.g[3], 32, 32, V1, GB(3));
@@ -888,21 +917,21 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     k_sum_children<<<nb(V2 * 64), 256, 0, s>>>(b_.dx, d1[1], d1[2], b_.acc, d2[0], d2[1], d2[2], 64);
     LHI_LAUNCH_CHECK();
     // layer 2
-    k_relu_grad<<<nb(V2 * 64), 256, 0, s>>>(b_.acc, b_.h2, V2 * 64, b_.g[2]);
+    k_relu_grad<<<nb(V2 * 64), 256, 0, s>>>(b_.acc, b_.h2, V2 * 64, relu_ ? 1 : 0, b_.g[2]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[2], 64, 64, b_.p1, 32, 32, d2, GW(2), status_, s);
     bias_grad(b_.g[2], 64, 64, V2, GB(2));
     launch_conv(b_.g[2], 64, WB(2), 32, nullptr, 32, d2, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     // layer 1: dh1 = g3 (skip) + unpool(dp1) / 8
     k_relu_grad_unpool<<<nb(V1 * 32), 256, 0, s>>>(b_.g[3], b_.dx, d2[0], d2[1], d2[2], b_.h1, d1[0], d1[1], d1[2], 32,
-                                                    b_.g[1]);
+                                                    relu_ ? 1 : 0, b_.g[1]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[1], 32, 32, b_.p0, 16, 16, d1, GW(1), status_, s);
     bias_grad(b_.g[1], 32, 32, V1, GB(1));
     launch_conv(b_.g[1], 32, WB(1), 16, nullptr, 16, d1, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     // layer 0: dh0 = g4 (skip) + unpool(dp0) / 8
     k_relu_grad_unpool<<<nb(V0 * 16), 256, 0, s>>>(b_.g[4], b_.dx, d1[0], d1[1], d1[2], b_.h0, d0[0], d0[1], d0[2], 16,
-                                                    b_.g[0]);
+                                                    relu_ ? 1 : 0, b_.g[0]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[0], 16, 16, b_.a0, 16, 4, d0, GW(0), status_, s);
     bias_grad(b_.g[0], 16, 16, V0, GB(0));

@@ -700,7 +700,9 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK t
     sc->threshold = cf.rel ? double(T(t * T(r0))) : double(t);
     sc->iter = 0;
     sc->true_now = 0;
-    const bool conv = r0 < sc->threshold;
+    // a zero right-hand side is solved by x = 0 (under the relative rule the
+    // threshold is then 0 as well, and r0 < threshold never holds)
+    const bool conv = r0 < sc->threshold || r0 == 0.0;
     const bool stop = conv || cf.maxit <= 0;
     sc->status = conv ? LHI_OK : LHI_E_NOT_CONVERGED;
     sc->stop = stop ? 1 : 0;
@@ -1345,12 +1347,13 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     } else {
         // host-driven loop; with the learned preconditioner the host also
         // applies the fallback rule between iterations
+        const bool no_fallback = fallback_iters_ < 0;
         const int cap = fallback_iters_ > 0 ? fallback_iters_ : sp_.max_iterations;
         enqueue_init(0, 0);
         if (learned) {
             learned_iters_ = 1;
             read_scalars();
-            if (!(sc_host_->rz_old > 0.0) && !sc_host_->stop) {
+            if (!no_fallback && !(sc_host_->rz_old > 0.0) && !sc_host_->stop) {
                 // r.M(r) <= 0: the network gives no descent direction; start over with the V-cycle
                 use_fallback_ = true;
                 fallback_at_ = 0;
@@ -1362,7 +1365,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
         for (;;) {
             read_scalars();
             if (sc_host_->stop) break;
-            if (learned && !use_fallback_) {
+            if (learned && !use_fallback_ && !no_fallback) {
                 const double res = sc_host_->residual;
                 const bool slow = prev > 0 && res > 0.95 * prev;
                 if (slow || sc_host_->iter >= cap) {
@@ -1423,7 +1426,7 @@ void LiquidImpl<T, TX>::active_tiles(int level, int32_t* active, int32_t* total,
 template <class T, class TX> void LiquidImpl<T, TX>::set_network(LearnedNet* net, int fallback_iterations) {
     if (sp_.preconditioner != LHI_PRECOND_LEARNED)
         throw std::invalid_argument("lhi_solver_set_network needs a handle created with LHI_PRECOND_LEARNED");
-    if (fallback_iterations < 0) throw std::invalid_argument("fallback_iterations must be >= 0");
+    if (fallback_iterations < -1) throw std::invalid_argument("fallback_iterations must be >= -1");
     net_ = net;
     fallback_iters_ = fallback_iterations;
 }

@@ -1,15 +1,22 @@
 // net.cuh -- the learned preconditioner: a small multilevel 3D convolutional
 // network M(r, masks) -> search direction, used inside flexible PCG.
 //
-// Network (3 levels, 3x3x3 convolutions, zero padding, ~140k parameters):
-//   a0 = [r / s, fluid, solid, air]            4 channels (stored as 16)  N
-//   h0 = relu(conv0(a0))                       16                         N
-//   h1 = relu(conv1(avgpool(h0)))              32                         N/2
-//   h2 = relu(conv2(avgpool(h1)))              64                         N/4
-//   u1 = relu(conv3(upsample(h2)) + h1)        32                         N/2
-//   u0 = relu(conv4(upsample(u1)) + h0)        16                         N
+// Network (3 levels, 3x3x3 convolutions, zero padding, no biases, ~140k
+// weights):
+//   a0 = r/s x [1, next to air, next to solid, 0]   4 channels (stored as 16)  N
+//   h0 = act(conv0(a0))                        16                         N
+//   h1 = act(conv1(avgpool(h0)))               32                         N/2
+//   h2 = act(conv2(avgpool(h1)))               64                         N/4
+//   u1 = act(conv3(upsample(h2)) + h1)         32                         N/2
+//   u0 = act(conv4(upsample(u1)) + h0)         16                         N
+// act is the identity by default (a linear multilevel operator: a fixed
+// preconditioner for a given geometry, which flexible CG needs to keep its
+// conjugate directions) or ReLU (lhi_net_set_relu).
 //   z  = s * conv5(u0)  on fluid cells          1                         N
-// s = RMS of r over fluid cells, so M(a r) = a M(r).  Activations are BF16
+// s = RMS of r over fluid cells.  The fluid / air / solid masks enter
+// multiplied by r and nothing is added, so M(a r) = a M(r) for a > 0 and
+// M(0) = 0: a constant offset in z would stall the conjugate directions.
+// The packed layout keeps a bias vector per layer; it is ignored.  Activations are BF16
 // channels-last (voxel-major, channels contiguous, padded to 16); every
 // convolution accumulates in FP32.  Parameters are FP32 master copies with
 // BF16 working copies for the tensor cores.
@@ -123,6 +130,7 @@ public:
     long long wfwd_off_[kNetLayers] = {};
     long long wbwd_off_[kNetLayers] = {};
     bool wfmt_stale_ = true;
+    bool relu_ = false;         // activation between layers: ReLU, or none (a linear network)
     NetBuffers b_;
     const uint8_t* last_type_ = nullptr;  // cell types of the last forward (device)
     NetStatus* status_ = nullptr;

@@ -70,6 +70,16 @@ class LearnedNet:
             raise ValueError(f"expected {num_params()} parameters, got {a.size}")
         call("lhi_net_set_params", self._h, _p(a))
 
+    def set_relu(self, on):
+        """ReLU between layers (default off: a linear multilevel operator)."""
+        call("lhi_net_set_relu", self._h, 1 if on else 0)
+
+    def save(self, path):
+        call("lhi_net_save", self._h, str(path).encode())
+
+    def load(self, path):
+        call("lhi_net_load", self._h, str(path).encode())
+
     def forward(self, r, type_, solid=None, scale=0.0):
         rr = np.ascontiguousarray(r, np.float32)
         tt = np.ascontiguousarray(type_, np.uint8)

@@ -13,6 +13,10 @@ lhi_scene_seed_particles, zero (or per-primitive) initial velocity, gravity
             [0.55,0.65]x[0,0.3]x[0.2,0.4] and [0.55,0.65]x[0,0.3]x[0.6,0.8],
             seed 3, dt 1/960, 100 steps
   damN    : any N with dam64's layout (small parity cases)
+  batch   : random_scene(): the batched form's scenes -- grid size from
+            {32, 48, 64, 96}, 1-4 fluid primitives (axis boxes with sides
+            U[0.15, 0.5], spheres with radius U[0.1, 0.25], centres inside
+            the walls), 0-3 solid boxes covering 5-15% of the volume
 """
 from dataclasses import dataclass, field
 
@@ -135,6 +139,41 @@ def dam256():
         prims=[{"kind": abi.FLUID_BOX, "a": (0.0, 0.0, 0.0), "b": (0.35, 0.7, 1.0)}],
         seed=3, dt=1.0 / 960.0, steps=100,
         solver=dict(num_level=5, num_pre_smooth=2, num_post_smooth=2))
+
+
+def random_scene(rng, n=None, sizes=(32, 48, 64, 96), steps=100, dt=1.0 / 480.0, seed=None):
+    """One scene of the batched form, drawn from ``rng`` (numpy Generator)."""
+    n = int(n if n is not None else rng.choice(sizes))
+    lo, hi = 1.5 / n, 1.0 - 1.5 / n
+    prims = []
+    for _ in range(int(rng.integers(1, 5))):
+        if rng.uniform() < 0.5:
+            side = rng.uniform(0.15, 0.5, size=3)
+            c = rng.uniform(lo + side / 2, hi - side / 2)
+            prims.append({"kind": abi.FLUID_BOX, "a": tuple(c - side / 2), "b": tuple(c + side / 2)})
+        else:
+            rad = rng.uniform(0.1, 0.25)
+            c = rng.uniform(lo + rad, hi - rad, size=3)
+            prims.append({"kind": abi.FLUID_SPHERE, "a": tuple(c), "b": (rad, 0.0, 0.0)})
+    nsolid = int(rng.integers(0, 4))
+    boxes = []
+    if nsolid:
+        frac = rng.uniform(0.05, 0.15) / nsolid
+        for _ in range(nsolid):
+            aspect = rng.uniform(0.5, 2.0, size=3)
+            side = np.clip(aspect * frac ** (1.0 / 3.0) / np.prod(aspect) ** (1.0 / 3.0), 0.05, 0.8)
+            c = rng.uniform(lo + side / 2, hi - side / 2)
+            boxes.append(box(tuple(c - side / 2), tuple(c + side / 2)))
+    # union tree: node 0 = walls U solids
+    boundary = [{"kind": abi.BOUNDARY_NONE, "left": 1}, walls(n)]
+    for b in boxes:
+        root = dict(boundary[0])
+        boundary[0] = {"kind": abi.BOUNDARY_UNION, "left": len(boundary), "right": len(boundary) + 1}
+        boundary.append(root if root["kind"] != abi.BOUNDARY_NONE else walls(n))
+        boundary.append(b)
+    return SceneSpec(name=f"batch{n}", n=n, boundary=boundary, prims=prims,
+                     seed=int(seed if seed is not None else rng.integers(0, 2 ** 31)), dt=dt, steps=steps,
+                     solver=dict(num_level=4 if n <= 64 else 5, num_pre_smooth=2, num_post_smooth=2))
 
 
 def get(name):

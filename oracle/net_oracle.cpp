@@ -8,21 +8,27 @@
 // rounding (round to nearest even) at exactly the points where the GPU
 // stores BF16 tensors, so GPU and oracle agree to FP32 accumulation order.
 //
-//   a0 = [bf16(r / s), fluid, solid, air]           (4 channels)
-//   h0 = bf16(relu(conv0(a0) + b0))                 16 ch, N
+//   a0 = bf16(r / s) x [1, next to air, next to solid, 0] on cells with
+//        type != 0 (air neighbour: in-grid, type 0, not solid; solid
+//        neighbour: solid or outside the grid)
+//   h0 = bf16(act(conv0(a0)))                       16 ch, N
 //   p0 = bf16(avg8(h0))                             16 ch, N/2
-//   h1 = bf16(relu(conv1(p0) + b1))                 32 ch, N/2
+//   h1 = bf16(act(conv1(p0)))                       32 ch, N/2
 //   p1 = bf16(avg8(h1))                             32 ch, N/4
-//   h2 = bf16(relu(conv2(p1) + b2))                 64 ch, N/4
-//   u1 = bf16(relu(conv3(up(h2)) + b3 + h1))        32 ch, N/2
-//   u0 = bf16(relu(conv4(up(u1)) + b4 + h0))        16 ch, N
-//   z  = fluid ? s * (conv5(u0) + b5) : 0           1 ch,  N
+//   h2 = bf16(act(conv2(p1)))                       64 ch, N/4
+//   u1 = bf16(act(conv3(up(h2)) + h1))              32 ch, N/2
+//   u0 = bf16(act(conv4(up(u1)) + h0))              16 ch, N
+// act = identity (default) or ReLU (lho_net_set_relu).
+//   z  = fluid ? s * conv5(u0) : 0                  1 ch,  N
+// No biases: the packed bias entries are ignored and get zero gradient.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
 namespace {
+
+bool g_relu = false;  // activation: ReLU or identity (the GPU default)
 
 constexpr int L = 6;
 constexpr int CIN[L] = {4, 16, 32, 64, 32, 16};
@@ -148,7 +154,7 @@ Vec act(const Vec& acc, int C, const float* b, const Vec* skip) {
     for (size_t i = 0; i < acc.size(); ++i) {
         float v = float(acc[i]) + b[i % C];
         if (skip) v += float((*skip)[i]);
-        out[i] = bf(v > 0.f ? v : 0.f);
+        out[i] = bf((!g_relu || v > 0.f) ? v : 0.f);
     }
     return out;
 }
@@ -170,7 +176,11 @@ std::vector<float> wbf(const float* p, int l) {
     for (float& v : w) v = bf(v);
     return w;
 }
-const float* bias(const float* p, int l) { return p + poff(l) + 27LL * COUT[l] * CIN[l]; }
+const float kZeroBias[64] = {};
+const float* bias(const float* p, int l) {
+    (void)p, (void)l;
+    return kZeroBias;  // bias-free network
+}
 
 Fwd forward(const float* params, const int dims[3], const float* r, const uint8_t* type, const uint8_t* solid,
             double scale) {
@@ -190,14 +200,29 @@ Fwd forward(const float* params, const int dims[3], const float* r, const uint8_
     }
     f.s = scale > 0 ? float(scale) : float((cnt > 0 && ss > 0) ? std::sqrt(ss / cnt) : 1.0);
     f.a0.assign(size_t(V0) * 4, 0.0);
-    for (long long v = 0; v < V0; ++v) {
-        const bool fl = f.fluid[size_t(v)];
-        const bool so = !fl && solid && solid[v];
-        f.a0[size_t(v) * 4 + 0] = bf(fl ? r[v] / f.s : 0.f);
-        f.a0[size_t(v) * 4 + 1] = fl ? 1.0 : 0.0;
-        f.a0[size_t(v) * 4 + 2] = so ? 1.0 : 0.0;
-        f.a0[size_t(v) * 4 + 3] = (!fl && !so) ? 1.0 : 0.0;
-    }
+    const Grid& g0 = f.g0;
+    for (int x = 0; x < g0.n[0]; ++x)
+        for (int y = 0; y < g0.n[1]; ++y)
+            for (int z = 0; z < g0.n[2]; ++z) {
+                const long long v = g0.idx(x, y, z);
+                if (!f.fluid[size_t(v)]) continue;
+                bool air = false, sol = false;
+                const int d[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                for (int k = 0; k < 6; ++k) {
+                    const int xx = x + d[k][0], yy = y + d[k][1], zz = z + d[k][2];
+                    if (!g0.in(xx, yy, zz)) {
+                        sol = true;
+                        continue;
+                    }
+                    const long long u = g0.idx(xx, yy, zz);
+                    if (solid && solid[u]) sol = true;
+                    else if (type[u] == 0) air = true;
+                }
+                const double rh = bf(r[v] / f.s);
+                f.a0[size_t(v) * 4 + 0] = rh;
+                f.a0[size_t(v) * 4 + 1] = air ? rh : 0.0;
+                f.a0[size_t(v) * 4 + 2] = sol ? rh : 0.0;
+            }
     f.h0 = act(conv(f.g0, f.a0, 4, wbf(params, 0), 16), 16, bias(params, 0), nullptr);
     f.p0 = pool(f.g0, f.g1, f.h0, 16);
     f.h1 = act(conv(f.g1, f.p0, 16, wbf(params, 1), 32), 32, bias(params, 1), nullptr);
@@ -209,14 +234,14 @@ Fwd forward(const float* params, const int dims[3], const float* r, const uint8_
     f.u0 = act(conv(f.g0, f.q0, 32, wbf(params, 4), 16), 16, bias(params, 4), &f.h0);
     Vec y = conv(f.g0, f.u0, 16, wbf(params, 5), 1);
     f.y.resize(size_t(V0));
-    for (long long v = 0; v < V0; ++v) f.y[size_t(v)] = float(y[size_t(v)]) + bias(params, 5)[0];
+    for (long long v = 0; v < V0; ++v) f.y[size_t(v)] = float(y[size_t(v)]);
     return f;
 }
 
 // bf16(d * relu'(u))
 Vec relu_grad(const Vec& d, const Vec& u) {
     Vec g(d.size());
-    for (size_t i = 0; i < d.size(); ++i) g[i] = bf(u[i] > 0.0 ? float(d[i]) : 0.f);
+    for (size_t i = 0; i < d.size(); ++i) g[i] = bf((!g_relu || u[i] > 0.0) ? float(d[i]) : 0.f);
     return g;
 }
 
@@ -244,7 +269,7 @@ Vec relu_grad_unpool(const Grid& f, const Grid& c, const Vec& skip, const Vec& d
                     const size_t i = size_t(f.idx(x, y, z)) * C + ch;
                     float d = float(skip[i]);
                     if (c.in(x >> 1, y >> 1, z >> 1)) d += 0.125f * float(dc[size_t(c.idx(x >> 1, y >> 1, z >> 1)) * C + ch]);
-                    g[i] = bf(u[i] > 0.0 ? d : 0.f);
+                    g[i] = bf((!g_relu || u[i] > 0.0) ? d : 0.f);
                 }
     return g;
 }
@@ -256,7 +281,7 @@ Vec to_float(const Vec& v) {
 }
 
 void bgrad(const Vec& g, int C, double* db) {
-    for (size_t i = 0; i < g.size(); ++i) db[i % C] += g[i];
+    (void)g, (void)C, (void)db;  // bias-free network: zero bias gradients
 }
 
 }  // namespace
@@ -264,6 +289,9 @@ void bgrad(const Vec& g, int C, double* db) {
 extern "C" {
 
 __attribute__((visibility("default"))) long long lho_net_num_params() { return poff(L); }
+
+// relu = 1: ReLU between layers; 0: identity (the GPU network's default)
+__attribute__((visibility("default"))) void lho_net_set_relu(int relu) { g_relu = relu != 0; }
 
 __attribute__((visibility("default"))) int lho_net_forward(const float* params, const int32_t dims[3], const float* r,
                                                            const uint8_t* type, const uint8_t* solid, double scale,

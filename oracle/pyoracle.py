@@ -481,12 +481,17 @@ def _net_lib():
         lib.lho_net_num_params.restype = C.c_longlong
         lib.lho_net_forward.argtypes = [_vp, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp]
         lib.lho_net_backward.argtypes = [_vp, C.POINTER(C.c_int32), _vp, _vp, _vp, C.c_double, _vp, _vp]
+        lib.lho_net_set_relu.argtypes = [C.c_int32]
         lib._net_ready = True
     return lib
 
 
 def net_num_params():
     return int(_net_lib().lho_net_num_params())
+
+
+def net_set_relu(on):
+    _net_lib().lho_net_set_relu(1 if on else 0)
 
 
 def net_forward(params, r, type_, solid=None, scale=0.0):

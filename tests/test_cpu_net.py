@@ -20,7 +20,7 @@ def bf(t):
     return t + (r - t).detach()
 
 
-def torch_net(params, r, type_, solid):
+def torch_net(params, r, type_, solid, relu):
     p = torch.tensor(params, dtype=torch.float64, requires_grad=True)
     ws, bs, off = [], [], 0
     for cin, cout in LAYERS:
@@ -32,18 +32,27 @@ def torch_net(params, r, type_, solid):
     fl = torch.tensor(type_ != 0)
     rr = torch.tensor(r, dtype=torch.float64)
     s = float(np.float32(np.sqrt(np.sum(r.astype(np.float64) ** 2 * (type_ != 0)) / max(1, (type_ != 0).sum()))))
-    so = torch.tensor(solid != 0) & ~fl
-    a0 = torch.stack([bf(torch.where(fl, (rr.float() / np.float32(s)).double(), torch.zeros_like(rr))),
-                      fl.double(), so.double(), (~fl & ~so).double()])[None]
+    # neighbour classes: air (in-grid, type 0, not solid), solid (solid or outside)
+    pad_t = np.pad(type_, 1, constant_values=0)
+    pad_s = np.pad(solid, 1, constant_values=1)
+    air = np.zeros(type_.shape, bool)
+    sol = np.zeros(type_.shape, bool)
+    nx, ny, nz = type_.shape
+    for d in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+        sl = tuple(slice(1 + d[k], 1 + d[k] + type_.shape[k]) for k in range(3))
+        sol |= pad_s[sl] != 0
+        air |= (pad_s[sl] == 0) & (pad_t[sl] == 0)
+    rh = bf(torch.where(fl, (rr.float() / np.float32(s)).double(), torch.zeros_like(rr)))
+    a0 = torch.stack([rh, rh * torch.tensor(air), rh * torch.tensor(sol), torch.zeros_like(rh)])[None]
 
     def conv(x, l):
         return F.conv3d(x, ws[l], padding=1)
 
     def act(x, l, skip=None):
-        v = x + bs[l][None, :, None, None, None]
+        v = x  # bias-free network
         if skip is not None:
             v = v + skip
-        return bf(torch.relu(v))
+        return bf(torch.relu(v) if relu else v)
 
     def pool(x):
         return bf(F.avg_pool3d(x, 2))
@@ -60,7 +69,7 @@ def torch_net(params, r, type_, solid):
     h2 = act(conv(pool(h1), 2), 2)
     u1 = act(conv(up(h2, torch.zeros(1, 64, *h1.shape[2:], dtype=torch.float64)), 3), 3, h1)
     u0 = act(conv(up(u1, torch.zeros(1, 32, *h0.shape[2:], dtype=torch.float64)), 4), 4, h0)
-    y = conv(u0, 5)[0, 0] + bs[5][0]
+    y = conv(u0, 5)[0, 0]
     z = torch.where(fl, y * s, torch.zeros_like(y))
     return p, z
 
@@ -69,12 +78,14 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
 
 
+@pytest.mark.parametrize("relu", [False, True])
 @pytest.mark.parametrize("shape", [(8, 8, 8), (9, 6, 10)])
-def test_net_oracle_matches_torch(oracle_mod, shape):
+def test_net_oracle_matches_torch(oracle_mod, shape, relu):
     r, t, s = net_case(shape, seed=3)
     params = random_params(oracle_mod.net_num_params(), seed=4)
+    oracle_mod.net_set_relu(relu)
     z_o = oracle_mod.net_forward(params, r, t, s)
-    p, z_t = torch_net(params, r, t, s)
+    p, z_t = torch_net(params, r, t, s, relu)
     assert rel(z_o, z_t.detach().numpy()) < 1e-4
     dz = np.random.default_rng(5).standard_normal(shape).astype(np.float32)
     (z_t * torch.tensor(dz, dtype=torch.float64)).sum().backward()

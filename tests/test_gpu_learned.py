@@ -74,6 +74,29 @@ def test_fpcg_converges_and_gains_over_unpreconditioned_cg(oracle_mod, trained):
           f"MGPCG {mg_iters}; CG without a preconditioner {stp['iterations']}")
 
 
+def test_committed_network_gain_over_cg_without_preconditioner(oracle_mod, lhi):
+    """What the shipped network (liquidhairinteration_b200/weights, made by
+    liquidhairinteration_b200.train) gains over the method without it: after
+    20 iterations FPCG with the network alone (no fallback) leaves a smaller
+    relative residual than CG without a preconditioner on the 64^3 dam break.
+    (It is a weak preconditioner: the V-cycle reaches 1e-6 in about 10.)"""
+    import os
+    from liquidhairinteration_b200.net import LearnedNet
+    spec = scenes.dam(64)
+    net = LearnedNet(seed=0)
+    net.load(os.path.join(os.path.dirname(abi.__file__), "weights", "fpcg.lhinet"))
+    out = {}
+    for mode, over in (("net", dict(preconditioner=abi.PRECOND_LEARNED)), ("cg", dict(preconditioner=abi.PRECOND_NONE))):
+        g = _scene_after_p2g(oracle_mod, spec, spec.solver_params(coarse_cells=64, max_iterations=20, **over))
+        if mode == "net":
+            g.GetSolver().SetNetwork(net, fallbackIterations=-1)
+        st = g.GetSolver().Solve(spec.density, spec.dt)
+        out[mode] = st["final_residual"] / st["initial_residual"]
+    print(f"relative residual after 20 iterations: network-only FPCG {out['net']:.3f}, CG {out['cg']:.3f}")
+    assert out["net"] < out["cg"], out
+    net.close()
+
+
 def test_untrained_network_falls_back_to_vcycle(oracle_mod, lhi):
     from liquidhairinteration_b200.net import LearnedNet
     spec = scenes.dam(32)

@@ -49,22 +49,28 @@ def net(lhi):
     n.close()
 
 
+@pytest.mark.parametrize("relu", [False, True])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_net_forward_matches_oracle(oracle_mod, net, shape):
+def test_net_forward_matches_oracle(oracle_mod, net, shape, relu):
     r, t, s = net_case(shape, seed=11)
     params = random_params(oracle_mod.net_num_params(), seed=12)
     net.set_params(params)
+    net.set_relu(relu)
+    oracle_mod.net_set_relu(relu)
     z = net.forward(r, t, s)
     z_o = oracle_mod.net_forward(params, r, t, s)
     assert np.all(z[t == 0] == 0)
     assert rel(z, z_o) < 1e-2, rel(z, z_o)
 
 
+@pytest.mark.parametrize("relu", [False, True])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_net_gradients_match_oracle(oracle_mod, net, shape):
+def test_net_gradients_match_oracle(oracle_mod, net, shape, relu):
     r, t, s = net_case(shape, seed=13)
     params = random_params(oracle_mod.net_num_params(), seed=14)
     net.set_params(params)
+    net.set_relu(relu)
+    oracle_mod.net_set_relu(relu)
     dz = np.random.default_rng(15).standard_normal(shape).astype(np.float32)
     g = net.backward(r, t, s, dz)
     g_o = oracle_mod.net_backward(params, r, t, s, dz)
@@ -82,3 +88,12 @@ def test_net_scale_invariance(net):
     z1 = net.forward(r, t, s)
     z2 = net.forward(np.float32(4.0) * r, t, s)
     assert rel(z2, 4.0 * z1) < 1e-6
+
+
+def test_linear_network_is_linear(net):
+    """The default (identity activation) network is linear in r: M(a + b) = M(a) + M(b) up to BF16 storage."""
+    net.set_relu(False)
+    r, t, s = net_case((16, 16, 16), seed=19)
+    r2, _, _ = net_case((16, 16, 16), seed=20)
+    za, zb, zab = net.forward(r, t, s, scale=1.0), net.forward(r2, t, s, scale=1.0), net.forward(r + r2, t, s, scale=1.0)
+    assert rel(zab, za + zb) < 3e-2
