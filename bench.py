@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eager", action="store_true", help="host-driven PCG loop instead of the solve graph")
+    ap.add_argument("--no-fpcg", action="store_true", help="skip the learned-preconditioner FPCG leg")
     return ap.parse_args()
 
 
@@ -239,6 +240,12 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": int(algo), "avg_launch_ms": round(avg_ms, 5),
                 "launches_profiled": n_launch, "active_tiles_level0": f"{active}/{total}"}
 
+    # ---- learned-preconditioner FPCG on the same scene (V-cycle fallback on
+    # a < 5% residual drop), timed the same way over a few steps
+    fpcg = None
+    if not args.no_fpcg:
+        fpcg = run_fpcg(args, spec, stream_of=lambda m: torch.cuda.ExternalStream(m.stream_ptr()))
+
     # ---- e2e through the C-ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -294,6 +301,7 @@ def run_ours(args):
             "solve_ms": round(solve_avg, 3), "cg_iterations": round(sum(iters) / len(iters), 2),
             "particles_per_s": round(n_particles / (ms_step * 1e-3), 1),
             "scenes_per_s": round(world * 1000.0 / ms_step, 3),
+            "fpcg": fpcg,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clock_info,
             "kernel_ms_per_step": {k: round(v[1] / prof_steps, 3) for k, v in prof.items()},
@@ -301,6 +309,47 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_fpcg(args, spec, stream_of, steps=None):
+    """ms/step, solve ms and iterations of FPCG with the shipped network
+    (liquidhairinteration_b200/weights/fpcg.lhinet) on the same scene."""
+    import torch
+    from liquidhairinteration_b200 import abi, scenes
+    from liquidhairinteration_b200.net import LearnedNet
+    if args.precision == "fp64":
+        return {"unavailable": "the learned preconditioner runs on FP32 / mixed handles"}
+    net = LearnedNet(seed=0)
+    net.load(os.path.join(ROOT, "liquidhairinteration_b200", "weights", "fpcg.lhinet"))
+    m = scenes.build(spec, args.precision, spec.solver_params(preconditioner=abi.PRECOND_LEARNED))
+    m.GetSolver().SetNetwork(net, fallbackIterations=0)
+    k = steps or max(1, min(5, args.steps))
+    for _ in range(max(1, min(2, args.warmup))):
+        m.PreStep(spec.dt)
+        m.Step(spec.dt)
+    stream = stream_of(m)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    it, sol, nit, fb = [], [], [], []
+    m.sync()
+    e0.record(stream)
+    for _ in range(k):
+        m.PreStep(spec.dt)
+        m.Step(spec.dt)
+        st = m.GetSolver().Stats()
+        it.append(st["iterations"])
+        sol.append(st["solve_ms"])
+        a, b = m.GetSolver().LearnedStats()
+        nit.append(a)
+        fb.append(b)
+    e1.record(stream)
+    e1.synchronize()
+    out = {"ms_per_step": round(e0.elapsed_time(e1) / k, 3), "solve_ms": round(sum(sol) / k, 3),
+           "cg_iterations": round(sum(it) / k, 2), "network_iterations": round(sum(nit) / k, 2),
+           "fallback_at": fb, "steps": k,
+           "network": "3-level conv net, 16/32/64 channels, BF16 tcgen05 convolutions, liquidhairinteration_b200/weights/fpcg.lhinet"}
+    m.close()
+    net.close()
+    return out
 
 
 # --------------------------------------------------------- reference arm

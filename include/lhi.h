@@ -278,7 +278,10 @@ LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, co
 /* The handle's CUDA stream (cudaStream_t), e.g. to record events around
    calls; all of the handle's device work is ordered on it. */
 LHI_API int lhi_liquid_stream(lhi_liquid* h, void** stream);
-/* Number of kernels this library has launched in the process so far. */
+/* Number of kernels this library has launched in the process so far,
+   counting the kernels a solve graph replay ran (its loop body once per
+   PCG iteration; the V-cycle kernels of the final iteration, which return
+   at once, included). */
 LHI_API int lhi_kernel_launch_count(int64_t* count);
 /* Kernel categories timed by the optional profiler. */
 #define LHI_KERNEL_SORT 0         /* cell keys, radix sort, permutation, cell ranges */

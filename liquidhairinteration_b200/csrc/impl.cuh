@@ -341,6 +341,7 @@ public:
     cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on
     cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body
     cudaGraphExec_t solve_exec_ = nullptr;
+    long long graph_init_kernels_ = 0, graph_body_kernels_ = 0, graph_final_kernels_ = 0;
     // learned preconditioner
     LearnedNet* net_ = nullptr;
     int fallback_iters_ = 0;

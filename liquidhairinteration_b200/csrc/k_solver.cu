@@ -1290,7 +1290,9 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         LHI_CUDA(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cg, nullptr, nullptr));
         cudaGraphConditionalHandle h;
         LHI_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+        const long long c0 = g_kernel_launches.load();
         enqueue_init(h, 1);
+        const long long c1 = g_kernel_launches.load();
         LHI_CUDA(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cg, &deps, &nd));
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
@@ -1303,8 +1305,10 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         LHI_CUDA(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
         LHI_CUDA(cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         cur_ = side_;
+        long long c2 = 0;
         try {
             enqueue_body(h, 1);
+            c2 = g_kernel_launches.load();
         } catch (...) {
             cur_ = stream_;
             cudaGraph_t b2 = nullptr;
@@ -1315,7 +1319,12 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         cudaGraph_t body_out = nullptr;
         LHI_CUDA(cudaStreamEndCapture(side_, &body_out));
         enqueue_final();
-        LHI_CUDA(cudaStreamEndCapture(stream_, &g));
+        const long long c3 = g_kernel_launches.load();
+        graph_init_kernels_ = c1 - c0;
+        graph_body_kernels_ = c2 - c1;
+        graph_final_kernels_ = c3 - c2;
+        // captured launches did not run: the replays below count what runs
+        g_kernel_launches.fetch_sub(c3 - c0);
     } catch (...) {
         cur_ = stream_;
         cudaGraph_t g2 = nullptr;
@@ -1336,6 +1345,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     solver_init();
     build_rhs();
     build_lhs(rho, dt);
+    bool graph_replayed = false;
     const bool learned = sp_.preconditioner == LHI_PRECOND_LEARNED;
     if (learned && !net_) throw std::invalid_argument("LHI_PRECOND_LEARNED without a network (lhi_solver_set_network)");
     use_fallback_ = false;
@@ -1344,6 +1354,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     if (!sp_.eager && !prof_.on && !learned && snap_cap_ == 0) {
         if (!solve_exec_) build_solve_graph();
         LHI_CUDA(cudaGraphLaunch(solve_exec_, stream_));
+        graph_replayed = true;
     } else {
         // host-driven loop; with the learned preconditioner the host also
         // applies the fallback rule between iterations
@@ -1383,6 +1394,9 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     read_scalars();
     float ms = 0.f;
     LHI_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    if (graph_replayed)  // kernels the replay ran: init, one body per loop trip, final
+        g_kernel_launches.fetch_add(graph_init_kernels_ + graph_final_kernels_ +
+                                    graph_body_kernels_ * (long long)std::max(sc_host_->iter, 0));
     stats_.iterations = sc_host_->iter;
     stats_.initial_residual = sc_host_->residual0;
     stats_.final_residual = sc_host_->residual;
