@@ -274,6 +274,18 @@ LHI_API int lhi_liquid_field_size(const lhi_liquid* h, int32_t field, int32_t le
 LHI_API int lhi_liquid_get_field(lhi_liquid* h, int32_t field, int32_t level, void* out);
 LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, const void* in);
 
+/* Asynchronous steps (on = 1): lhi_liquid_step / lhi_liquid_projection /
+   lhi_solver_solve enqueue the whole solve on the handle's stream and return
+   at once with LHI_OK; the solve's status and statistics are read (with a
+   synchronisation) by lhi_solver_get_stats.  Independent handles stepped in
+   this mode run concurrently on the GPU (the batched form).  Solves that the
+   host drives (learned preconditioner, residual recording, profiling, eager)
+   still wait. */
+LHI_API int lhi_liquid_set_async(lhi_liquid* h, int32_t on);
+/* Empty string while solves run as CUDA graphs; otherwise why the solve
+   graph could not be built, in which case every solve runs host-driven. */
+LHI_API const char* lhi_solver_graph_error(lhi_liquid* h);
+
 /* ------------------------------------------------------- measurement */
 /* The handle's CUDA stream (cudaStream_t), e.g. to record events around
    calls; all of the handle's device work is ordered on it. */
@@ -350,6 +362,8 @@ LHI_API int lhi_solver_learned_stats(lhi_liquid* h, int32_t* network_iterations,
    recording and frees them).  Recording solves run host-driven. */
 LHI_API int lhi_solver_record_residuals(lhi_liquid* h, int32_t max_snapshots);
 LHI_API int lhi_solver_num_snapshots(lhi_liquid* h, int32_t* count);
+/* Recorded residual `index` (0 = oldest kept) as ncells floats (host). */
+LHI_API int lhi_solver_get_snapshot(lhi_liquid* h, int32_t index, float* out);
 /* Adam training of the network on the handle's recorded residuals with the
    handle's level-0 matrix A (from its last BuildLHS): each step draws
    `batch` snapshots r (seeded), accumulates the gradient of

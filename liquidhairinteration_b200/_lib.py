@@ -55,6 +55,7 @@ SIGNATURES = {
     "lhi_solver_learned_stats": [_h, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
     "lhi_solver_record_residuals": [_h, C.c_int32],
     "lhi_solver_num_snapshots": [_h, C.POINTER(C.c_int32)],
+    "lhi_solver_get_snapshot": [_h, C.c_int32, _vp],
     "lhi_net_train": [C.c_void_p, _h, C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.POINTER(C.c_double),
                       C.POINTER(C.c_double)],
     "lhi_net_tensor_core_selftest": [C.c_int32, C.c_int32, _vp, _vp, _vp, C.POINTER(C.c_int32)],
@@ -74,6 +75,8 @@ SIGNATURES = {
     "lhi_liquid_get_field": [_h, C.c_int32, C.c_int32, _vp],
     "lhi_liquid_set_field": [_h, C.c_int32, C.c_int32, _vp],
     "lhi_liquid_stream": [_h, C.POINTER(C.c_void_p)],
+    "lhi_liquid_set_async": [_h, C.c_int32],
+    "lhi_solver_graph_error": [_h],
     "lhi_kernel_launch_count": [C.POINTER(C.c_int64)],
     "lhi_liquid_profile": [_h, C.c_int32],
     "lhi_liquid_profile_read": [_h, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
@@ -84,7 +87,7 @@ SIGNATURES = {
     "lhi_scene_spawn_lattice": [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_int64, C.c_int32,
                                 C.POINTER(C.c_int64), _vp],
 }
-_RESTYPE = {"lhi_last_error": C.c_char_p}
+_RESTYPE = {"lhi_last_error": C.c_char_p, "lhi_solver_graph_error": C.c_char_p}
 
 _LIB = None
 

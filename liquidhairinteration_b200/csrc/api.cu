@@ -424,6 +424,15 @@ LHI_API int lhi_solver_num_snapshots(lhi_liquid* h, int32_t* count) {
     return LHI_OK;
 }
 
+LHI_API int lhi_solver_get_snapshot(lhi_liquid* h, int32_t index, float* out) {
+    NEED_HANDLE(h);
+    if (!out) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->get_snapshot(index, out);
+        return LHI_OK;
+    });
+}
+
 LHI_API int lhi_net_train(lhi_net* net, lhi_liquid* h, int32_t steps, int32_t batch, double lr, uint64_t seed,
                           double* first_loss, double* last_loss) {
     NEED_HANDLE(h);
@@ -507,8 +516,10 @@ LHI_API int lhi_solver_solve(lhi_liquid* h, double density, double dt, lhi_solve
 LHI_API int lhi_solver_get_stats(lhi_liquid* h, lhi_solve_stats* stats) {
     NEED_HANDLE(h);
     if (!stats) return fail(LHI_E_INVALID_ARG, "null argument");
-    *stats = h->impl->stats();
-    return LHI_OK;
+    return guarded([&]() -> int {
+        *stats = h->impl->stats();  // synchronises when an asynchronous solve is pending
+        return LHI_OK;
+    });
 }
 
 LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void* out) {
@@ -555,6 +566,17 @@ LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, co
         h->impl->set_field(field, level, in);
         return LHI_OK;
     });
+}
+
+LHI_API const char* lhi_solver_graph_error(lhi_liquid* h) {
+    if (!h || !h->impl) return "null handle";
+    return h->impl->graph_error().c_str();
+}
+
+LHI_API int lhi_liquid_set_async(lhi_liquid* h, int32_t on) {
+    NEED_HANDLE(h);
+    h->impl->set_async(on != 0);
+    return LHI_OK;
 }
 
 LHI_API int lhi_liquid_stream(lhi_liquid* h, void** stream) {

@@ -9,6 +9,7 @@
 //   TX : scalar of the outer CG iterate x (double in the mixed mode)
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -196,13 +197,16 @@ public:
     virtual void build_lhs(double rho, double dt) = 0;
     virtual void apply_preconditioner() = 0;
     virtual int solve(double rho, double dt) = 0;
-    virtual lhi_solve_stats stats() const = 0;
+    virtual lhi_solve_stats stats() = 0;
+    virtual void set_async(bool on) = 0;
+    virtual const std::string& graph_error() const = 0;
     virtual void get_ax(int level, const void* x, void* out) = 0;
     virtual void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) = 0;
     virtual void set_network(LearnedNet* net, int fallback_iterations) = 0;
     virtual void learned_stats(int32_t* net_iters, int32_t* fallback_at) = 0;
     virtual void record_residuals(int max_snapshots) = 0;
     virtual int num_snapshots() const = 0;
+    virtual void get_snapshot(int index, float* host) = 0;
     virtual void train(LearnedNet* net, int steps, int batch, double lr, uint64_t seed, double* first,
                        double* last) = 0;
     virtual int field_size(int field, int level, int64_t* count, int32_t* eb) = 0;
@@ -246,7 +250,13 @@ public:
     void build_lhs(double rho, double dt) override;
     void apply_preconditioner() override;
     int solve(double rho, double dt) override;
-    lhi_solve_stats stats() const override { return stats_; }
+    lhi_solve_stats stats() override {
+        if (stats_pending_) finish_stats();
+        return stats_;
+    }
+    void set_async(bool on) override { async_ = on; }
+    const std::string& graph_error() const override { return graph_error_; }
+    void finish_stats();
     void get_ax(int level, const void* x, void* out) override;
     void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) override;
     void set_network(LearnedNet* net, int fallback_iterations) override;
@@ -256,6 +266,13 @@ public:
     }
     void record_residuals(int max_snapshots) override;
     int num_snapshots() const override { return snap_count_; }
+    void get_snapshot(int index, float* host) override {
+        if (index < 0 || index >= snap_count_) throw std::invalid_argument("snapshot index out of range");
+        const int slot = (snap_next_ - snap_count_ + index + snap_cap_) % snap_cap_;
+        LHI_CUDA(cudaMemcpyAsync(host, snaps_ + size_t(slot) * size_t(ncell_), sizeof(float) * ncell_,
+                                 cudaMemcpyDeviceToHost, stream_));
+        LHI_CUDA(cudaStreamSynchronize(stream_));
+    }
     void train(LearnedNet* net, int steps, int batch, double lr, uint64_t seed, double* first, double* last) override;
     void ensure_solid_cells();
     void ensure_net_type();
@@ -342,6 +359,11 @@ public:
     cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body
     cudaGraphExec_t solve_exec_ = nullptr;
     long long graph_init_kernels_ = 0, graph_body_kernels_ = 0, graph_final_kernels_ = 0;
+    bool async_ = false;         // steps do not wait for the solve; statistics are read on demand
+    bool stats_pending_ = false; // the last graph solve's statistics are still on the device
+    bool last_solve_graph_ = false;
+    bool solved_once_ = false;   // graphs are captured from the second solve on
+    std::string graph_error_;    // why the solve graph could not be built (then solves run host-driven)
     // learned preconditioner
     LearnedNet* net_ = nullptr;
     int fallback_iters_ = 0;

@@ -25,6 +25,7 @@
 // reads the stop flag after every iteration.
 #include <algorithm>
 #include <random>
+#include <string>
 
 #include "impl.cuh"
 
@@ -1281,6 +1282,8 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_final() {
 // the graph is built on the first solve and replayed after.
 template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
     cudaGraph_t g = nullptr;
+    LHI_CUDA(cudaStreamSynchronize(stream_));  // surfaces any earlier asynchronous error before capturing
+    LHI_CUDA(cudaGetLastError());
     LHI_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     try {
         cudaStreamCaptureStatus st;
@@ -1320,6 +1323,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         LHI_CUDA(cudaStreamEndCapture(side_, &body_out));
         enqueue_final();
         const long long c3 = g_kernel_launches.load();
+        LHI_CUDA(cudaStreamEndCapture(stream_, &g));
         graph_init_kernels_ = c1 - c0;
         graph_body_kernels_ = c2 - c1;
         graph_final_kernels_ = c3 - c2;
@@ -1333,14 +1337,24 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         throw;
     }
     cudaGraphExec_t exec = nullptr;
-    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphInstantiateParams ip = {};
+    cudaError_t e = cudaGraphInstantiateWithParams(&exec, g, &ip);
+    std::string why;
+    if (e != cudaSuccess) {
+        cudaGraphNodeType nt = cudaGraphNodeTypeEmpty;
+        if (ip.errNode_out) cudaGraphNodeGetType(ip.errNode_out, &nt);
+        why = std::string("solve graph instantiation failed: ") + cudaGetErrorString(e) + " (result " +
+              std::to_string(int(ip.result_out)) + ", node type " + std::to_string(int(nt)) + ")";
+        cudaGetLastError();
+    }
     cudaGraphDestroy(g);
-    LHI_CUDA(e);
+    if (e != cudaSuccess) throw CudaError(e, why);
     solve_exec_ = exec;
 }
 
 // CGSolver<3>::Solve (PressureSolver.cpp:839-934)
 template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt) {
+    if (stats_pending_) finish_stats();
     LHI_CUDA(cudaEventRecord(ev0_, stream_));
     solver_init();
     build_rhs();
@@ -1351,8 +1365,20 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     use_fallback_ = false;
     learned_iters_ = 0;
     fallback_at_ = -1;
-    if (!sp_.eager && !prof_.on && !learned && snap_cap_ == 0) {
-        if (!solve_exec_) build_solve_graph();
+    // The first solve of a handle runs host-driven: it launches (and so
+    // loads) every kernel of the loop once, which must not happen for the
+    // first time inside a stream capture; later solves replay the graph.
+    const bool graph_ok = solved_once_;
+    solved_once_ = true;
+    if (!sp_.eager && !prof_.on && !learned && snap_cap_ == 0 && graph_ok && graph_error_.empty() && !solve_exec_) {
+        try {
+            build_solve_graph();
+        } catch (const CudaError& err) {
+            graph_error_ = err.what();  // keep solving, host-driven (lhi_solver_graph_error)
+            cudaGetLastError();         // the failed capture's error is not this solve's
+        }
+    }
+    if (!sp_.eager && !prof_.on && !learned && snap_cap_ == 0 && graph_ok && solve_exec_) {
         LHI_CUDA(cudaGraphLaunch(solve_exec_, stream_));
         graph_replayed = true;
     } else {
@@ -1391,10 +1417,19 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
         enqueue_final();
     }
     LHI_CUDA(cudaEventRecord(ev1_, stream_));
+    last_solve_graph_ = graph_replayed;
+    stats_pending_ = true;
+    if (async_ && graph_replayed) return LHI_OK;  // read by stats() later
+    finish_stats();
+    return stats_.status;
+}
+
+// Statistics of the last solve from the device scalars (synchronises).
+template <class T, class TX> void LiquidImpl<T, TX>::finish_stats() {
     read_scalars();
     float ms = 0.f;
     LHI_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
-    if (graph_replayed)  // kernels the replay ran: init, one body per loop trip, final
+    if (last_solve_graph_)  // kernels the replay ran: init, one body per loop trip, final
         g_kernel_launches.fetch_add(graph_init_kernels_ + graph_final_kernels_ +
                                     graph_body_kernels_ * (long long)std::max(sc_host_->iter, 0));
     stats_.iterations = sc_host_->iter;
@@ -1403,7 +1438,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     stats_.true_residual = std::sqrt(sc_host_->true2);
     stats_.solve_ms = ms;
     stats_.status = sc_host_->status;
-    return stats_.status;
+    stats_pending_ = false;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::spmv(int level, const T* x, T* y) {

@@ -26,6 +26,7 @@ def test_cpp_scene_loop_runs_on_gpu(lhi):
     out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
     res = json.loads(out.stdout.strip().splitlines()[-1])
+    print(res)
     assert res["particles"] > 10000
     assert res["correct_volume_throws"]
     assert 0.0 < res["ymin"] < res["ymax"] < 0.6
