@@ -82,6 +82,14 @@ extern "C" {
                                     A z includes the diagonal, so w = 0.5 gives z_GS / 2     */
 #define LHI_SMOOTHER_DAMPED_GS 1 /* z = z + w (r - A z) / diag: damped Gauss-Seidel           */
 
+/* Red-black sweep kernels of the FP32 V-cycle.  FUSED: one pass per sweep
+   over shared-memory tiles staged by TMA, both colours, into a second
+   solution buffer (levels whose z extent is a multiple of 4; other levels
+   and FP64 use SPLIT).  SPLIT: one launch per colour, in place.  Both give
+   the same values. */
+#define LHI_SWEEP_FUSED 0
+#define LHI_SWEEP_SPLIT 1
+
 typedef struct lhi_grid_desc {
     int32_t dim[3];        /* gridDimension (SceneParameter.h:137)          */
     int32_t reserved;
@@ -111,7 +119,8 @@ typedef struct lhi_solver_params {   /* SolverParameter<3> (SceneParameter.h:10-
                                         synchronisation per iteration); 0: the
                                         loop runs on the device as a CUDA graph
                                         with a conditional while node          */
-    int32_t reserved[1];
+    int32_t sweep_kernel;            /* LHI_SWEEP_* (0 = fused where the level
+                                        allows it)                             */
 } lhi_solver_params;
 
 typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> */

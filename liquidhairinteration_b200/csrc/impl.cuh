@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "lhi.h"
 #include "net.cuh"
+#include "tma.cuh"
 
 namespace lhi {
 
@@ -56,7 +57,8 @@ struct SolveScalars {
     int status;       // LHI_OK / LHI_E_NOT_CONVERGED / LHI_E_NAN
     int true_now;     // this iteration recomputes r = b - A x
     int tile_count[kMaxLevels];
-    int pad_i[2];
+    int timeout;      // a bounded wait on a shared-memory staging copy gave up
+    int pad_i[1];
 };
 
 // Active-tile set of one level: 8 x 8 x 32-cell tiles (x, y, z) holding a
@@ -85,6 +87,12 @@ template <class T> struct LevelDev {
     int ntiles = 0;
     uint8_t* tile_flag = nullptr;            // ntiles
     int32_t* tiles = nullptr;                // active tile ids, count in SolveScalars::tile_count
+    // fused red-black sweep (FP32 levels whose nz is a multiple of 4)
+    bool fused = false;
+    T* zb = nullptr;                         // the sweep writes here, then z and zb swap
+    uint8_t* mask = nullptr;                 // neighbour mask per cell, [nx][ny][mpitch]
+    int mpitch = 0;
+    CUtensorMap tm_z, tm_zb, tm_r, tm_d, tm_cx, tm_cy, tm_cz, tm_m;
 };
 
 // Optional per-category device timing: CUDA events on the handle's stream
@@ -297,7 +305,10 @@ public:
     void vcycle();
     void build_tiles();
     void setup_coarse();
+    void setup_fused();  // second z buffers, masks and tensor maps of the fused sweep
+    void build_masks();
     void enqueue_vcycle();
+    void enqueue_vcycle_levels();
     void enqueue_precond();
     void enqueue_init(unsigned long long cond, int use_cond);
     void enqueue_body(unsigned long long cond, int use_cond);

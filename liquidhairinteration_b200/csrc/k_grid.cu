@@ -388,6 +388,7 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
         LHI_CUDA(cudaMemsetAsync(L.tiles, 0, sizeof(int32_t) * nt, stream_));
     }
     setup_coarse();
+    setup_fused();
     tile_grid_ = kSMs * 6;
     LHI_CUDA(cudaMalloc(&rhs_, sizeof(T) * ncell_));
     LHI_CUDA(cudaMalloc(&x_, sizeof(TX) * ncell_));
@@ -442,6 +443,8 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
         F(lv_[l].phi);
         F(lv_[l].r);
         F(lv_[l].z);
+        F(lv_[l].zb);
+        F(lv_[l].mask);
         F(lv_[l].tile_flag);
         F(lv_[l].tiles);
     }

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <random>
 #include <string>
+#include <type_traits>
 
 #include "impl.cuh"
 
@@ -399,6 +400,164 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_sweep(LevelK<T> L, TileK tk
             if (act[k] && smooth7(c[k], rv[k], w, variant, out)) z[idx[k]] = out;
         }
     }
+}
+
+// ------------------------------------------------- fused red-black sweep
+// One damped red-black Gauss-Seidel sweep (both colours) of an FP32 level in
+// one pass.  A CTA takes an active 8 x 8 x 32 tile T and stages by TMA:
+//   Z  (z_in)    T grown by 2 cells in x and y, z from z0-4: 12 x 12 x 40
+//   R, D, CZ     T grown by 1 in x and y:                    10 x 10 x 40
+//   CX           as R with x from x0-2:                      11 x 10 x 40
+//   CY           as R with y from y0-2:                      10 x 11 x 40
+//   M (bytes)    T grown by 1, z from z0-16:                 10 x 10 x 64
+// It updates colour 0 on T grown by one cell (the ring recomputes exactly
+// what the neighbouring tiles compute), then colour 1 on T, in place in
+// shared memory, and writes T to z_out.  Reading z_in and writing z_out
+// keeps the neighbours' halo reads on the old values.  Each cell's update is
+// the arithmetic of smooth7 in the same order, so the values equal those of
+// two k_sweep launches.  Cells outside the grid read diag 0 and are skipped.
+namespace rb {
+constexpr int kZW = 40;
+constexpr int kZ = 12 * 12 * kZW;
+constexpr int kR = 10 * 10 * kZW;
+constexpr int kC = 11 * 10 * kZW;
+constexpr int kMW = 64;
+constexpr int kM = 10 * 10 * kMW;
+constexpr uint32_t kTx = uint32_t((kZ + 3 * kR + 2 * kC) * 4 + kM);  // bytes the 7 boxes deliver
+constexpr int al(int b) { return (b + 127) & ~127; }
+constexpr int oZ = 128;
+constexpr int oR = oZ + al(kZ * 4);
+constexpr int oD = oR + al(kR * 4);
+constexpr int oCZ = oD + al(kR * 4);
+constexpr int oCX = oCZ + al(kR * 4);
+constexpr int oCY = oCX + al(kC * 4);
+constexpr int oM = oCY + al(kC * 4);
+constexpr int kSmem = oM + al(kM);
+}  // namespace rb
+
+// Mask bits of a cell: 0..5 neighbour +x, -x, +y, -y, +z, -z exists with phi < 0;
+// 6: the cell's own type is not 0.
+__device__ __forceinline__ void rb_cell(float* __restrict__ Zs, const float* __restrict__ Rs,
+                                        const float* __restrict__ Ds, const float* __restrict__ CZs,
+                                        const float* __restrict__ CXs, const float* __restrict__ CYs,
+                                        const uint8_t* __restrict__ Ms, int lx, int ly, int lz, float w, int variant) {
+    const int ri = ((lx + 1) * 10 + (ly + 1)) * rb::kZW + (lz + 4);
+    const float d = Ds[ri];
+    if (is_small(d)) return;
+    const int zi = ((lx + 2) * 12 + (ly + 2)) * rb::kZW + (lz + 4);
+    const unsigned m = Ms[((lx + 1) * 10 + (ly + 1)) * rb::kMW + (lz + 16)];
+    const float zc = Zs[zi];
+    float ax = 0.f;
+    if (m & 64u) {
+        const int xi = ((lx + 2) * 10 + (ly + 1)) * rb::kZW + (lz + 4);
+        const int yi = ((lx + 1) * 11 + (ly + 2)) * rb::kZW + (lz + 4);
+        ax = zc * d;
+        if (m & 1u) ax += Zs[zi + 12 * rb::kZW] * CXs[xi];
+        if (m & 2u) ax += Zs[zi - 12 * rb::kZW] * CXs[xi - 10 * rb::kZW];
+        if (m & 4u) ax += Zs[zi + rb::kZW] * CYs[yi];
+        if (m & 8u) ax += Zs[zi - rb::kZW] * CYs[yi - rb::kZW];
+        if (m & 16u) ax += Zs[zi + 1] * CZs[ri];
+        if (m & 32u) ax += Zs[zi - 1] * CZs[ri - 1];
+    }
+    const float term = (Rs[ri] - ax) / d;
+    float out;
+    if (variant == LHI_SMOOTHER_DAMPED_GS) out = zc + w * term;
+    else out = float((1.0 - double(w)) * double(zc) + double(float(w * term)));
+    Zs[zi] = out;
+}
+
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_rb_fused(const __grid_constant__ CUtensorMap mz, const __grid_constant__ CUtensorMap mr,
+               const __grid_constant__ CUtensorMap md, const __grid_constant__ CUtensorMap mcx,
+               const __grid_constant__ CUtensorMap mcy, const __grid_constant__ CUtensorMap mcz,
+               const __grid_constant__ CUtensorMap mm, int nx, int ny, int nz, const int32_t* __restrict__ ids,
+               const int* __restrict__ count, int tdy, int tdz, float* __restrict__ zout, float w, int variant,
+               SolveScalars* __restrict__ sc) {
+    if (sc->stop) return;
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    float* Zs = reinterpret_cast<float*>(sm + rb::oZ);
+    float* Rs = reinterpret_cast<float*>(sm + rb::oR);
+    float* Ds = reinterpret_cast<float*>(sm + rb::oD);
+    float* CZs = reinterpret_cast<float*>(sm + rb::oCZ);
+    float* CXs = reinterpret_cast<float*>(sm + rb::oCX);
+    float* CYs = reinterpret_cast<float*>(sm + rb::oCY);
+    uint8_t* Ms = sm + rb::oM;
+    if (threadIdx.x == 0) bar_init(bar, 1);
+    __syncthreads();
+    const int units = *count;
+    unsigned parity = 0;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int id = ids[u];
+        const int tz = id % tdz, rest = id / tdz;
+        const int ty = rest % tdy, tx = rest / tdy;
+        const int x0 = tx * kTileX, y0 = ty * kTileY, z0 = tz * kTileZ;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            bar_expect_tx(bar, rb::kTx);
+            tma_load_box(Zs, &mz, z0 - 4, y0 - 2, x0 - 2, bar);
+            tma_load_box(Rs, &mr, z0 - 4, y0 - 1, x0 - 1, bar);
+            tma_load_box(Ds, &md, z0 - 4, y0 - 1, x0 - 1, bar);
+            tma_load_box(CZs, &mcz, z0 - 4, y0 - 1, x0 - 1, bar);
+            tma_load_box(CXs, &mcx, z0 - 4, y0 - 1, x0 - 2, bar);
+            tma_load_box(CYs, &mcy, z0 - 4, y0 - 2, x0 - 1, bar);
+            tma_load_box(Ms, &mm, z0 - 16, y0 - 1, x0 - 1, bar);
+        }
+        if (!bar_wait(bar, parity)) {
+            if (threadIdx.x == 0) {
+                sc->timeout = 1;
+                sc->status = LHI_E_TIMEOUT;
+                sc->stop = 1;
+            }
+            return;
+        }
+        parity ^= 1u;
+        // colour 0 ((x + y + z) even) on T grown by one cell: 10 x 10 rows of 17
+        for (int q = threadIdx.x; q < 100 * 17; q += kTileThreads) {
+            const int row = q / 17, k = q - row * 17;
+            const int lx = row / 10 - 1, ly = row - (row / 10) * 10 - 1;
+            const int lz = ((x0 + lx + y0 + ly + z0 - 1) & 1) - 1 + 2 * k;
+            rb_cell(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant);
+        }
+        __syncthreads();
+        // colour 1 on T: 8 x 8 rows of 16
+        for (int q = threadIdx.x; q < 64 * 16; q += kTileThreads) {
+            const int row = q >> 4, k = q & 15;
+            const int lx = row >> 3, ly = row & 7;
+            const int lz = ((x0 + lx + y0 + ly + z0 + 1) & 1) + 2 * k;
+            rb_cell(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant);
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < 64 * 8; q += kTileThreads) {
+            const int row = q >> 3, c = q & 7;
+            const int lx = row >> 3, ly = row & 7;
+            const int x = x0 + lx, y = y0 + ly, z = z0 + 4 * c;
+            if (x < nx && y < ny && z < nz) {
+                const float4 v = *reinterpret_cast<const float4*>(Zs + ((lx + 2) * 12 + (ly + 2)) * rb::kZW + 4 + 4 * c);
+                *reinterpret_cast<float4*>(zout + ((long long)x * ny + y) * nz + z) = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Neighbour masks of one level for the fused sweep (bits as rb_cell reads them).
+template <class T>
+__global__ void k_level_mask(LevelK<T> L, uint8_t* __restrict__ mask, int pitch) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    if (i >= n) return;
+    int x, y, z;
+    decode(i, L.ny, L.nz, x, y, z);
+    const long long sy = L.nz, sx = (long long)L.ny * L.nz;
+    unsigned m = L.type[i] != 0 ? 64u : 0u;
+    if (x + 1 < L.nx && L.type[i + sx] == 2) m |= 1u;
+    if (x > 0 && L.type[i - sx] == 2) m |= 2u;
+    if (y + 1 < L.ny && L.type[i + sy] == 2) m |= 4u;
+    if (y > 0 && L.type[i - sy] == 2) m |= 8u;
+    if (z + 1 < L.nz && L.type[i + 1] == 2) m |= 16u;
+    if (z > 0 && L.type[i - 1] == 2) m |= 32u;
+    mask[((long long)x * L.ny + y) * pitch + z] = uint8_t(m);
 }
 
 // CGSolver<3>::Restrict (PressureSolver.cpp:796-819) at one coarse cell: the
@@ -1033,7 +1192,46 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
         LHI_LAUNCH_CHECK();
     }
     build_tiles();
+    build_masks();
     net_type_fresh_ = false;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::build_masks() {
+    for (int l = 0; l < nlev_; ++l) {
+        LevelDev<T>& L = lv_[l];
+        if (!L.fused) continue;
+        k_level_mask<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(lk(L), L.mask, L.mpitch);
+        LHI_LAUNCH_CHECK();
+    }
+}
+
+// Levels that the fused sweep can take: FP32, z extent a multiple of 4 (TMA
+// strides are multiples of 16 bytes) and boxes no larger than the level.
+template <class T, class TX> void LiquidImpl<T, TX>::setup_fused() {
+    if constexpr (std::is_same<T, float>::value) {
+        LHI_CUDA(cudaFuncSetAttribute(k_rb_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, rb::kSmem));
+        for (int l = 0; l < nlev_; ++l) {
+            LevelDev<T>& L = lv_[l];
+            if (L.n == 0 || L.nz % 4 != 0 || L.nx < 12 || L.ny < 12 || L.nz < rb::kMW) continue;
+            L.mpitch = (L.nz + 15) / 16 * 16;
+            const size_t mb = size_t(L.nx) * L.ny * L.mpitch;
+            LHI_CUDA(cudaMalloc(&L.zb, sizeof(T) * L.n));
+            LHI_CUDA(cudaMalloc(&L.mask, mb));
+            LHI_CUDA(cudaMemsetAsync(L.zb, 0, sizeof(T) * L.n, stream_));
+            LHI_CUDA(cudaMemsetAsync(L.mask, 0, mb, stream_));
+            const auto F32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+            L.tm_z = make_box_map(L.z, F32, 4, L.nx, L.ny, L.nz, L.nz, 12, 12, rb::kZW);
+            L.tm_zb = make_box_map(L.zb, F32, 4, L.nx, L.ny, L.nz, L.nz, 12, 12, rb::kZW);
+            L.tm_r = make_box_map(L.r, F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 10, rb::kZW);
+            L.tm_d = make_box_map(L.diag, F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 10, rb::kZW);
+            L.tm_cz = make_box_map(L.cf[2], F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 10, rb::kZW);
+            L.tm_cx = make_box_map(L.cf[0], F32, 4, L.nx, L.ny, L.nz, L.nz, 11, 10, rb::kZW);
+            L.tm_cy = make_box_map(L.cf[1], F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 11, rb::kZW);
+            L.tm_m = make_box_map(L.mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.nx, L.ny, L.nz, L.mpitch, 10, 10,
+                                  rb::kMW);
+            L.fused = true;
+        }
+    }
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_tiles() {
@@ -1056,6 +1254,20 @@ template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweep
     if (L.n == 0 || sweeps <= 0 || G == 0) return;
     const T w = T(sp_.smoothing_factor);
     const int cat = (level == 0) ? LHI_KERNEL_SMOOTH_FINE : LHI_KERNEL_SMOOTH_COARSE;
+    if (L.fused && sp_.sweep_kernel == LHI_SWEEP_FUSED) {
+        const unsigned GF = unsigned(std::min(L.ntiles, 2 * kSMs));
+        for (int s = 0; s < sweeps; ++s) {
+            auto ps_ = scope(cat);
+            k_rb_fused<<<GF, kTileThreads, rb::kSmem, cur_>>>(
+                L.tm_z, L.tm_r, L.tm_d, L.tm_cx, L.tm_cy, L.tm_cz, L.tm_m, L.nx, L.ny, L.nz, L.tiles,
+                &sc_->tile_count[level], L.tdim[1], L.tdim[2], reinterpret_cast<float*>(L.zb), float(w),
+                sp_.smoother, sc_);
+            LHI_LAUNCH_CHECK();
+            std::swap(L.z, L.zb);
+            std::swap(L.tm_z, L.tm_zb);
+        }
+        return;
+    }
     const TileK tk = tile_k(L, &sc_->tile_count[level], tile_grid_, 4);
     for (int s = 0; s < sweeps; ++s)
         for (int phase = 0; phase < 2; ++phase) {
@@ -1120,6 +1332,21 @@ template <class T, class TX> void LiquidImpl<T, TX>::setup_coarse() {
 
 // CGSolver<3>::ApplyPreconditioner multigrid branch (PressureSolver.cpp:730-771)
 template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle() {
+    T* z_at_start[kMaxLevels];
+    for (int l = 0; l < nlev_; ++l) z_at_start[l] = lv_[l].z;
+    enqueue_vcycle_levels();
+    // an odd number of fused sweeps on a level leaves its result in the other
+    // buffer: copy it back so every V-cycle starts and ends on the same one
+    for (int l = 0; l < nlev_; ++l) {
+        LevelDev<T>& L = lv_[l];
+        if (L.z == z_at_start[l]) continue;
+        LHI_CUDA(cudaMemcpyAsync(L.zb, L.z, sizeof(T) * L.n, cudaMemcpyDeviceToDevice, cur_));
+        std::swap(L.z, L.zb);
+        std::swap(L.tm_z, L.tm_zb);
+    }
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle_levels() {
     const int last = nlev_ - 1;
     const int Lc = coarse_level_;
     if (Lc <= last) {
@@ -1437,7 +1664,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::finish_stats() {
     stats_.final_residual = sc_host_->residual;
     stats_.true_residual = std::sqrt(sc_host_->true2);
     stats_.solve_ms = ms;
-    stats_.status = sc_host_->status;
+    stats_.status = sc_host_->timeout ? LHI_E_TIMEOUT : sc_host_->status;
     stats_pending_ = false;
 }
 
