@@ -67,7 +67,8 @@ struct SolveScalars {
 constexpr int kTileX = 8, kTileY = 8, kTileZ = 32;
 constexpr int kTileThreads = 256;  // 8 warps: warp w takes x = x0 + w, lane = z - z0
 constexpr int kDefaultCoarseCells = 4096;  // levels below the finest this small go to one CTA
-constexpr size_t kCoarseSmemBytes = 200 * 1024;  // shared memory of that CTA
+constexpr size_t kCoarseSmemBytes = 224 * 1024;  // shared memory of that CTA
+constexpr int kCoarseThreads = 1024;
 
 struct GridGeom {
     int nx, ny, nz;
@@ -365,6 +366,9 @@ public:
     LevelDev<T> lv_[kMaxLevels];
     int coarse_level_ = 0;   // first level solved by the single-CTA coarse kernel (nlev_ if none)
     size_t coarse_smem_ = 0; // its dynamic shared memory
+    uint32_t* coarse_list_ = nullptr;  // per-colour update lists of the coarse levels
+    long long coarse_list_off_[kMaxLevels] = {};
+    int* coarse_counts_ = nullptr;
     int tile_grid_ = 0;      // persistent CTAs of the tile kernels
     cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on
     cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body

@@ -448,6 +448,8 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
         F(lv_[l].tile_flag);
         F(lv_[l].tiles);
     }
+    F(coarse_list_);
+    F(coarse_counts_);
     if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
     F(solid_cell_);
     F(net_type_);

@@ -651,51 +651,96 @@ template <class T> struct CoarseLevels {
     LevelK<T> L[kMaxLevels];
     T* r[kMaxLevels];
     T* z[kMaxLevels];
+    const uint32_t* list[kMaxLevels];
+    const int* counts;
 };
 
-// Sweeps of one level inside the CTA: thread t owns cells t + k * blockDim
-// (k < 4 per batch of 4 * blockDim cells); coordinates of the first batch are decoded
-// once, and each colour loads all of a thread's cells before updating.
+// Per-colour lists of the cells a coarse sweep updates (diag not small), one
+// 32-bit entry per cell: index (low 16 bits) | neighbour mask << 16 (bits as
+// the fused sweep's masks).  Built once per BuildLHS by one CTA; counts[2l]
+// ends colour 0 of level l and counts[2l + 1] ends colour 1.
+struct CoarseLists {
+    uint32_t* list[kMaxLevels];
+    int* counts;
+};
+
 template <class T>
-__device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z, T w, int variant, int sweeps) {
-    const int n = L.nx * L.ny * L.nz;
-    constexpr int kPer = 4;  // cells per thread per batch
-    int ci[kPer], cx[kPer], cy[kPer], cz[kPer];
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-        ci[k] = threadIdx.x + k * blockDim.x;
-        const int i = ci[k] < n ? ci[k] : 0;
-        cz[k] = i % L.nz;
-        cy[k] = (i / L.nz) % L.ny;
-        cx[k] = i / (L.nz * L.ny);
+__global__ void __launch_bounds__(1024) k_coarse_lists(CoarseLevels<T> c, CoarseLists cl) {
+    __shared__ int warp_tot[32];
+    __shared__ int base;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    for (int l = c.first; l <= c.last; ++l) {
+        const LevelK<T>& L = c.L[l];
+        const int n = L.nx * L.ny * L.nz;
+        const int sy = L.nz, sx = L.ny * L.nz;
+        if (threadIdx.x == 0) base = 0;
+        __syncthreads();
+        for (int colour = 0; colour < 2; ++colour) {
+            for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+                const int i = c0 + threadIdx.x;
+                uint32_t ent = 0;
+                int f = 0;
+                if (i < n) {
+                    const int zz = i % L.nz, y = (i / L.nz) % L.ny, x = i / sx;
+                    if (((x + y + zz) & 1) == colour && !is_small(L.diag[i])) {
+                        unsigned m = L.type[i] != 0 ? 64u : 0u;
+                        if (x + 1 < L.nx && L.type[i + sx] == 2) m |= 1u;
+                        if (x > 0 && L.type[i - sx] == 2) m |= 2u;
+                        if (y + 1 < L.ny && L.type[i + sy] == 2) m |= 4u;
+                        if (y > 0 && L.type[i - sy] == 2) m |= 8u;
+                        if (zz + 1 < L.nz && L.type[i + 1] == 2) m |= 16u;
+                        if (zz > 0 && L.type[i - 1] == 2) m |= 32u;
+                        ent = uint32_t(i) | (m << 16);
+                        f = 1;
+                    }
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, f);
+                if (lane == 0) warp_tot[wp] = __popc(bal);
+                __syncthreads();
+                int off = base;
+                for (int k = 0; k < wp; ++k) off += warp_tot[k];
+                if (f) cl.list[l][off + __popc(bal & ((1u << lane) - 1u))] = ent;
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < int(blockDim.x >> 5); ++k) base += warp_tot[k];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) cl.counts[2 * l + colour] = base;
+            __syncthreads();
+        }
     }
+}
+
+// Sweeps of one level inside the CTA over its colour lists: smooth7's
+// arithmetic in the same order on shared-memory rows.
+template <class T>
+__device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z, const uint32_t* list, int n0,
+                                           int n01, T w, int variant, int sweeps) {
+    const int sy = L.nz, sx = L.ny * L.nz;
     for (int s = 0; s < sweeps; ++s)
-        for (int phase = 0; phase < 2; ++phase) {
-            for (int base = 0; base < n; base += kPer * blockDim.x) {
-                Cell7<T, T> c[kPer];
-                T rv[kPer];
-                bool act[kPer];
-                int ii[kPer];
-#pragma unroll
-                for (int k = 0; k < kPer; ++k) {
-                    int i = base + ci[k], x = cx[k], y = cy[k], zz = cz[k];
-                    if (base > 0) {
-                        zz = i % L.nz;
-                        y = (i / L.nz) % L.ny;
-                        x = i / (L.nz * L.ny);
-                    }
-                    ii[k] = i;
-                    act[k] = i < n && ((x + y + zz) & 1) == phase;
-                    if (act[k]) {
-                        load7(L, z, i, x, y, zz, c[k]);
-                        rv[k] = r[i];
-                    }
+        for (int colour = 0; colour < 2; ++colour) {
+            const int end = colour ? n01 : n0;
+            for (int e = (colour ? n0 : 0) + int(threadIdx.x); e < end; e += blockDim.x) {
+                const uint32_t ent = list[e];
+                const int i = int(ent & 0xffffu);
+                const unsigned m = ent >> 16;
+                const T d = L.diag[i];
+                const T zc = z[i];
+                T ax = T(0);
+                if (m & 64u) {
+                    ax = zc * d;
+                    if (m & 1u) ax += z[i + sx] * L.cx[i];
+                    if (m & 2u) ax += z[i - sx] * L.cx[i - sx];
+                    if (m & 4u) ax += z[i + sy] * L.cy[i];
+                    if (m & 8u) ax += z[i - sy] * L.cy[i - sy];
+                    if (m & 16u) ax += z[i + 1] * L.cz[i];
+                    if (m & 32u) ax += z[i - 1] * L.cz[i - 1];
                 }
-#pragma unroll
-                for (int k = 0; k < kPer; ++k) {
-                    T out;
-                    if (act[k] && smooth7(c[k], rv[k], w, variant, out)) z[ii[k]] = out;
-                }
+                const T term = (r[i] - ax) / d;
+                T out;
+                if (variant == LHI_SMOOTHER_DAMPED_GS) out = zc + w * term;
+                else out = T((1.0 - double(w)) * double(zc) + double(T(w * term)));
+                z[i] = out;
             }
             __syncthreads();
         }
@@ -704,13 +749,15 @@ __device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z,
 // The whole coarse V-cycle in one CTA with every coarse level staged in
 // shared memory: r, z, diag, cx, cy, cz (Scalar) and type per level.
 template <class T>
-__global__ void __launch_bounds__(512) k_coarse_cycle(CoarseLevels<T> c, T w, int variant, int pre, int post, int fin,
-                                                        const int* __restrict__ stop) {
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(CoarseLevels<T> c, T w, int variant, int pre, int post,
+                                                                   int fin, const int* __restrict__ stop) {
     if (*stop) return;
     extern __shared__ __align__(16) unsigned char smem[];
     LevelK<T> S[kMaxLevels];
     T* r[kMaxLevels];
     T* z[kMaxLevels];
+    uint32_t* lst[kMaxLevels];
+    int n0[kMaxLevels], n01[kMaxLevels];
     size_t off = 0;
     for (int l = c.first; l <= c.last; ++l) {
         const LevelK<T>& G = c.L[l];
@@ -725,7 +772,12 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarseLevels<T> c, T w, in
         off += size_t(6) * n * sizeof(T);
         uint8_t* ty = smem + off;
         off += (size_t(n) + 15) & ~size_t(15);
+        lst[l] = reinterpret_cast<uint32_t*>(smem + off);
+        off += size_t(n) * 4;
         S[l] = LevelK<T>{G.nx, G.ny, G.nz, d, ax, ay, az, ty};
+        n0[l] = c.counts[2 * l];
+        n01[l] = c.counts[2 * l + 1];
+        for (int e = threadIdx.x; e < n01[l]; e += blockDim.x) lst[l][e] = c.list[l][e];
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             d[i] = G.diag[i];
             ax[i] = G.cx[i];
@@ -738,7 +790,7 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarseLevels<T> c, T w, in
     }
     __syncthreads();
     for (int l = c.first; l < c.last; ++l) {
-        cta_smooth(S[l], r[l], z[l], w, variant, pre);
+        cta_smooth(S[l], r[l], z[l], lst[l], n0[l], n01[l], w, variant, pre);
         const LevelK<T>& C = S[l + 1];
         const int n = C.nx * C.ny * C.nz;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -747,7 +799,7 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarseLevels<T> c, T w, in
         }
         __syncthreads();
     }
-    cta_smooth(S[c.last], r[c.last], z[c.last], w, variant, fin);
+    cta_smooth(S[c.last], r[c.last], z[c.last], lst[c.last], n0[c.last], n01[c.last], w, variant, fin);
     for (int l = c.last - 1; l >= c.first; --l) {
         const LevelK<T>& C = S[l + 1];
         const LevelK<T>& F = S[l];
@@ -763,7 +815,7 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarseLevels<T> c, T w, in
             }
         }
         __syncthreads();
-        cta_smooth(F, r[l], z[l], w, variant, post);
+        cta_smooth(F, r[l], z[l], lst[l], n0[l], n01[l], w, variant, post);
     }
     for (int l = c.first; l <= c.last; ++l) {
         const int n = S[l].nx * S[l].ny * S[l].nz;
@@ -1119,6 +1171,23 @@ __global__ void k_loss_grad(LevelK<T> L, const float* __restrict__ e, int batch,
     if (blockIdx.x == 0 && threadIdx.x == 0) red[2] += red[0] / rr / batch;
 }
 
+// The coarse kernel's view of levels [first, nlev): pointers and lists.
+template <class T>
+CoarseLevels<T> coarse_levels_of(const LevelDev<T>* lv, int nlev, int first, uint32_t* list, const long long* off,
+                                 int* counts) {
+    CoarseLevels<T> c{};
+    c.first = first;
+    c.last = nlev - 1;
+    for (int l = first; l < nlev; ++l) {
+        c.L[l] = lk(lv[l]);
+        c.r[l] = lv[l].r;
+        c.z[l] = lv[l].z;
+        c.list[l] = list + off[l];
+    }
+    c.counts = counts;
+    return c;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- host side
@@ -1203,7 +1272,16 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_masks() {
         k_level_mask<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(lk(L), L.mask, L.mpitch);
         LHI_LAUNCH_CHECK();
     }
+    if (coarse_level_ < nlev_) {
+        CoarseLists cl{};
+        for (int l = coarse_level_; l < nlev_; ++l) cl.list[l] = coarse_list_ + coarse_list_off_[l];
+        cl.counts = coarse_counts_;
+        k_coarse_lists<T><<<1, 1024, 0, cur_>>>(
+            coarse_levels_of(lv_, nlev_, coarse_level_, coarse_list_, coarse_list_off_, coarse_counts_), cl);
+        LHI_LAUNCH_CHECK();
+    }
 }
+
 
 // Levels that the fused sweep can take: FP32, z extent a multiple of 4 (TMA
 // strides are multiples of 16 bytes) and boxes no larger than the level.
@@ -1308,7 +1386,8 @@ template <class T, class TX> void LiquidImpl<T, TX>::prolong_to(int level) {
 // Bytes of shared memory the coarse kernel needs for levels [first, nlev).
 template <class T> static size_t coarse_bytes(const LevelDev<T>* lv, int first, int nlev) {
     size_t b = 0;
-    for (int l = first; l < nlev; ++l) b += size_t(6) * lv[l].n * sizeof(T) + ((size_t(lv[l].n) + 15) & ~size_t(15));
+    for (int l = first; l < nlev; ++l)
+        b += size_t(6) * lv[l].n * sizeof(T) + ((size_t(lv[l].n) + 15) & ~size_t(15)) + size_t(4) * lv[l].n;
     return b;
 }
 
@@ -1328,6 +1407,16 @@ template <class T, class TX> void LiquidImpl<T, TX>::setup_coarse() {
     }
     LHI_CUDA(cudaFuncSetAttribute(k_coarse_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(kCoarseSmemBytes)));
+    long long nl = 0;
+    for (int l = coarse_level_; l < nlev_; ++l) {
+        coarse_list_off_[l] = nl;
+        nl += lv_[l].n;
+    }
+    if (coarse_level_ < nlev_) {
+        LHI_CUDA(cudaMalloc(&coarse_list_, sizeof(uint32_t) * size_t(std::max(nl, 1LL))));
+        LHI_CUDA(cudaMalloc(&coarse_counts_, sizeof(int) * 2 * kMaxLevels));
+        LHI_CUDA(cudaMemsetAsync(coarse_counts_, 0, sizeof(int) * 2 * kMaxLevels, stream_));
+    }
 }
 
 // CGSolver<3>::ApplyPreconditioner multigrid branch (PressureSolver.cpp:730-771)
@@ -1354,17 +1443,11 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle_levels() {
             smooth(l, sp_.num_pre_smooth);
             restrict_to(l + 1);
         }
-        CoarseLevels<T> c{};
-        c.first = Lc;
-        c.last = last;
-        for (int l = Lc; l <= last; ++l) {
-            c.L[l] = lk(lv_[l]);
-            c.r[l] = lv_[l].r;
-            c.z[l] = lv_[l].z;
-        }
+        const CoarseLevels<T> c =
+            coarse_levels_of(lv_, nlev_, coarse_level_, coarse_list_, coarse_list_off_, coarse_counts_);
         {
             auto ps_ = scope(LHI_KERNEL_SMOOTH_COARSE);
-            k_coarse_cycle<T><<<1, 512, coarse_smem_, cur_>>>(c, T(sp_.smoothing_factor), sp_.smoother,
+            k_coarse_cycle<T><<<1, kCoarseThreads, coarse_smem_, cur_>>>(c, T(sp_.smoothing_factor), sp_.smoother,
                                                                 sp_.num_pre_smooth, sp_.num_post_smooth,
                                                                 sp_.num_final_smooth, &sc_->stop);
             LHI_LAUNCH_CHECK();
