@@ -151,12 +151,18 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
                                     double(radius) * (1.0 + 1e-6);
                         if (double(cur) < lb) continue;
                     }
+                    // the particles of a cell off the grid's outer layer were sorted
+                    // into it by their own unclamped Point2Index: all inside the window
+                    const bool own = wx > 0 && wx < g.nx - 1 && wy > 0 && wy < g.ny - 1 && wz > 0 &&
+                                     wz < g.nz - 1;
                     for (int p = s; p < e; ++p) {
                         T qx = px[p], qy = py[p], qz = pz[p];
-                        int tx = cell_trunc(qx, g.mn[0], g.dx[0]);
-                        int ty = cell_trunc(qy, g.mn[1], g.dx[1]);
-                        int tz = cell_trunc(qz, g.mn[2], g.dx[2]);
-                        if (abs(tx - cx) > d0 || abs(ty - cy) > d1 || abs(tz - cz) > d2) continue;
+                        if (!own) {
+                            int tx = cell_trunc(qx, g.mn[0], g.dx[0]);
+                            int ty = cell_trunc(qy, g.mn[1], g.dx[1]);
+                            int tz = cell_trunc(qz, g.mn[2], g.dx[2]);
+                            if (abs(tx - cx) > d0 || abs(ty - cy) > d1 || abs(tz - cz) > d2) continue;
+                        }
                         T dist = X<T>::sqrt(sqnorm3(X<T>::sub(cpx, qx), X<T>::sub(cpy, qy), X<T>::sub(cpz, qz)));
                         T ph = X<T>::sub(dist, radius);
                         cur = (cur < ph) ? cur : ph;
@@ -492,46 +498,63 @@ template <class T> __device__ void solid_grad_at(const GridP<T>& g, const T* sp,
 }
 
 // Gather of one face component (LiquidModel.cpp:738-761 and its y/z twins).
+// On each axis the window nodes that contribute (offset inside the clipped
+// window, |e| < 1.5, node inside the face grid) are one run of at most 3
+// consecutive nodes; the sum visits that run in the reference's ascending
+// order.  The x.y weight products are formed once per (x, y) pair: the same
+// products as the reference's (wX * wY) * wZ, so every term is bit-identical.
 template <class T, int A>
 __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3], const T g3[3], const int ci[3],
                                               const T* __restrict__ vf, T& velA, T col[3]) {
-    const int hx = g.nx - 1 + (A == 0), hy = g.ny - 1 + (A == 1), hz = g.nz - 1 + (A == 2);
+    const int hmax[3] = {g.nx - 1 + (A == 0), g.ny - 1 + (A == 1), g.nz - 1 + (A == 2)};
     const long long fy = g.ny + (A == 1), fz = g.nz + (A == 2);
-    T ew[3][4], eg[3][4];
-    bool ok[3][4];
+    T ew[3][3], eg[3][3];
+    int first[3], cnt[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        int lo = off_lo(d[i]), hi = off_hi(i, A, d[i]);
+        const int lo = off_lo(d[i]), hi = off_hi(i, A, d[i]);
+        int kb = 4, ke = -1;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            int o = k - 1;
-            int node = ci[i] + o;
-            T c = (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
-            T e = X<T>::sub(g3[i], c);
-            ok[i][k] = (o >= lo && o <= hi && !(fabs(e) >= T(1.5f)));
-            ew[i][k] = ok[i][k] ? qweight(e) : T(0);
-            eg[i][k] = ok[i][k] ? gqweight(e) : T(0);
+            const int o = k - 1;
+            const int node = ci[i] + o;
+            const T c = (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
+            const T e = X<T>::sub(g3[i], c);
+            if (o >= lo && o <= hi && !(fabs(e) >= T(1.5f)) && node >= 0 && node <= hmax[i]) {
+                kb = min(kb, k);
+                ke = k;
+            }
+        }
+        first[i] = ci[i] + kb - 1;
+        cnt[i] = max(ke - kb + 1, 0);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int node = first[i] + j;
+            const T c = (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
+            const T e = X<T>::sub(g3[i], c);
+            ew[i][j] = j < cnt[i] ? qweight(e) : T(0);
+            eg[i][j] = j < cnt[i] ? gqweight(e) : T(0);
         }
     }
-    for (int kx = 0; kx < 4; ++kx) {
-        if (!ok[0][kx]) continue;
-        int xi = ci[0] + kx - 1;
-        if (xi < 0 || xi > hx) continue;
-        for (int ky = 0; ky < 4; ++ky) {
-            if (!ok[1][ky]) continue;
-            int yi = ci[1] + ky - 1;
-            if (yi < 0 || yi > hy) continue;
-            for (int kz = 0; kz < 4; ++kz) {
-                if (!ok[2][kz]) continue;
-                int zi = ci[2] + kz - 1;
-                if (zi < 0 || zi > hz) continue;
-                T wX = ew[0][kx], wY = ew[1][ky], wZ = ew[2][kz];
-                T gX = eg[0][kx], gY = eg[1][ky], gZ = eg[2][kz];
-                T weight = X<T>::mul(X<T>::mul(wX, wY), wZ);
-                T gw0 = X<T>::mul(X<T>::mul(gX, wY), wZ);
-                T gw1 = X<T>::mul(X<T>::mul(wX, gY), wZ);
-                T gw2 = X<T>::mul(X<T>::mul(wX, wY), gZ);
-                T val = vf[((long long)xi * fy + yi) * fz + zi];
+#pragma unroll
+    for (int jx = 0; jx < 3; ++jx) {
+        if (jx >= cnt[0]) break;
+        const T wX = ew[0][jx], gX = eg[0][jx];
+#pragma unroll
+        for (int jy = 0; jy < 3; ++jy) {
+            if (jy >= cnt[1]) break;
+            const T wY = ew[1][jy], gY = eg[1][jy];
+            const T wXY = X<T>::mul(wX, wY), gXwY = X<T>::mul(gX, wY), wXgY = X<T>::mul(wX, gY);
+            const T* row = vf + ((long long)(first[0] + jx) * fy + (first[1] + jy)) * fz + first[2];
+#pragma unroll
+            for (int jz = 0; jz < 3; ++jz) {
+                if (jz >= cnt[2]) break;
+                const T wZ = ew[2][jz], gZ = eg[2][jz];
+                const T weight = X<T>::mul(wXY, wZ);
+                const T gw0 = X<T>::mul(gXwY, wZ);
+                const T gw1 = X<T>::mul(wXgY, wZ);
+                const T gw2 = X<T>::mul(wXY, gZ);
+                const T val = row[jz];
                 velA = X<T>::add(velA, X<T>::mul(val, weight));
                 col[0] = X<T>::add(col[0], X<T>::mul(val, gw0));
                 col[1] = X<T>::add(col[1], X<T>::mul(val, gw1));
