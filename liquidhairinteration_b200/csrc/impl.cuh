@@ -308,6 +308,7 @@ public:
     void setup_coarse();
     void setup_fused();  // second z buffers, masks and tensor maps of the fused sweep
     void build_masks();
+    void setup_spmv();  // tensor maps of the finest level's TMA SpMV
     void enqueue_vcycle();
     void enqueue_vcycle_levels();
     void enqueue_precond();
@@ -369,6 +370,8 @@ public:
     uint32_t* coarse_list_ = nullptr;  // per-colour update lists of the coarse levels
     long long coarse_list_off_[kMaxLevels] = {};
     int* coarse_counts_ = nullptr;
+    bool spmv_tma_ = false;
+    CUtensorMap tm_sp_[6];  // p, diag, cx, cy, cz, mask boxes of the TMA SpMV
     int tile_grid_ = 0;      // persistent CTAs of the tile kernels
     cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on
     cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body

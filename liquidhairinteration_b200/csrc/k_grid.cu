@@ -398,6 +398,7 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     LHI_CUDA(cudaMemsetAsync(x_, 0, sizeof(TX) * ncell_, stream_));
     LHI_CUDA(cudaMemsetAsync(p_, 0, sizeof(T) * ncell_, stream_));
     LHI_CUDA(cudaMemsetAsync(ap_, 0, sizeof(T) * ncell_, stream_));
+    setup_spmv();
     LHI_CUDA(cudaMalloc(&sc_, sizeof(SolveScalars)));
     LHI_CUDA(cudaMemsetAsync(sc_, 0, sizeof(SolveScalars), stream_));
     LHI_CUDA(cudaHostAlloc(&sc_host_, sizeof(SolveScalars), cudaHostAllocDefault));

@@ -294,6 +294,26 @@ template <class F> __device__ __forceinline__ void for_tiles(const TileK& tk, in
     }
 }
 
+// for_tiles with a thread's rows of a work unit handed over together:
+// f(x, z, i0, rows, ys) where row k < rows is cell i0 + k * ys * nz (y
+// ascending).  Kernels load every row before using any, so a thread keeps
+// up to 8 rows of loads in flight; per-thread sums keep for_tiles' order.
+template <class F> __device__ __forceinline__ void for_tile_cols(const TileK& tk, int nx, int ny, int nz, F&& f) {
+    const int units = *tk.count * tk.ysplit;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int t = u / tk.ysplit, sub = u - t * tk.ysplit;
+        const int id = tk.ids[t];
+        const int tz = id % tk.tdz, rest = id / tk.tdz;
+        const int ty = rest % tk.tdy, tx = rest / tk.tdy;
+        const int x = tx * kTileX + w, z = tz * kTileZ + lane;
+        if (x >= nx || z >= nz) continue;
+        const int yb = ty * kTileY + sub, ye = min(ty * kTileY + kTileY, ny);
+        const int rows = yb < ye ? (ye - yb + tk.ysplit - 1) / tk.ysplit : 0;
+        f(x, z, ((long long)x * ny + yb) * nz + z, yb, rows, tk.ysplit);
+    }
+}
+
 struct TileLevels {
     int nlev;
     int tdim[kMaxLevels][3];
@@ -503,7 +523,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             tma_load_box(CYs, &mcy, z0 - 4, y0 - 2, x0 - 1, bar);
             tma_load_box(Ms, &mm, z0 - 16, y0 - 1, x0 - 1, bar);
         }
-        if (!bar_wait(bar, parity)) {
+        if (__syncthreads_or(!bar_wait(bar, parity))) {  // every thread leaves together
             if (threadIdx.x == 0) {
                 sc->timeout = 1;
                 sc->status = LHI_E_TIMEOUT;
@@ -639,9 +659,23 @@ __global__ void __launch_bounds__(kTileThreads) k_prolong_t(int fnx, int fny, in
                                                             int cnx, int cny, int cnz, T* __restrict__ zf,
                                                             const int* __restrict__ stop) {
     if (*stop) return;
-    for_tiles(tk, fnx, fny, fnz, [&](int x, int y, int z, long long i) {
-        const int cx = x >> 1, cy = y >> 1, cz = z >> 1;
-        if (cx < cnx && cy < cny && cz < cnz) zf[i] = zf[i] + zc[((long long)cx * cny + cy) * cnz + cz];
+    for_tile_cols(tk, fnx, fny, fnz, [&](int x, int z, long long i0, int yb, int rows, int ys) {
+        const long long st = (long long)ys * fnz;
+        const int cx = x >> 1, cz = z >> 1;
+        bool on[kTileY];
+        T fv[kTileY], cv[kTileY];
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k) {
+            const int cy = (yb + k * ys) >> 1;
+            on[k] = k < rows && cx < cnx && cy < cny && cz < cnz;
+            if (on[k]) {
+                fv[k] = zf[i0 + k * st];
+                cv[k] = zc[((long long)cx * cny + cy) * cnz + cz];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            if (on[k]) zf[i0 + k * st] = fv[k] + cv[k];
     });
 }
 
@@ -921,6 +955,103 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK t
     if (cf.use_cond) cudaGraphSetConditional(cf.cond, stop ? 0u : 1u);
 }
 
+// ------------------------------------------------- TMA-staged SpMV
+// Ap = A p with p.Ap for the finest level, one 8 x 8 x 32 tile per step: p
+// grown by one cell in x and y (z from z0-4), diag, the coefficients with
+// the -x / -y / -z neighbours' faces, and the neighbour mask staged by TMA.
+// A thread owns (x0 + warp, z0 + lane) and the tile's 8 rows, as k_cg_spmv,
+// and sums p.Ap in the same order.
+namespace sp {
+constexpr int kP = 10 * 10 * 40, kD = 8 * 8 * 32, kCX = 9 * 8 * 32, kCY = 8 * 9 * 32, kCZ = 8 * 8 * 36, kM = kD;
+constexpr uint32_t kTx = uint32_t((kP + kD + kCX + kCY + kCZ) * 4 + kM);
+constexpr int oP = 128, oD = oP + kP * 4, oCX = oD + kD * 4, oCY = oCX + kCX * 4, oCZ = oCY + kCY * 4,
+              oM = oCZ + kCZ * 4, kSmem = oM + kM;
+static_assert(kP * 4 % 128 == 0 && kCX * 4 % 128 == 0 && kCZ * 4 % 128 == 0, "128-byte aligned boxes");
+}  // namespace sp
+
+__global__ void __launch_bounds__(kTileThreads, 4)
+    k_spmv_tma(const __grid_constant__ CUtensorMap mp, const __grid_constant__ CUtensorMap md,
+               const __grid_constant__ CUtensorMap mcx, const __grid_constant__ CUtensorMap mcy,
+               const __grid_constant__ CUtensorMap mcz, const __grid_constant__ CUtensorMap mm, int nx, int ny, int nz,
+               const int32_t* __restrict__ ids, const int* __restrict__ count, int tdy, int tdz, float* __restrict__ ap,
+               double* __restrict__ partials, unsigned* __restrict__ counter, SolveScalars* __restrict__ sc,
+               CgConf cf) {
+    if (sc->stop) return;
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    const float* Ps = reinterpret_cast<const float*>(sm + sp::oP);
+    const float* Ds = reinterpret_cast<const float*>(sm + sp::oD);
+    const float* CXs = reinterpret_cast<const float*>(sm + sp::oCX);
+    const float* CYs = reinterpret_cast<const float*>(sm + sp::oCY);
+    const float* CZs = reinterpret_cast<const float*>(sm + sp::oCZ);
+    const uint8_t* Ms = sm + sp::oM;
+    if (threadIdx.x == 0) bar_init(bar, 1);
+    __syncthreads();
+    double v[1] = {0.0};
+    const int units = *count;
+    const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned parity = 0;
+    bool failed = false;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int id = ids[u];
+        const int tz = id % tdz, rest = id / tdz;
+        const int ty = rest % tdy, tx = rest / tdy;
+        const int x0 = tx * kTileX, y0 = ty * kTileY, z0 = tz * kTileZ;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            bar_expect_tx(bar, sp::kTx);
+            tma_load_box(sm + sp::oP, &mp, z0 - 4, y0 - 1, x0 - 1, bar);
+            tma_load_box(sm + sp::oD, &md, z0, y0, x0, bar);
+            tma_load_box(sm + sp::oCX, &mcx, z0, y0, x0 - 1, bar);
+            tma_load_box(sm + sp::oCY, &mcy, z0, y0 - 1, x0, bar);
+            tma_load_box(sm + sp::oCZ, &mcz, z0 - 4, y0, x0, bar);
+            tma_load_box(sm + sp::oM, &mm, z0, y0, x0, bar);
+        }
+        if (__syncthreads_or(!bar_wait(bar, parity))) {  // every thread leaves together
+            failed = true;
+            break;
+        }
+        parity ^= 1u;
+        const int x = x0 + wp, zz = z0 + lane;
+        if (x < nx && zz < nz) {
+#pragma unroll
+            for (int ly = 0; ly < kTileY; ++ly) {
+                const int y = y0 + ly;
+                if (y >= ny) break;
+                const int pi = ((wp + 1) * 10 + (ly + 1)) * 40 + (lane + 4);
+                const int ci = (wp * 8 + ly) * 32 + lane;
+                const unsigned m = Ms[ci];
+                const float pc = Ps[pi];
+                float a = 0.f;
+                if (m & 64u) {
+                    a = pc * Ds[ci];
+                    if (m & 1u) a += Ps[pi + 400] * CXs[ci + 256];
+                    if (m & 2u) a += Ps[pi - 400] * CXs[ci];
+                    if (m & 4u) a += Ps[pi + 40] * CYs[(wp * 9 + ly + 1) * 32 + lane];
+                    if (m & 8u) a += Ps[pi - 40] * CYs[(wp * 9 + ly) * 32 + lane];
+                    if (m & 16u) a += Ps[pi + 1] * CZs[(wp * 8 + ly) * 36 + lane + 4];
+                    if (m & 32u) a += Ps[pi - 1] * CZs[(wp * 8 + ly) * 36 + lane + 3];
+                }
+                ap[((long long)x * ny + y) * nz + zz] = a;
+                if ((m & 64u) && in_region(x, y, zz, nx, ny, nz, cf.region)) v[0] += double(pc) * double(a);
+            }
+        }
+        __syncthreads();
+    }
+    if (failed) {
+        if (threadIdx.x == 0) {
+            sc->timeout = 1;
+            sc->status = LHI_E_TIMEOUT;
+            sc->stop = 1;
+        }
+        // the CTA still takes part in the grid-wide sum below
+    }
+    double tot[1];
+    if (!grid_sum_last<1>(v, partials, counter, tot)) return;
+    sc->denom = tot[0];
+    sc->alpha = sc->rz_old / tot[0];
+}
+
 // Ap = A p; p.Ap over the update region; alpha = rz / p.Ap (PressureSolver.cpp:873-888).
 // A thread owns (x, z) of a tile and 8 rows, loaded 4 rows at a time.
 template <class T>
@@ -980,12 +1111,30 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_update_xr(LevelK<T> L, Tile
     if (sc->stop) return;
     const double alpha = sc->alpha;
     double v[1] = {0.0};
-    for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zi, long long i) {
-        if (L.type[i] == 0 || !in_region(xi, yi, zi, L.nx, L.ny, L.nz, cf.region)) return;
-        x[i] = TX(double(x[i]) + alpha * double(p[i]));
-        const T rn = T(double(r[i]) - alpha * double(ap[i]));
-        r[i] = rn;
-        v[0] += double(rn) * double(rn);
+    for_tile_cols(tk, L.nx, L.ny, L.nz, [&](int xi, int zi, long long i0, int yb, int rows, int ys) {
+        const long long st = (long long)ys * L.nz;
+        bool on[kTileY];
+        TX xv[kTileY];
+        T pv[kTileY], rv[kTileY], av[kTileY];
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            on[k] = k < rows && L.type[i0 + k * st] != 0 && in_region(xi, yb + k * ys, zi, L.nx, L.ny, L.nz, cf.region);
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            if (on[k]) {
+                xv[k] = x[i0 + k * st];
+                pv[k] = p[i0 + k * st];
+                rv[k] = r[i0 + k * st];
+                av[k] = ap[i0 + k * st];
+            }
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            if (on[k]) {
+                x[i0 + k * st] = TX(double(xv[k]) + alpha * double(pv[k]));
+                const T rn = T(double(rv[k]) - alpha * double(av[k]));
+                r[i0 + k * st] = rn;
+                v[0] += double(rn) * double(rn);
+            }
     });
     double tot[1];
     if (!grid_sum_last<1>(v, partials, counter, tot)) return;
@@ -1043,10 +1192,27 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_dot_rz(LevelK<T> L, TileK t
                                                             SolveScalars* __restrict__ sc, CgConf cf) {
     if (sc->stop) return;
     double v[2] = {0.0, 0.0};
-    for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zz, long long i) {
-        const T zi = z[i];
-        v[0] += double(r[i]) * double(zi);
-        if (L.type[i] != 0 && in_region(xi, yi, zz, L.nx, L.ny, L.nz, cf.region)) v[1] += double(ap[i]) * double(zi);
+    for_tile_cols(tk, L.nx, L.ny, L.nz, [&](int xi, int zz, long long i0, int yb, int rows, int ys) {
+        const long long st = (long long)ys * L.nz;
+        bool on[kTileY];
+        T zv[kTileY], rv[kTileY], av[kTileY];
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k) {
+            on[k] = k < rows && L.type[i0 + k * st] != 0 && in_region(xi, yb + k * ys, zz, L.nx, L.ny, L.nz, cf.region);
+            if (k < rows) {
+                zv[k] = z[i0 + k * st];
+                rv[k] = r[i0 + k * st];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            if (on[k]) av[k] = ap[i0 + k * st];
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k) {
+            if (k >= rows) break;
+            v[0] += double(rv[k]) * double(zv[k]);
+            if (on[k]) v[1] += double(av[k]) * double(zv[k]);
+        }
     });
     double tot[2];
     if (!grid_sum_last<2>(v, partials, counter, tot)) return;
@@ -1063,8 +1229,21 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_update_p(LevelK<T> L, TileK
                                                               T* __restrict__ p, const SolveScalars* __restrict__ sc) {
     if (sc->stop) return;
     const double beta = sc->beta;
-    for_tiles(tk, L.nx, L.ny, L.nz, [&](int x, int y, int zz, long long i) {
-        if (L.type[i] != 0) p[i] = T(double(z[i]) + beta * double(p[i]));
+    for_tile_cols(tk, L.nx, L.ny, L.nz, [&](int x, int zz, long long i0, int yb, int rows, int ys) {
+        const long long st = (long long)ys * L.nz;
+        bool on[kTileY];
+        T zv[kTileY], pv[kTileY];
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k) on[k] = k < rows && L.type[i0 + k * st] != 0;
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            if (on[k]) {
+                zv[k] = z[i0 + k * st];
+                pv[k] = p[i0 + k * st];
+            }
+#pragma unroll
+        for (int k = 0; k < kTileY; ++k)
+            if (on[k]) p[i0 + k * st] = T(double(zv[k]) + beta * double(pv[k]));
     });
 }
 
@@ -1312,6 +1491,23 @@ template <class T, class TX> void LiquidImpl<T, TX>::setup_fused() {
     }
 }
 
+// Tensor maps of the finest level's TMA SpMV (on the CG direction p).
+template <class T, class TX> void LiquidImpl<T, TX>::setup_spmv() {
+    if constexpr (std::is_same<T, float>::value) {
+        LevelDev<T>& L = lv_[0];
+        if (!L.fused) return;
+        LHI_CUDA(cudaFuncSetAttribute(k_spmv_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, sp::kSmem));
+        const auto F32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        tm_sp_[0] = make_box_map(p_, F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 10, 40);
+        tm_sp_[1] = make_box_map(L.diag, F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 8, 32);
+        tm_sp_[2] = make_box_map(L.cf[0], F32, 4, L.nx, L.ny, L.nz, L.nz, 9, 8, 32);
+        tm_sp_[3] = make_box_map(L.cf[1], F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 9, 32);
+        tm_sp_[4] = make_box_map(L.cf[2], F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 8, 36);
+        tm_sp_[5] = make_box_map(L.mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.nx, L.ny, L.nz, L.mpitch, 8, 8, 32);
+        spmv_tma_ = true;
+    }
+}
+
 template <class T, class TX> void LiquidImpl<T, TX>::build_tiles() {
     TileLevels tl{};
     tl.nlev = 0;
@@ -1549,7 +1745,13 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_body(unsigned long 
     const CgConf cf = make_conf(sp_, cond, use_cond);
     {
         auto ps_ = scope(LHI_KERNEL_SPMV);
-        k_cg_spmv<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, p_, ap_, partials_, counter_, sc_, cf);
+        if (spmv_tma_ && sp_.sweep_kernel == LHI_SWEEP_FUSED)
+            k_spmv_tma<<<G, kTileThreads, sp::kSmem, cur_>>>(
+                tm_sp_[0], tm_sp_[1], tm_sp_[2], tm_sp_[3], tm_sp_[4], tm_sp_[5], L0.nx, L0.ny, L0.nz, L0.tiles,
+                &sc_->tile_count[0], L0.tdim[1], L0.tdim[2], reinterpret_cast<float*>(ap_), partials_, counter_, sc_,
+                cf);
+        else
+            k_cg_spmv<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, p_, ap_, partials_, counter_, sc_, cf);
         LHI_LAUNCH_CHECK();
     }
     {

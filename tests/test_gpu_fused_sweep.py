@@ -1,11 +1,11 @@
 """The fused red-black sweep (both colours in one pass over TMA-staged
-tiles, into a second solution buffer) against the two-launch sweep and the
-oracle.
+tiles, into a second solution buffer) and the TMA-staged SpMV against the
+two-launch sweep, the row-batched SpMV and the oracle.
 
 Every cell update of the fused kernel is the same arithmetic, in the same
 order, on the same values as the two in-place colour launches, so V-cycles
-and whole pressure solves agree bit for bit; odd sweep counts exercise the
-copy back into the level's solution buffer.  The fused kernel takes levels
+agree bit for bit; odd sweep counts exercise the copy back into the level's
+solution buffer.  Whole solves agree to the last bits of the p.Ap sums.  The fused kernel takes levels
 whose z extent is at least 64, so the scenes here are 64^3 and 128^3.
 """
 import numpy as np
@@ -99,8 +99,11 @@ def test_fused_solve_matches_split(lhi, state64, prec):
         assert st2["iterations"] == st["iterations"] and st2["status"] == st["status"], (st, st2)
         out.append((st["status"], st["iterations"], g.field("pressure")))
         g.close()
-    assert out[0][:2] == out[1][:2]
-    assert_bitwise(out[1][2], out[0][2], "pressure")
+    # LHI_SWEEP_FUSED also selects the TMA SpMV, which sums p.Ap over whole
+    # tiles per CTA; the split path's SpMV spreads a small grid's tile rows
+    # over several CTAs, so alpha can differ in its last bits
+    assert out[0][0] == out[1][0] and abs(out[0][1] - out[1][1]) <= 1
+    assert rel_l2(out[1][2], out[0][2]) < 1e-6
 
 
 def test_fused_vcycle_close_to_oracle(oracle_mod, lhi):
