@@ -43,6 +43,15 @@ struct CudaError : std::runtime_error {
 
 constexpr int kSMs = 148;
 
+// (x, y, z) of entry i of an [..][ny][nz] array (z fastest), in 32-bit
+// arithmetic: every grid and face array has fewer than 2^32 entries.
+__device__ __forceinline__ void idx3(long long i, int ny, int nz, int& x, int& y, int& z) {
+    const unsigned u = unsigned(i), t = u / unsigned(nz);
+    z = int(u - t * unsigned(nz));
+    y = int(t % unsigned(ny));
+    x = int(t / unsigned(ny));
+}
+
 inline unsigned blocks_for(long long n, int threads) {
     long long b = (n + threads - 1) / threads;
     if (b < 1) b = 1;

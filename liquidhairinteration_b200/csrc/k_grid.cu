@@ -27,7 +27,8 @@ template <class T> __global__ void k_boundary(BoundaryProgram prog, G3<T> g, T* 
     const int fy = g.ny + 1, fz = g.nz + 1;
     long long n = (long long)(g.nx + 1) * fy * fz;
     if (i >= n) return;
-    int zi = int(i % fz), yi = int((i / fz) % fy), xi = int(i / ((long long)fy * fz));
+    int xi, yi, zi;
+    idx3(i, fy, fz, xi, yi, zi);
     T p[3] = {X<T>::add(X<T>::mul(T(xi), g.dx[0]), g.mn[0]), X<T>::add(X<T>::mul(T(yi), g.dx[1]), g.mn[1]),
               X<T>::add(X<T>::mul(T(zi), g.dx[2]), g.mn[2])};
     T val[kMaxBoundaryNodes];
@@ -66,7 +67,8 @@ __global__ void k_face_fractions(const T* __restrict__ sp, int nx, int ny, int n
     const int fx = nx + (comp == 0), fy = ny + (comp == 1), fz = nz + (comp == 2);
     long long n = (long long)fx * fy * fz;
     if (i >= n) return;
-    int zi = int(i % fz), yi = int((i / fz) % fy), xi = int(i / ((long long)fy * fz));
+    int xi, yi, zi;
+    idx3(i, fy, fz, xi, yi, zi);
     const long long sy = nz + 1, sx = (long long)(ny + 1) * (nz + 1);
     long long a = xi * sx + yi * sy + zi;
     long long b = (comp == 0) ? a + sy : a + sx;
@@ -79,7 +81,8 @@ template <class T> __global__ void k_gravity(T* __restrict__ vy, int nx, int ny,
     const int fy = ny + 1;
     long long n = (long long)nx * fy * nz;
     if (i >= n) return;
-    int z = int(i % nz), y = int((i / nz) % fy), x = int(i / ((long long)fy * nz));
+    int x, y, z;
+    idx3(i, fy, nz, x, y, z);
     if (x >= 1 && x < nx - 1 && y >= 1 && y < ny && z >= 1 && z < nz - 1) vy[i] = X<T>::add(vy[i], gdt);
 }
 
@@ -157,27 +160,36 @@ struct ExtRange {
     int ny1, nz1;                // isValid extents (ny+1, nz+1)
 };
 
+// Face (x, y, z) of this thread inside the range (32-bit index arithmetic:
+// every face array has fewer than 2^31 entries).
+__device__ __forceinline__ bool ext_cell(const ExtRange& r, int& x, int& y, int& z) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ey = r.y1 - r.y0 + 1, ez = r.z1 - r.z0 + 1;
+    if (ey <= 0 || ez <= 0 || i >= unsigned(r.x1 - r.x0 + 1) * unsigned(ey) * unsigned(ez)) return false;
+    const unsigned t = i / unsigned(ez);
+    z = r.z0 + int(i - t * unsigned(ez));
+    y = r.y0 + int(t % unsigned(ey));
+    x = r.x0 + int(t / unsigned(ey));
+    return true;
+}
+
 template <class T> __global__ void k_extrap_init(ExtRange r, const T* __restrict__ lw, uint8_t* __restrict__ valid) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int ey = r.y1 - r.y0 + 1, ez = r.z1 - r.z0 + 1;
-    long long n = (long long)(r.x1 - r.x0 + 1) * ey * ez;
-    if (i >= n || ey <= 0 || ez <= 0) return;
-    int z = r.z0 + int(i % ez), y = r.y0 + int((i / ez) % ey), x = r.x0 + int(i / ((long long)ey * ez));
+    int x, y, z;
+    if (!ext_cell(r, x, y, z)) return;
     long long f = ((long long)x * r.fy + y) * r.fz + z;
     valid[((long long)x * r.ny1 + y) * r.nz1 + z] = (lw[f] > T(0)) ? 0 : 255;
 }
 
+// With t == v the sweep runs in place: it writes only faces that were not
+// valid before sweep k, and it reads only faces that were, so the values
+// equal those of the sweep into a separate buffer.
 template <class T>
-__global__ void k_extrap_sweep(ExtRange r, int k, const T* __restrict__ v, T* __restrict__ t,
-                               uint8_t* __restrict__ valid) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int ey = r.y1 - r.y0 + 1, ez = r.z1 - r.z0 + 1;
-    long long n = (long long)(r.x1 - r.x0 + 1) * ey * ez;
-    if (i >= n || ey <= 0 || ez <= 0) return;
-    int z = r.z0 + int(i % ez), y = r.y0 + int((i / ez) % ey), x = r.x0 + int(i / ((long long)ey * ez));
+__global__ void k_extrap_sweep(ExtRange r, int k, const T* v, T* t, uint8_t* __restrict__ valid) {
+    int x, y, z;
+    if (!ext_cell(r, x, y, z)) return;
     long long f = ((long long)x * r.fy + y) * r.fz + z;
     long long vi = ((long long)x * r.ny1 + y) * r.nz1 + z;
-    t[f] = v[f];
+    if (t != v) t[f] = v[f];
     if (valid[vi] <= k) return;
     T sum = T(0);
     int count = 0;
@@ -197,11 +209,8 @@ __global__ void k_extrap_sweep(ExtRange r, int k, const T* __restrict__ v, T* __
 }
 
 __global__ void k_extrap_finish(ExtRange r, uint8_t* __restrict__ valid) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int ey = r.y1 - r.y0 + 1, ez = r.z1 - r.z0 + 1;
-    long long n = (long long)(r.x1 - r.x0 + 1) * ey * ez;
-    if (i >= n || ey <= 0 || ez <= 0) return;
-    int z = r.z0 + int(i % ez), y = r.y0 + int((i / ez) % ey), x = r.x0 + int(i / ((long long)ey * ez));
+    int x, y, z;
+    if (!ext_cell(r, x, y, z)) return;
     long long vi = ((long long)x * r.ny1 + y) * r.nz1 + z;
     uint8_t v = valid[vi];
     valid[vi] = (v == 255) ? 255 : 0;
@@ -218,7 +227,8 @@ __global__ void k_divergence(int nx, int ny, int nz, T h, const T* __restrict__ 
     long long n = (long long)nx * ny * nz;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         if (phi[c] > T(0)) continue;
-        int z = int(c % nz), y = int((c / nz) % ny), x = int(c / ((long long)ny * nz));
+        int x, y, z;
+        idx3(c, ny, nz, x, y, z);
         long long fxi = ((long long)x * ny + y) * nz + z, fxs = (long long)ny * nz;
         long long fyi = ((long long)x * (ny + 1) + y) * nz + z, fys = nz;
         long long fzi = ((long long)x * ny + y) * (nz + 1) + z;
@@ -242,7 +252,8 @@ __global__ void k_divergence_max(int nx, int ny, int nz, T h, const T* __restric
     long long n = (long long)nx * ny * nz;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         if (phi[c] > T(0)) continue;
-        int z = int(c % nz), y = int((c / nz) % ny), x = int(c / ((long long)ny * nz));
+        int x, y, z;
+        idx3(c, ny, nz, x, y, z);
         // only cells whose six faces the velocity update touches: [1, N-3]^3
         if (x < 1 || x > nx - 3 || y < 1 || y > ny - 3 || z < 1 || z > nz - 3) continue;
         long long fxi = ((long long)x * ny + y) * nz + z, fxs = (long long)ny * nz;
@@ -554,12 +565,21 @@ template <class T, class TX> void LiquidImpl<T, TX>::extrapolate() {
             k_extrap_init<T><<<blocks_for(n, 256), 256, 0, stream_>>>(r, lw_[a], valid_);
             LHI_LAUNCH_CHECK();
         }
+        // The reference sweeps into tempV and swaps (std::swap(m_grid.tempVx,
+        // m_grid.vx)) after every sweep.  The first sweeps run in place on vx;
+        // the last one (odd count) or two (even count) go through tempV with
+        // the swaps, which leaves vx and tempVx holding the reference's last
+        // two states in the reference's buffers (faces outside the range keep
+        // each buffer's own values).
+        const int jacobi_from = extrap_iters_ - ((extrap_iters_ % 2) ? 1 : 2);
         for (int k = 0; k < extrap_iters_; ++k) {
+            const bool swap = k >= jacobi_from;
             if (n > 0) {
-                k_extrap_sweep<T><<<blocks_for(n, 256), 256, 0, stream_>>>(r, k, v_[a], tv_[a], valid_);
+                k_extrap_sweep<T><<<blocks_for(n, 256), 256, 0, stream_>>>(r, k, v_[a], swap ? tv_[a] : v_[a],
+                                                                         valid_);
                 LHI_LAUNCH_CHECK();
             }
-            std::swap(v_[a], tv_[a]);  // std::swap(m_grid.tempVx, m_grid.vx)
+            if (swap) std::swap(v_[a], tv_[a]);
         }
         if (n > 0) {
             k_extrap_finish<<<blocks_for(n, 256), 256, 0, stream_>>>(r, valid_);

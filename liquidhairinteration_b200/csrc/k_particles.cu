@@ -62,7 +62,8 @@ __global__ void k_occupancy(const int32_t* __restrict__ cs, int nx, int ny, int 
     long long nc = (long long)nx * ny * nz;
     if (c >= nc) return;
     if (cs[c + 1] == cs[c]) return;
-    int z = int(c % nz), y = int((c / nz) % ny), x = int(c / ((long long)ny * nz));
+    int x, y, z;
+    idx3(c, ny, nz, x, y, z);
     occ[((long long)(x >> 2) * oy + (y >> 2)) * oz + (z >> 2)] = 1;
 }
 
@@ -109,7 +110,8 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long nc = (long long)g.nx * g.ny * g.nz;
     if (c >= nc) return;
-    int cz = int(c % g.nz), cy = int((c / g.nz) % g.ny), cx = int(c / ((long long)g.ny * g.nz));
+    int cx, cy, cz;
+    idx3(c, g.ny, g.nz, cx, cy, cz);
     int x0 = max(0, cx - d0), x1 = min(g.nx - 1, cx + d0);
     int y0 = max(0, cy - d1), y1 = min(g.ny - 1, cy + d1);
     int z0 = max(0, cz - d2), z1 = min(g.nz - 1, cz + d2);
@@ -400,7 +402,8 @@ __global__ void k_p2g_normalize(T* __restrict__ v, const T* __restrict__ w, int 
     T wv = w[i];
     T r = !is_small(wv) ? X<T>::div(v[i], wv) : T(0);
     if (gravity) {
-        int z = int(i % fz), y = int((i / fz) % fy), x = int(i / ((long long)fy * fz));
+        int x, y, z;
+        idx3(i, fy, fz, x, y, z);
         if (x >= 1 && x < nx - 1 && y >= 1 && y < ny && z >= 1 && z < nz - 1) r = X<T>::add(r, gdt);
     }
     v[i] = r;

@@ -49,12 +49,7 @@ template <class T> LevelK<T> lk(const LevelDev<T>& L) {
     return LevelK<T>{L.nx, L.ny, L.nz, L.diag, L.cf[0], L.cf[1], L.cf[2], L.type};
 }
 
-__device__ __forceinline__ void decode(long long i, int ny, int nz, int& x, int& y, int& z) {
-    z = int(i % nz);
-    long long t = i / nz;
-    y = int(t % ny);
-    x = int(t / ny);
-}
+__device__ __forceinline__ void decode(long long i, int ny, int nz, int& x, int& y, int& z) { idx3(i, ny, nz, x, y, z); }
 
 // CGSolver<3>::GetAx (PressureSolver.cpp:700-717), computed in C
 template <class C, class T, class V>
