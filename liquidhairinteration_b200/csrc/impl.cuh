@@ -94,6 +94,9 @@ template <class T> struct LevelDev {
     uint8_t* mask = nullptr;                 // neighbour mask per cell, [nx][ny][mpitch]
     int mpitch = 0;
     CUtensorMap tm_z, tm_zb, tm_r, tm_d, tm_cx, tm_cy, tm_cz, tm_m;
+    // one-tile boxes of the TMA restriction: z (and zb) grown by one cell,
+    // r, diag, the coefficients with the -x / -y / -z faces, the mask
+    CUtensorMap ts_z, ts_zb, ts_r, ts_d, ts_cx, ts_cy, ts_cz, ts_m;
 };
 
 // Optional per-category device timing: CUDA events on the handle's stream

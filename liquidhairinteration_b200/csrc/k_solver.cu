@@ -440,14 +440,18 @@ constexpr int kMW = 64;
 constexpr int kM = 10 * 10 * kMW;
 constexpr uint32_t kTx = uint32_t((kZ + 3 * kR + 2 * kC) * 4 + kM);  // bytes the 7 boxes deliver
 constexpr int al(int b) { return (b + 127) & ~127; }
-constexpr int oZ = 128;
+// offsets inside one stage
+constexpr int oZ = 0;
 constexpr int oR = oZ + al(kZ * 4);
 constexpr int oD = oR + al(kR * 4);
 constexpr int oCZ = oD + al(kR * 4);
 constexpr int oCX = oCZ + al(kR * 4);
 constexpr int oCY = oCX + al(kC * 4);
 constexpr int oM = oCY + al(kC * 4);
-constexpr int kSmem = oM + al(kM);
+constexpr int kStage = oM + al(kM);
+constexpr int kBase = 128;  // two mbarriers, then two stages
+constexpr int kSmem = kBase + 2 * kStage;
+constexpr int kThreads = 512;
 }  // namespace rb
 
 // Mask bits of a cell: 0..5 neighbour +x, -x, +y, -y, +z, -z exists with phi < 0;
@@ -481,7 +485,33 @@ __device__ __forceinline__ void rb_cell(float* __restrict__ Zs, const float* __r
     Zs[zi] = out;
 }
 
-__global__ void __launch_bounds__(kTileThreads, 2)
+// Tile id u of the active list -> origin of its 8 x 8 x 32 cells.
+__device__ __forceinline__ void tile_origin(const int32_t* __restrict__ ids, int u, int tdy, int tdz, int& x0, int& y0,
+                                            int& z0) {
+    const int id = ids[u];
+    const int tz = id % tdz, rest = id / tdz;
+    z0 = tz * kTileZ;
+    y0 = (rest % tdy) * kTileY;
+    x0 = (rest / tdy) * kTileX;
+}
+
+__device__ __forceinline__ void rb_issue(unsigned char* st, uint64_t* bar, const CUtensorMap* mz, const CUtensorMap* mr,
+                                         const CUtensorMap* md, const CUtensorMap* mcx, const CUtensorMap* mcy,
+                                         const CUtensorMap* mcz, const CUtensorMap* mm, int x0, int y0, int z0) {
+    fence_proxy_async();
+    bar_expect_tx(bar, rb::kTx);
+    tma_load_box(st + rb::oZ, mz, z0 - 4, y0 - 2, x0 - 2, bar);
+    tma_load_box(st + rb::oR, mr, z0 - 4, y0 - 1, x0 - 1, bar);
+    tma_load_box(st + rb::oD, md, z0 - 4, y0 - 1, x0 - 1, bar);
+    tma_load_box(st + rb::oCZ, mcz, z0 - 4, y0 - 1, x0 - 1, bar);
+    tma_load_box(st + rb::oCX, mcx, z0 - 4, y0 - 1, x0 - 2, bar);
+    tma_load_box(st + rb::oCY, mcy, z0 - 4, y0 - 2, x0 - 1, bar);
+    tma_load_box(st + rb::oM, mm, z0 - 16, y0 - 1, x0 - 1, bar);
+}
+
+// One CTA per SM walks its tiles through two shared-memory stages: the
+// boxes of the next tile are in flight while the current one is smoothed.
+__global__ void __launch_bounds__(rb::kThreads, 1)
     k_rb_fused(const __grid_constant__ CUtensorMap mz, const __grid_constant__ CUtensorMap mr,
                const __grid_constant__ CUtensorMap md, const __grid_constant__ CUtensorMap mcx,
                const __grid_constant__ CUtensorMap mcy, const __grid_constant__ CUtensorMap mcz,
@@ -491,44 +521,48 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     if (sc->stop) return;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-    float* Zs = reinterpret_cast<float*>(sm + rb::oZ);
-    float* Rs = reinterpret_cast<float*>(sm + rb::oR);
-    float* Ds = reinterpret_cast<float*>(sm + rb::oD);
-    float* CZs = reinterpret_cast<float*>(sm + rb::oCZ);
-    float* CXs = reinterpret_cast<float*>(sm + rb::oCX);
-    float* CYs = reinterpret_cast<float*>(sm + rb::oCY);
-    uint8_t* Ms = sm + rb::oM;
-    if (threadIdx.x == 0) bar_init(bar, 1);
+    if (threadIdx.x == 0) {
+        bar_init(&bar[0], 1);
+        bar_init(&bar[1], 1);
+    }
     __syncthreads();
     const int units = *count;
-    unsigned parity = 0;
-    for (int u = blockIdx.x; u < units; u += gridDim.x) {
-        const int id = ids[u];
-        const int tz = id % tdz, rest = id / tdz;
-        const int ty = rest % tdy, tx = rest / tdy;
-        const int x0 = tx * kTileX, y0 = ty * kTileY, z0 = tz * kTileZ;
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            bar_expect_tx(bar, rb::kTx);
-            tma_load_box(Zs, &mz, z0 - 4, y0 - 2, x0 - 2, bar);
-            tma_load_box(Rs, &mr, z0 - 4, y0 - 1, x0 - 1, bar);
-            tma_load_box(Ds, &md, z0 - 4, y0 - 1, x0 - 1, bar);
-            tma_load_box(CZs, &mcz, z0 - 4, y0 - 1, x0 - 1, bar);
-            tma_load_box(CXs, &mcx, z0 - 4, y0 - 1, x0 - 2, bar);
-            tma_load_box(CYs, &mcy, z0 - 4, y0 - 2, x0 - 1, bar);
-            tma_load_box(Ms, &mm, z0 - 16, y0 - 1, x0 - 1, bar);
+    if (threadIdx.x == 0 && int(blockIdx.x) < units) {
+        int a, b, c;
+        tile_origin(ids, blockIdx.x, tdy, tdz, a, b, c);
+        rb_issue(sm + rb::kBase, &bar[0], &mz, &mr, &md, &mcx, &mcy, &mcz, &mm, a, b, c);
+    }
+    int it = 0;
+    for (int u = blockIdx.x; u < units; u += gridDim.x, ++it) {
+        const int s = it & 1;
+        unsigned char* st = sm + rb::kBase + s * rb::kStage;
+        int x0, y0, z0;
+        tile_origin(ids, u, tdy, tdz, x0, y0, z0);
+        const int un = u + int(gridDim.x);
+        if (threadIdx.x == 0 && un < units) {  // the other stage was released by the last barrier
+            int a, b, c;
+            tile_origin(ids, un, tdy, tdz, a, b, c);
+            rb_issue(sm + rb::kBase + (s ^ 1) * rb::kStage, &bar[s ^ 1], &mz, &mr, &md, &mcx, &mcy, &mcz, &mm, a, b,
+                     c);
         }
-        if (__syncthreads_or(!bar_wait(bar, parity))) {  // every thread leaves together
+        if (__syncthreads_or(!bar_wait(&bar[s], (it >> 1) & 1))) {  // every thread leaves together
             if (threadIdx.x == 0) {
                 sc->timeout = 1;
                 sc->status = LHI_E_TIMEOUT;
                 sc->stop = 1;
+                if (un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);  // the prefetch, bounded too
             }
             return;
         }
-        parity ^= 1u;
+        float* Zs = reinterpret_cast<float*>(st + rb::oZ);
+        const float* Rs = reinterpret_cast<const float*>(st + rb::oR);
+        const float* Ds = reinterpret_cast<const float*>(st + rb::oD);
+        const float* CZs = reinterpret_cast<const float*>(st + rb::oCZ);
+        const float* CXs = reinterpret_cast<const float*>(st + rb::oCX);
+        const float* CYs = reinterpret_cast<const float*>(st + rb::oCY);
+        const uint8_t* Ms = st + rb::oM;
         // colour 0 ((x + y + z) even) on T grown by one cell: 10 x 10 rows of 17
-        for (int q = threadIdx.x; q < 100 * 17; q += kTileThreads) {
+        for (int q = threadIdx.x; q < 100 * 17; q += rb::kThreads) {
             const int row = q / 17, k = q - row * 17;
             const int lx = row / 10 - 1, ly = row - (row / 10) * 10 - 1;
             const int lz = ((x0 + lx + y0 + ly + z0 - 1) & 1) - 1 + 2 * k;
@@ -536,14 +570,14 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         }
         __syncthreads();
         // colour 1 on T: 8 x 8 rows of 16
-        for (int q = threadIdx.x; q < 64 * 16; q += kTileThreads) {
+        for (int q = threadIdx.x; q < 64 * 16; q += rb::kThreads) {
             const int row = q >> 4, k = q & 15;
             const int lx = row >> 3, ly = row & 7;
             const int lz = ((x0 + lx + y0 + ly + z0 + 1) & 1) + 2 * k;
             rb_cell(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant);
         }
         __syncthreads();
-        for (int q = threadIdx.x; q < 64 * 8; q += kTileThreads) {
+        for (int q = threadIdx.x; q < 64 * 8; q += rb::kThreads) {
             const int row = q >> 3, c = q & 7;
             const int lx = row >> 3, ly = row & 7;
             const int x = x0 + lx, y = y0 + ly, z = z0 + 4 * c;
@@ -954,17 +988,36 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK t
 // Ap = A p with p.Ap for the finest level, one 8 x 8 x 32 tile per step: p
 // grown by one cell in x and y (z from z0-4), diag, the coefficients with
 // the -x / -y / -z neighbours' faces, and the neighbour mask staged by TMA.
-// A thread owns (x0 + warp, z0 + lane) and the tile's 8 rows, as k_cg_spmv,
-// and sums p.Ap in the same order.
+// A thread owns (x0 + warp, z0 + lane) and the tile's 8 rows, as k_cg_spmv
+// does; the CTAs take other tiles than k_cg_spmv's, so p.Ap is grouped
+// differently in its last bits.
 namespace sp {
 constexpr int kP = 10 * 10 * 40, kD = 8 * 8 * 32, kCX = 9 * 8 * 32, kCY = 8 * 9 * 32, kCZ = 8 * 8 * 36, kM = kD;
 constexpr uint32_t kTx = uint32_t((kP + kD + kCX + kCY + kCZ) * 4 + kM);
-constexpr int oP = 128, oD = oP + kP * 4, oCX = oD + kD * 4, oCY = oCX + kCX * 4, oCZ = oCY + kCY * 4,
-              oM = oCZ + kCZ * 4, kSmem = oM + kM;
-static_assert(kP * 4 % 128 == 0 && kCX * 4 % 128 == 0 && kCZ * 4 % 128 == 0, "128-byte aligned boxes");
+// offsets inside one stage; two mbarriers, then two stages
+constexpr int oP = 0, oD = oP + kP * 4, oCX = oD + kD * 4, oCY = oCX + kCX * 4, oCZ = oCY + kCY * 4,
+              oM = oCZ + kCZ * 4, kStage = oM + kM;
+constexpr int kBase = 128, kSmem = kBase + 2 * kStage;
+static_assert(kP * 4 % 128 == 0 && kCX * 4 % 128 == 0 && kCZ * 4 % 128 == 0 && kStage % 128 == 0,
+              "128-byte aligned boxes");
 }  // namespace sp
 
-__global__ void __launch_bounds__(kTileThreads, 4)
+__device__ __forceinline__ void sp_issue(unsigned char* st, uint64_t* bar, const CUtensorMap* mp, const CUtensorMap* md,
+                                         const CUtensorMap* mcx, const CUtensorMap* mcy, const CUtensorMap* mcz,
+                                         const CUtensorMap* mm, int x0, int y0, int z0) {
+    fence_proxy_async();
+    bar_expect_tx(bar, sp::kTx);
+    tma_load_box(st + sp::oP, mp, z0 - 4, y0 - 1, x0 - 1, bar);
+    tma_load_box(st + sp::oD, md, z0, y0, x0, bar);
+    tma_load_box(st + sp::oCX, mcx, z0, y0, x0 - 1, bar);
+    tma_load_box(st + sp::oCY, mcy, z0, y0 - 1, x0, bar);
+    tma_load_box(st + sp::oCZ, mcz, z0 - 4, y0, x0, bar);
+    tma_load_box(st + sp::oM, mm, z0, y0, x0, bar);
+}
+
+// Two CTAs per SM, each walking its tiles through two stages (the next
+// tile's boxes in flight while the current one is multiplied).
+__global__ void __launch_bounds__(kTileThreads, 2)
     k_spmv_tma(const __grid_constant__ CUtensorMap mp, const __grid_constant__ CUtensorMap md,
                const __grid_constant__ CUtensorMap mcx, const __grid_constant__ CUtensorMap mcy,
                const __grid_constant__ CUtensorMap mcz, const __grid_constant__ CUtensorMap mm, int nx, int ny, int nz,
@@ -974,39 +1027,43 @@ __global__ void __launch_bounds__(kTileThreads, 4)
     if (sc->stop) return;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-    const float* Ps = reinterpret_cast<const float*>(sm + sp::oP);
-    const float* Ds = reinterpret_cast<const float*>(sm + sp::oD);
-    const float* CXs = reinterpret_cast<const float*>(sm + sp::oCX);
-    const float* CYs = reinterpret_cast<const float*>(sm + sp::oCY);
-    const float* CZs = reinterpret_cast<const float*>(sm + sp::oCZ);
-    const uint8_t* Ms = sm + sp::oM;
-    if (threadIdx.x == 0) bar_init(bar, 1);
+    if (threadIdx.x == 0) {
+        bar_init(&bar[0], 1);
+        bar_init(&bar[1], 1);
+    }
     __syncthreads();
     double v[1] = {0.0};
     const int units = *count;
     const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned parity = 0;
+    if (threadIdx.x == 0 && int(blockIdx.x) < units) {
+        int a, b, c;
+        tile_origin(ids, blockIdx.x, tdy, tdz, a, b, c);
+        sp_issue(sm + sp::kBase, &bar[0], &mp, &md, &mcx, &mcy, &mcz, &mm, a, b, c);
+    }
     bool failed = false;
-    for (int u = blockIdx.x; u < units; u += gridDim.x) {
-        const int id = ids[u];
-        const int tz = id % tdz, rest = id / tdz;
-        const int ty = rest % tdy, tx = rest / tdy;
-        const int x0 = tx * kTileX, y0 = ty * kTileY, z0 = tz * kTileZ;
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            bar_expect_tx(bar, sp::kTx);
-            tma_load_box(sm + sp::oP, &mp, z0 - 4, y0 - 1, x0 - 1, bar);
-            tma_load_box(sm + sp::oD, &md, z0, y0, x0, bar);
-            tma_load_box(sm + sp::oCX, &mcx, z0, y0, x0 - 1, bar);
-            tma_load_box(sm + sp::oCY, &mcy, z0, y0 - 1, x0, bar);
-            tma_load_box(sm + sp::oCZ, &mcz, z0 - 4, y0, x0, bar);
-            tma_load_box(sm + sp::oM, &mm, z0, y0, x0, bar);
+    int it = 0;
+    for (int u = blockIdx.x; u < units; u += gridDim.x, ++it) {
+        const int s = it & 1;
+        const unsigned char* st = sm + sp::kBase + s * sp::kStage;
+        int x0, y0, z0;
+        tile_origin(ids, u, tdy, tdz, x0, y0, z0);
+        const int un = u + int(gridDim.x);
+        if (threadIdx.x == 0 && un < units) {  // the other stage was released by the last barrier
+            int a, b, c;
+            tile_origin(ids, un, tdy, tdz, a, b, c);
+            sp_issue(sm + sp::kBase + (s ^ 1) * sp::kStage, &bar[s ^ 1], &mp, &md, &mcx, &mcy, &mcz, &mm, a, b, c);
         }
-        if (__syncthreads_or(!bar_wait(bar, parity))) {  // every thread leaves together
+        if (__syncthreads_or(!bar_wait(&bar[s], (it >> 1) & 1))) {  // every thread leaves together
+            if (threadIdx.x == 0 && un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);  // the prefetch, bounded
             failed = true;
             break;
         }
-        parity ^= 1u;
+        const float* Ps = reinterpret_cast<const float*>(st + sp::oP);
+        const float* Ds = reinterpret_cast<const float*>(st + sp::oD);
+        const float* CXs = reinterpret_cast<const float*>(st + sp::oCX);
+        const float* CYs = reinterpret_cast<const float*>(st + sp::oCY);
+        const float* CZs = reinterpret_cast<const float*>(st + sp::oCZ);
+        const uint8_t* Ms = st + sp::oM;
         const int x = x0 + wp, zz = z0 + lane;
         if (x < nx && zz < nz) {
 #pragma unroll
@@ -1033,18 +1090,116 @@ __global__ void __launch_bounds__(kTileThreads, 4)
         }
         __syncthreads();
     }
-    if (failed) {
-        if (threadIdx.x == 0) {
-            sc->timeout = 1;
-            sc->status = LHI_E_TIMEOUT;
-            sc->stop = 1;
-        }
-        // the CTA still takes part in the grid-wide sum below
+    if (failed && threadIdx.x == 0) {
+        sc->timeout = 1;
+        sc->status = LHI_E_TIMEOUT;
+        sc->stop = 1;
     }
+    // every CTA takes part in the grid-wide sum, a failed one too
     double tot[1];
     if (!grid_sum_last<1>(v, partials, counter, tot)) return;
     sc->denom = tot[0];
     sc->alpha = sc->rz_old / tot[0];
+}
+
+// ------------------------------------------------- TMA restriction
+// CGSolver<3>::Restrict from one active fine tile: z grown by one cell, r,
+// diag, coefficients and mask staged by TMA; the residual r - A z of the
+// tile's 2048 cells goes to shared memory, then each of its 4 x 4 x 16
+// coarse cells sums its 8 children in the reference's order (restrict_cell).
+// Coarse cells whose children all lie in inactive fine tiles are air cells
+// whose restriction is 0, which they already hold.
+namespace rs {
+constexpr int kR = 8 * 8 * 32;
+constexpr int oP = 128, oR = oP + sp::kP * 4, oD = oR + kR * 4, oCX = oD + sp::kD * 4, oCY = oCX + sp::kCX * 4,
+              oCZ = oCY + sp::kCY * 4, oM = oCZ + sp::kCZ * 4, oRes = oM + sp::kM, kSmem = oRes + kR * 4;
+constexpr uint32_t kTx = sp::kTx + kR * 4;
+}  // namespace rs
+
+__global__ void __launch_bounds__(kTileThreads, 3)
+    k_restrict_tma(const __grid_constant__ CUtensorMap mz, const __grid_constant__ CUtensorMap mr,
+                   const __grid_constant__ CUtensorMap md, const __grid_constant__ CUtensorMap mcx,
+                   const __grid_constant__ CUtensorMap mcy, const __grid_constant__ CUtensorMap mcz,
+                   const __grid_constant__ CUtensorMap mm, int nx, int ny, int nz, const int32_t* __restrict__ ids,
+                   const int* __restrict__ count, int tdy, int tdz, int cnx, int cny, int cnz, float* __restrict__ rc,
+                   float* __restrict__ zc, SolveScalars* __restrict__ sc) {
+    if (sc->stop) return;
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    const float* Ps = reinterpret_cast<const float*>(sm + rs::oP);
+    const float* Rs = reinterpret_cast<const float*>(sm + rs::oR);
+    const float* Ds = reinterpret_cast<const float*>(sm + rs::oD);
+    const float* CXs = reinterpret_cast<const float*>(sm + rs::oCX);
+    const float* CYs = reinterpret_cast<const float*>(sm + rs::oCY);
+    const float* CZs = reinterpret_cast<const float*>(sm + rs::oCZ);
+    const uint8_t* Ms = sm + rs::oM;
+    float* Res = reinterpret_cast<float*>(sm + rs::oRes);
+    if (threadIdx.x == 0) bar_init(bar, 1);
+    __syncthreads();
+    const int units = *count;
+    const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned parity = 0;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        int x0, y0, z0;
+        tile_origin(ids, u, tdy, tdz, x0, y0, z0);
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            bar_expect_tx(bar, rs::kTx);
+            tma_load_box(sm + rs::oP, &mz, z0 - 4, y0 - 1, x0 - 1, bar);
+            tma_load_box(sm + rs::oR, &mr, z0, y0, x0, bar);
+            tma_load_box(sm + rs::oD, &md, z0, y0, x0, bar);
+            tma_load_box(sm + rs::oCX, &mcx, z0, y0, x0 - 1, bar);
+            tma_load_box(sm + rs::oCY, &mcy, z0, y0 - 1, x0, bar);
+            tma_load_box(sm + rs::oCZ, &mcz, z0 - 4, y0, x0, bar);
+            tma_load_box(sm + rs::oM, &mm, z0, y0, x0, bar);
+        }
+        if (__syncthreads_or(!bar_wait(bar, parity))) {  // every thread leaves together
+            if (threadIdx.x == 0) {
+                sc->timeout = 1;
+                sc->status = LHI_E_TIMEOUT;
+                sc->stop = 1;
+            }
+            return;
+        }
+        parity ^= 1u;
+#pragma unroll
+        for (int ly = 0; ly < kTileY; ++ly) {
+            const int pi = ((wp + 1) * 10 + (ly + 1)) * 40 + (lane + 4);
+            const int ci = (wp * 8 + ly) * 32 + lane;
+            const unsigned m = Ms[ci];
+            const float zc0 = Ps[pi];
+            float a = 0.f;
+            if (m & 64u) {
+                a = zc0 * Ds[ci];
+                if (m & 1u) a += Ps[pi + 400] * CXs[ci + 256];
+                if (m & 2u) a += Ps[pi - 400] * CXs[ci];
+                if (m & 4u) a += Ps[pi + 40] * CYs[(wp * 9 + ly + 1) * 32 + lane];
+                if (m & 8u) a += Ps[pi - 40] * CYs[(wp * 9 + ly) * 32 + lane];
+                if (m & 16u) a += Ps[pi + 1] * CZs[(wp * 8 + ly) * 36 + lane + 4];
+                if (m & 32u) a += Ps[pi - 1] * CZs[(wp * 8 + ly) * 36 + lane + 3];
+            }
+            Res[ci] = Rs[ci] - a;
+        }
+        __syncthreads();
+        {
+            const int t = threadIdx.x;
+            const int i = t >> 6, j = (t >> 4) & 3, k = t & 15;
+            const int cx = (x0 >> 1) + i, cy = (y0 >> 1) + j, cz = (z0 >> 1) + k;
+            if (cx < cnx && cy < cny && cz < cnz) {
+                float acc = 0.f;
+#pragma unroll
+                for (int c8 = 0; c8 < 8; ++c8) {
+                    const int a = (c8 >> 2) & 1, b = (c8 >> 1) & 1, c = c8 & 1;
+                    const float res = Res[((2 * i + a) * 8 + (2 * j + b)) * 32 + 2 * k + c];
+                    acc = float(double(acc) + 0.125 * double(res));
+                }
+                const long long o = ((long long)cx * cny + cy) * cnz + cz;
+                rc[o] = acc;
+                zc[o] = 0.f;
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // Ap = A p; p.Ap over the update region; alpha = rz / p.Ap (PressureSolver.cpp:873-888).
@@ -1462,6 +1617,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_masks() {
 template <class T, class TX> void LiquidImpl<T, TX>::setup_fused() {
     if constexpr (std::is_same<T, float>::value) {
         LHI_CUDA(cudaFuncSetAttribute(k_rb_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, rb::kSmem));
+        LHI_CUDA(cudaFuncSetAttribute(k_restrict_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, rs::kSmem));
         for (int l = 0; l < nlev_; ++l) {
             LevelDev<T>& L = lv_[l];
             if (L.n == 0 || L.nz % 4 != 0 || L.nx < 12 || L.ny < 12 || L.nz < rb::kMW) continue;
@@ -1481,6 +1637,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::setup_fused() {
             L.tm_cy = make_box_map(L.cf[1], F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 11, rb::kZW);
             L.tm_m = make_box_map(L.mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.nx, L.ny, L.nz, L.mpitch, 10, 10,
                                   rb::kMW);
+            L.ts_z = make_box_map(L.z, F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 10, 40);
+            L.ts_zb = make_box_map(L.zb, F32, 4, L.nx, L.ny, L.nz, L.nz, 10, 10, 40);
+            L.ts_r = make_box_map(L.r, F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 8, 32);
+            L.ts_d = make_box_map(L.diag, F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 8, 32);
+            L.ts_cx = make_box_map(L.cf[0], F32, 4, L.nx, L.ny, L.nz, L.nz, 9, 8, 32);
+            L.ts_cy = make_box_map(L.cf[1], F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 9, 32);
+            L.ts_cz = make_box_map(L.cf[2], F32, 4, L.nx, L.ny, L.nz, L.nz, 8, 8, 36);
+            L.ts_m = make_box_map(L.mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.nx, L.ny, L.nz, L.mpitch, 8, 8, 32);
             L.fused = true;
         }
     }
@@ -1524,16 +1688,17 @@ template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweep
     const T w = T(sp_.smoothing_factor);
     const int cat = (level == 0) ? LHI_KERNEL_SMOOTH_FINE : LHI_KERNEL_SMOOTH_COARSE;
     if (L.fused && sp_.sweep_kernel == LHI_SWEEP_FUSED) {
-        const unsigned GF = unsigned(std::min(L.ntiles, 2 * kSMs));
+        const unsigned GF = unsigned(std::min(L.ntiles, kSMs));
         for (int s = 0; s < sweeps; ++s) {
             auto ps_ = scope(cat);
-            k_rb_fused<<<GF, kTileThreads, rb::kSmem, cur_>>>(
+            k_rb_fused<<<GF, rb::kThreads, rb::kSmem, cur_>>>(
                 L.tm_z, L.tm_r, L.tm_d, L.tm_cx, L.tm_cy, L.tm_cz, L.tm_m, L.nx, L.ny, L.nz, L.tiles,
                 &sc_->tile_count[level], L.tdim[1], L.tdim[2], reinterpret_cast<float*>(L.zb), float(w),
                 sp_.smoother, sc_);
             LHI_LAUNCH_CHECK();
             std::swap(L.z, L.zb);
             std::swap(L.tm_z, L.tm_zb);
+            std::swap(L.ts_z, L.ts_zb);
         }
         return;
     }
@@ -1551,7 +1716,13 @@ template <class T, class TX> void LiquidImpl<T, TX>::restrict_to(int level) {
     LevelDev<T>& F = lv_[level - 1];
     if (C.n == 0) return;
     auto ps_ = scope(LHI_KERNEL_RESTRICT);
-    if (level >= coarse_level_) {
+    if (F.fused && sp_.sweep_kernel == LHI_SWEEP_FUSED) {
+        const unsigned GR = unsigned(std::min(F.ntiles, 3 * kSMs));
+        k_restrict_tma<<<GR, kTileThreads, rs::kSmem, cur_>>>(
+            F.ts_z, F.ts_r, F.ts_d, F.ts_cx, F.ts_cy, F.ts_cz, F.ts_m, F.nx, F.ny, F.nz, F.tiles,
+            &sc_->tile_count[level - 1], F.tdim[1], F.tdim[2], C.nx, C.ny, C.nz, reinterpret_cast<float*>(C.r),
+            reinterpret_cast<float*>(C.z), sc_);
+    } else if (level >= coarse_level_) {
         k_restrict_dense<T><<<blocks_for(C.n, 256), 256, 0, cur_>>>(lk(F), F.r, F.z, C.nx, C.ny, C.nz, C.r, C.z,
                                                                      &sc_->stop);
     } else {
@@ -1623,6 +1794,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle() {
         LHI_CUDA(cudaMemcpyAsync(L.zb, L.z, sizeof(T) * L.n, cudaMemcpyDeviceToDevice, cur_));
         std::swap(L.z, L.zb);
         std::swap(L.tm_z, L.tm_zb);
+        std::swap(L.ts_z, L.ts_zb);
     }
 }
 
@@ -1741,7 +1913,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_body(unsigned long 
     {
         auto ps_ = scope(LHI_KERNEL_SPMV);
         if (spmv_tma_ && sp_.sweep_kernel == LHI_SWEEP_FUSED)
-            k_spmv_tma<<<G, kTileThreads, sp::kSmem, cur_>>>(
+            k_spmv_tma<<<std::min(G, unsigned(2 * kSMs)), kTileThreads, sp::kSmem, cur_>>>(
                 tm_sp_[0], tm_sp_[1], tm_sp_[2], tm_sp_[3], tm_sp_[4], tm_sp_[5], L0.nx, L0.ny, L0.nz, L0.tiles,
                 &sc_->tile_count[0], L0.tdim[1], L0.tdim[2], reinterpret_cast<float*>(ap_), partials_, counter_, sc_,
                 cf);
