@@ -101,7 +101,8 @@ __global__ void k_soa_to_aos(const T* __restrict__ pd, long long cap, const int3
 // cell c takes min(|x_c - x_p| - r) over particles p whose Point2Index cell
 // lies within +-d of c.  The minimum does not depend on visiting order, so
 // the result is bit-identical to the reference.  Window cells that provably
-// cannot lower the current minimum are skipped (bound with safety margin).
+// cannot lower the current minimum are skipped (bound with safety margin),
+// and the cell's own particles are visited first so the bound bites early.
 template <class T>
 __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* __restrict__ cs,
                                                     const uint8_t* __restrict__ occ, int ox, int oy, int oz,
@@ -132,46 +133,54 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
     const T* px = pd;
     const T* py = pd + cap;
     const T* pz = pd + 2 * cap;
-    for (int pass = 0; pass < 2; ++pass) {
-        for (int wx = x0; wx <= x1; ++wx)
-            for (int wy = y0; wy <= y1; ++wy) {
-                int ax = abs(wx - cx), ay = abs(wy - cy);
-                long long rowc = ((long long)wx * g.ny + wy) * g.nz;
-                for (int wz = z0; wz <= z1; ++wz) {
-                    int az = abs(wz - cz);
-                    bool inner = ax <= 1 && ay <= 1 && az <= 1;
-                    if (inner != (pass == 0)) continue;
-                    long long w = rowc + wz;
-                    int s = cs[w], e = cs[w + 1];
-                    if (s == e) continue;
-                    if (pass == 1) {
-                        // every particle of cell w is at least lb away from the centre
-                        T lx = T(fmax(double(ax) - 0.5, 0.0)) * g.dx[0];
-                        T ly = T(fmax(double(ay) - 0.5, 0.0)) * g.dx[1];
-                        T lz = T(fmax(double(az) - 0.5, 0.0)) * g.dx[2];
-                        double lb = sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
-                                    double(radius) * (1.0 + 1e-6);
-                        if (double(cur) < lb) continue;
-                    }
-                    // the particles of a cell off the grid's outer layer were sorted
-                    // into it by their own unclamped Point2Index: all inside the window
-                    const bool own = wx > 0 && wx < g.nx - 1 && wy > 0 && wy < g.ny - 1 && wz > 0 &&
-                                     wz < g.nz - 1;
-                    for (int p = s; p < e; ++p) {
-                        T qx = px[p], qy = py[p], qz = pz[p];
-                        if (!own) {
-                            int tx = cell_trunc(qx, g.mn[0], g.dx[0]);
-                            int ty = cell_trunc(qy, g.mn[1], g.dx[1]);
-                            int tz = cell_trunc(qz, g.mn[2], g.dx[2]);
-                            if (abs(tx - cx) > d0 || abs(ty - cy) > d1 || abs(tz - cz) > d2) continue;
-                        }
-                        T dist = X<T>::sqrt(sqnorm3(X<T>::sub(cpx, qx), X<T>::sub(cpy, qy), X<T>::sub(cpz, qz)));
-                        T ph = X<T>::sub(dist, radius);
-                        cur = (cur < ph) ? cur : ph;
-                    }
-                }
+    // Visits window cell (wx, wy, wz).  With prune, a cell is skipped when
+    // every point of its box is farther than cur + r from the centre (the
+    // bound holds for particles clamped into an outer-layer cell too: they
+    // lie beyond it).
+    auto visit = [&](int wx, int wy, int wz, bool prune) {
+        const long long w = ((long long)wx * g.ny + wy) * g.nz + wz;
+        const int s = cs[w], e = cs[w + 1];
+        if (s == e) return;
+        if (prune) {
+            const int ax = abs(wx - cx), ay = abs(wy - cy), az = abs(wz - cz);
+            T lx = T(fmax(double(ax) - 0.5, 0.0)) * g.dx[0];
+            T ly = T(fmax(double(ay) - 0.5, 0.0)) * g.dx[1];
+            T lz = T(fmax(double(az) - 0.5, 0.0)) * g.dx[2];
+            double lb = sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
+                        double(radius) * (1.0 + 1e-6);
+            if (double(cur) < lb) return;
+        }
+        // the particles of a cell off the grid's outer layer were sorted
+        // into it by their own unclamped Point2Index: all inside the window
+        const bool own = wx > 0 && wx < g.nx - 1 && wy > 0 && wy < g.ny - 1 && wz > 0 && wz < g.nz - 1;
+        for (int p = s; p < e; ++p) {
+            T qx = px[p], qy = py[p], qz = pz[p];
+            if (!own) {
+                int tx = cell_trunc(qx, g.mn[0], g.dx[0]);
+                int ty = cell_trunc(qy, g.mn[1], g.dx[1]);
+                int tz = cell_trunc(qz, g.mn[2], g.dx[2]);
+                if (abs(tx - cx) > d0 || abs(ty - cy) > d1 || abs(tz - cz) > d2) continue;
             }
-    }
+            T dist = X<T>::sqrt(sqnorm3(X<T>::sub(cpx, qx), X<T>::sub(cpy, qy), X<T>::sub(cpz, qz)));
+            T ph = X<T>::sub(dist, radius);
+            cur = (cur < ph) ? cur : ph;
+        }
+    };
+    // The minimum does not depend on the visiting order, so the cell's own
+    // particles go first: inside the liquid they already bring cur below the
+    // bound of every neighbouring cell.  Then the 26 neighbours, then the
+    // rest of the window, both pruned.
+    visit(cx, cy, cz, false);
+    for (int pass = 1; pass < 3; ++pass)
+        for (int wx = x0; wx <= x1; ++wx)
+            for (int wy = y0; wy <= y1; ++wy)
+                for (int wz = z0; wz <= z1; ++wz) {
+                    const int ax = abs(wx - cx), ay = abs(wy - cy), az = abs(wz - cz);
+                    if ((ax | ay | az) == 0) continue;
+                    const bool inner = ax <= 1 && ay <= 1 && az <= 1;
+                    if (inner != (pass == 1)) continue;
+                    visit(wx, wy, wz, true);
+                }
     phi[c] = cur;
 }
 
