@@ -5,7 +5,9 @@
 // A tile is 4096 keys handled by 8 warps; each warp owns 512 consecutive keys
 // and walks them 32 at a time, so the in-tile order is (warp, round, lane),
 // i.e. the input order.  Ranks inside a round come from __match_any_sync, so
-// equal digits keep their input order: the sort is stable.
+// equal digits keep their input order: the sort is stable.  The scatter
+// stages its tile in shared memory in digit order and writes every digit's
+// run of keys to consecutive global positions.
 #include "impl.cuh"
 
 namespace lhi {
@@ -132,25 +134,55 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* 
         __syncwarp();
     }
     __syncthreads();
-    // exclusive prefix over warps, digit by digit
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
+    // exclusive prefix over warps, digit by digit, then over digits: the
+    // tile-local start of every digit
+    __shared__ uint32_t dstart[kRadix];
+    __shared__ uint32_t dsum[kSortWarps];
+    static_assert(kSortThreads == kRadix, "one thread per digit");
+    {
+        const int d = threadIdx.x;
         uint32_t run = 0;
         for (int k = 0; k < kSortWarps; ++k) {
             uint32_t c = wcnt[k][d];
             wcnt[k][d] = run;
             run += c;
         }
+        uint32_t incl = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) dsum[w] = incl;
+        __syncthreads();
+        uint32_t wofs = 0;
+        for (int k = 0; k < w; ++k) wofs += dsum[k];
+        dstart[d] = wofs + incl - run;
     }
     __syncthreads();
+    // stage the tile in digit order (input order inside a digit) ...
+    __shared__ uint32_t skey[kSortTile];
+    __shared__ int32_t sval[kSortTile];
 #pragma unroll
     for (int r = 0; r < kSortRounds; ++r) {
         long long idx = wbase + r * 32 + lane;
         if (idx < n) {
             unsigned d = (key[r] >> shift) & (kRadix - 1);
-            long long pos = (long long)offs[(long long)d * ntiles + blockIdx.x] + wcnt[w][d] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+            const uint32_t lp = dstart[d] + wcnt[w][d] + rank[r];
+            skey[lp] = key[r];
+            sval[lp] = val[r];
         }
+    }
+    __syncthreads();
+    // ... and write each digit's run to consecutive global positions
+    const long long tbase = (long long)blockIdx.x * kSortTile;
+    const int tn = int(min((long long)kSortTile, n - tbase));
+    for (int i = threadIdx.x; i < tn; i += kSortThreads) {
+        const uint32_t k = skey[i];
+        const unsigned d = (k >> shift) & (kRadix - 1);
+        const long long pos = (long long)offs[(long long)d * ntiles + blockIdx.x] + (i - int(dstart[d]));
+        kout[pos] = k;
+        vout[pos] = sval[i];
     }
 }
 
