@@ -456,14 +456,15 @@ constexpr int kThreads = 512;
 
 // Mask bits of a cell: 0..5 neighbour +x, -x, +y, -y, +z, -z exists with phi < 0;
 // 6: the cell's own type is not 0.
-__device__ __forceinline__ void rb_cell(float* __restrict__ Zs, const float* __restrict__ Rs,
+__device__ __forceinline__ bool rb_eval(const float* __restrict__ Zs, const float* __restrict__ Rs,
                                         const float* __restrict__ Ds, const float* __restrict__ CZs,
                                         const float* __restrict__ CXs, const float* __restrict__ CYs,
-                                        const uint8_t* __restrict__ Ms, int lx, int ly, int lz, float w, int variant) {
+                                        const uint8_t* __restrict__ Ms, int lx, int ly, int lz, float w, int variant,
+                                        int& zi, float& out) {
     const int ri = ((lx + 1) * 10 + (ly + 1)) * rb::kZW + (lz + 4);
+    zi = ((lx + 2) * 12 + (ly + 2)) * rb::kZW + (lz + 4);
     const float d = Ds[ri];
-    if (is_small(d)) return;
-    const int zi = ((lx + 2) * 12 + (ly + 2)) * rb::kZW + (lz + 4);
+    if (is_small(d)) return false;
     const unsigned m = Ms[((lx + 1) * 10 + (ly + 1)) * rb::kMW + (lz + 16)];
     const float zc = Zs[zi];
     float ax = 0.f;
@@ -479,10 +480,9 @@ __device__ __forceinline__ void rb_cell(float* __restrict__ Zs, const float* __r
         if (m & 32u) ax += Zs[zi - 1] * CZs[ri - 1];
     }
     const float term = (Rs[ri] - ax) / d;
-    float out;
     if (variant == LHI_SMOOTHER_DAMPED_GS) out = zc + w * term;
     else out = float((1.0 - double(w)) * double(zc) + double(float(w * term)));
-    Zs[zi] = out;
+    return true;
 }
 
 // Tile id u of the active list -> origin of its 8 x 8 x 32 cells.
@@ -562,19 +562,46 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
         const float* CYs = reinterpret_cast<const float*>(st + rb::oCY);
         const uint8_t* Ms = st + rb::oM;
         // colour 0 ((x + y + z) even) on T grown by one cell: 10 x 10 rows of 17
-        for (int q = threadIdx.x; q < 100 * 17; q += rb::kThreads) {
-            const int row = q / 17, k = q - row * 17;
-            const int lx = row / 10 - 1, ly = row - (row / 10) * 10 - 1;
-            const int lz = ((x0 + lx + y0 + ly + z0 - 1) & 1) - 1 + 2 * k;
-            rb_cell(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant);
+        // a colour's updates read only the other colour: a thread evaluates
+        // all of its cells before storing any, so their loads overlap
+        {
+            constexpr int kN = (100 * 17 + rb::kThreads - 1) / rb::kThreads;
+            int zi[kN];
+            float out[kN];
+            bool upd[kN];
+#pragma unroll
+            for (int n = 0; n < kN; ++n) {
+                const int q = threadIdx.x + n * rb::kThreads;
+                upd[n] = false;
+                if (q < 100 * 17) {
+                    const int row = q / 17, k = q - row * 17;
+                    const int lx = row / 10 - 1, ly = row - (row / 10) * 10 - 1;
+                    const int lz = ((x0 + lx + y0 + ly + z0 - 1) & 1) - 1 + 2 * k;
+                    upd[n] = rb_eval(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant, zi[n], out[n]);
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < kN; ++n)
+                if (upd[n]) Zs[zi[n]] = out[n];
         }
         __syncthreads();
         // colour 1 on T: 8 x 8 rows of 16
-        for (int q = threadIdx.x; q < 64 * 16; q += rb::kThreads) {
-            const int row = q >> 4, k = q & 15;
-            const int lx = row >> 3, ly = row & 7;
-            const int lz = ((x0 + lx + y0 + ly + z0 + 1) & 1) + 2 * k;
-            rb_cell(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant);
+        {
+            constexpr int kN = 64 * 16 / rb::kThreads;
+            int zi[kN];
+            float out[kN];
+            bool upd[kN];
+#pragma unroll
+            for (int n = 0; n < kN; ++n) {
+                const int q = threadIdx.x + n * rb::kThreads;
+                const int row = q >> 4, k = q & 15;
+                const int lx = row >> 3, ly = row & 7;
+                const int lz = ((x0 + lx + y0 + ly + z0 + 1) & 1) + 2 * k;
+                upd[n] = rb_eval(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant, zi[n], out[n]);
+            }
+#pragma unroll
+            for (int n = 0; n < kN; ++n)
+                if (upd[n]) Zs[zi[n]] = out[n];
         }
         __syncthreads();
         for (int q = threadIdx.x; q < 64 * 8; q += rb::kThreads) {
@@ -590,7 +617,7 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
     }
 }
 
-// Neighbour masks of one level for the fused sweep (bits as rb_cell reads them).
+// Neighbour masks of one level for the fused sweep (bits as rb_eval reads them).
 template <class T>
 __global__ void k_level_mask(LevelK<T> L, uint8_t* __restrict__ mask, int pitch) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1162,6 +1189,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
             return;
         }
         parity ^= 1u;
+        float res[kTileY];  // all rows first, then the stores: their loads overlap
 #pragma unroll
         for (int ly = 0; ly < kTileY; ++ly) {
             const int pi = ((wp + 1) * 10 + (ly + 1)) * 40 + (lane + 4);
@@ -1178,8 +1206,10 @@ __global__ void __launch_bounds__(kTileThreads, 3)
                 if (m & 16u) a += Ps[pi + 1] * CZs[(wp * 8 + ly) * 36 + lane + 4];
                 if (m & 32u) a += Ps[pi - 1] * CZs[(wp * 8 + ly) * 36 + lane + 3];
             }
-            Res[ci] = Rs[ci] - a;
+            res[ly] = Rs[ci] - a;
         }
+#pragma unroll
+        for (int ly = 0; ly < kTileY; ++ly) Res[(wp * 8 + ly) * 32 + lane] = res[ly];
         __syncthreads();
         {
             const int t = threadIdx.x;
