@@ -135,8 +135,9 @@ def algorithmic_bytes(cat, A, C_cells, P, scalar=4):
         "smooth_fine": (7 * s + 1) * A,
         # Ap = A p and p.Ap: p, diag, 3 face coefficients, mask read, Ap written
         "spmv": (5 * s + 1 + s) * A,
-        # P2G accumulation: position, velocity, affine read once per particle,
-        # w and v written once per face of the three components
+        # P2G accumulation (k_p2g; the normalisation is timed with "grid"):
+        # position, velocity, affine read once per particle, w and v written
+        # once per face of the three components
         "p2g": 15 * s * P + 6 * s * C_cells,
         # G2P + advection: position read, velocity/affine/position written,
         # cell key and index written, face velocities read once
@@ -231,7 +232,7 @@ def run_ours(args):
     avg_ms = tot_ms / max(n_launch, 1)
     achieved = algo / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if os.path.exists(tpath):
         tj = json.load(open(tpath))
         traffic = tj.get(args.scene, {}).get(dominant)

@@ -310,7 +310,7 @@ LHI_API int lhi_kernel_launch_count(int64_t* count);
 #define LHI_KERNEL_P2G 2          /* P2G accumulation + normalisation                */
 #define LHI_KERNEL_G2P 3          /* G2P + advection                                 */
 #define LHI_KERNEL_EXTRAPOLATE 4  /* velocity extrapolation sweeps                    */
-#define LHI_KERNEL_GRID 5         /* clear, gravity, velocity update, RHS, divergence */
+#define LHI_KERNEL_GRID 5         /* clear, P2G normalisation + gravity, velocity update, RHS, divergence */
 #define LHI_KERNEL_LHS 6          /* per-level matrix assembly                        */
 #define LHI_KERNEL_SMOOTH_FINE 7  /* red-black smoothing on the finest level          */
 #define LHI_KERNEL_SMOOTH_COARSE 8 /* smoothing on the coarser levels                 */

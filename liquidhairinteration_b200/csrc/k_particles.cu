@@ -801,7 +801,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::p2g_normalize(bool with_gravity, T gdt) {
-    auto ps_ = scope(LHI_KERNEL_P2G);
+    auto ps_ = scope(LHI_KERNEL_GRID);  // a per-face grid pass (with gravity); P2G times the accumulation alone
     for (int a = 0; a < 3; ++a) {
         int fx = nx_ + (a == 0), fy = ny_ + (a == 1), fz = nz_ + (a == 2);
         k_p2g_normalize<T><<<blocks_for(nface_[a], 256), 256, 0, stream_>>>(
