@@ -1643,14 +1643,16 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_masks() {
 
 
 // Levels that the fused sweep can take: FP32, z extent a multiple of 4 (TMA
-// strides are multiples of 16 bytes) and boxes no larger than the level.
+// strides are multiples of 16 bytes), at least 12 cells in x and y and one
+// tile (32 cells) in z.  Boxes may reach past the level in z; TMA fills that
+// part with zeros, which reads as diag 0 and an empty mask.
 template <class T, class TX> void LiquidImpl<T, TX>::setup_fused() {
     if constexpr (std::is_same<T, float>::value) {
         LHI_CUDA(cudaFuncSetAttribute(k_rb_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, rb::kSmem));
         LHI_CUDA(cudaFuncSetAttribute(k_restrict_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, rs::kSmem));
         for (int l = 0; l < nlev_; ++l) {
             LevelDev<T>& L = lv_[l];
-            if (L.n == 0 || L.nz % 4 != 0 || L.nx < 12 || L.ny < 12 || L.nz < rb::kMW) continue;
+            if (L.n == 0 || L.nz % 4 != 0 || L.nx < 12 || L.ny < 12 || L.nz < kTileZ) continue;
             L.mpitch = (L.nz + 15) / 16 * 16;
             const size_t mb = size_t(L.nx) * L.ny * L.mpitch;
             LHI_CUDA(cudaMalloc(&L.zb, sizeof(T) * L.n));
