@@ -807,6 +807,68 @@ template <class T>
 __device__ __forceinline__ void cta_smooth(const LevelK<T>& L, const T* r, T* z, const uint32_t* list, int n0,
                                            int n01, T w, int variant, int sweeps) {
     const int sy = L.nz, sx = L.ny * L.nz;
+    constexpr int K = 1;  // cells per colour per thread kept in registers
+    if (n0 <= K * int(blockDim.x) && n01 - n0 <= K * int(blockDim.x)) {
+        // Every thread's cells (at most K per colour) keep diag, r, their six
+        // coefficients and mask in registers for all sweeps; a pass loads
+        // only the neighbours' z.
+        int ci[2][K];
+        unsigned cm[2][K];
+        T cd[2][K], cr[2][K], cf[2][K][6];
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int e = (c ? n0 : 0) + int(threadIdx.x) + k * int(blockDim.x);
+                ci[c][k] = -1;
+                if (e < (c ? n01 : n0)) {
+                    const uint32_t ent = list[e];
+                    const int i = int(ent & 0xffffu);
+                    ci[c][k] = i;
+                    cm[c][k] = ent >> 16;
+                    cd[c][k] = L.diag[i];
+                    cr[c][k] = r[i];
+                    const unsigned m = cm[c][k];
+                    cf[c][k][0] = (m & 1u) ? L.cx[i] : T(0);
+                    cf[c][k][1] = (m & 2u) ? L.cx[i - sx] : T(0);
+                    cf[c][k][2] = (m & 4u) ? L.cy[i] : T(0);
+                    cf[c][k][3] = (m & 8u) ? L.cy[i - sy] : T(0);
+                    cf[c][k][4] = (m & 16u) ? L.cz[i] : T(0);
+                    cf[c][k][5] = (m & 32u) ? L.cz[i - 1] : T(0);
+                }
+            }
+        for (int s = 0; s < sweeps; ++s)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                T out[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const int i = ci[c][k];
+                    if (i < 0) continue;
+                    const unsigned m = cm[c][k];
+                    const T d = cd[c][k];
+                    const T zc = z[i];
+                    T ax = T(0);
+                    if (m & 64u) {
+                        ax = zc * d;
+                        if (m & 1u) ax += z[i + sx] * cf[c][k][0];
+                        if (m & 2u) ax += z[i - sx] * cf[c][k][1];
+                        if (m & 4u) ax += z[i + sy] * cf[c][k][2];
+                        if (m & 8u) ax += z[i - sy] * cf[c][k][3];
+                        if (m & 16u) ax += z[i + 1] * cf[c][k][4];
+                        if (m & 32u) ax += z[i - 1] * cf[c][k][5];
+                    }
+                    const T term = (cr[c][k] - ax) / d;
+                    if (variant == LHI_SMOOTHER_DAMPED_GS) out[k] = zc + w * term;
+                    else out[k] = T((1.0 - double(w)) * double(zc) + double(T(w * term)));
+                }
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    if (ci[c][k] >= 0) z[ci[c][k]] = out[k];
+                __syncthreads();
+            }
+        return;
+    }
     for (int s = 0; s < sweeps; ++s)
         for (int colour = 0; colour < 2; ++colour) {
             const int end = colour ? n01 : n0;
