@@ -303,7 +303,7 @@ public:
     void p2g_accumulate();
     void p2g_normalize(bool with_gravity, T gdt);
     void g2p(bool advect, T dt);
-    void smooth(int level, int sweeps);
+    bool smooth(int level, int sweeps, bool final_dot = false);  // true if the sweep formed the r.z / Ap.z sums
     void restrict_to(int level);
     void prolong_to(int level);
     void vcycle();
@@ -374,6 +374,8 @@ public:
     long long coarse_list_off_[kMaxLevels] = {};
     int* coarse_counts_ = nullptr;
     bool spmv_tma_ = false;
+    bool fuse_dot_ = false;   // the V-cycle being enqueued is the PCG body's preconditioner
+    bool dot_fused_ = false;  // its last level-0 sweep formed r.z, Ap.z and beta
     CUtensorMap tm_sp_[6];  // p, diag, cx, cy, cz, mask boxes of the TMA SpMV
     int tile_grid_ = 0;      // persistent CTAs of the tile kernels
     cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on

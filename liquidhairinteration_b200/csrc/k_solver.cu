@@ -517,10 +517,12 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
                const __grid_constant__ CUtensorMap mcy, const __grid_constant__ CUtensorMap mcz,
                const __grid_constant__ CUtensorMap mm, int nx, int ny, int nz, const int32_t* __restrict__ ids,
                const int* __restrict__ count, int tdy, int tdz, float* __restrict__ zout, float w, int variant,
-               SolveScalars* __restrict__ sc) {
+               SolveScalars* __restrict__ sc, const float* __restrict__ ap, double* __restrict__ partials,
+               unsigned* __restrict__ counter, int final_dot, int region, int flexible) {
     if (sc->stop) return;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    double v[2] = {0.0, 0.0};  // r.z and Ap.z of the swept tiles (final_dot)
     if (threadIdx.x == 0) {
         bar_init(&bar[0], 1);
         bar_init(&bar[1], 1);
@@ -552,7 +554,16 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
                 sc->stop = 1;
                 if (un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);  // the prefetch, bounded too
             }
-            return;
+            break;  // a CTA that gave up still takes part in the grid-wide sum below
+        }
+        // final_dot: this thread's float4 of Ap (the tile's 512 float4s, one
+        // per thread), loaded now so the load overlaps the two colour phases
+        static_assert(64 * 8 == rb::kThreads, "one float4 of the tile per thread");
+        float4 apv = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (final_dot) {
+            const int row = threadIdx.x >> 3, c = threadIdx.x & 7;
+            const int x = x0 + (row >> 3), y = y0 + (row & 7), z = z0 + 4 * c;
+            if (x < nx && y < ny && z < nz) apv = *reinterpret_cast<const float4*>(ap + ((long long)x * ny + y) * nz + z);
         }
         float* Zs = reinterpret_cast<float*>(st + rb::oZ);
         const float* Rs = reinterpret_cast<const float*>(st + rb::oR);
@@ -609,12 +620,32 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
             const int lx = row >> 3, ly = row & 7;
             const int x = x0 + lx, y = y0 + ly, z = z0 + 4 * c;
             if (x < nx && y < ny && z < nz) {
-                const float4 v = *reinterpret_cast<const float4*>(Zs + ((lx + 2) * 12 + (ly + 2)) * rb::kZW + 4 + 4 * c);
-                *reinterpret_cast<float4*>(zout + ((long long)x * ny + y) * nz + z) = v;
+                const float4 zv = *reinterpret_cast<const float4*>(Zs + ((lx + 2) * 12 + (ly + 2)) * rb::kZW + 4 + 4 * c);
+                *reinterpret_cast<float4*>(zout + ((long long)x * ny + y) * nz + z) = zv;
+                if (final_dot) {  // k_cg_dot_rz's sums over the swept cells
+                    const float zz[4] = {zv.x, zv.y, zv.z, zv.w}, aa[4] = {apv.x, apv.y, apv.z, apv.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int lz = 4 * c + j;
+                        const float rv = Rs[((lx + 1) * 10 + (ly + 1)) * rb::kZW + (lz + 4)];
+                        v[0] += double(rv) * double(zz[j]);
+                        const unsigned m = Ms[((lx + 1) * 10 + (ly + 1)) * rb::kMW + (lz + 16)];
+                        if ((m & 64u) && in_region(x, y, z + j, nx, ny, nz, region))
+                            v[1] += double(aa[j]) * double(zz[j]);
+                    }
+                }
             }
         }
         __syncthreads();
     }
+    if (!final_dot) return;
+    double tot[2];
+    if (!grid_sum_last<2>(v, partials, counter, tot)) return;
+    const double rz_new = tot[0], apz = tot[1];
+    sc->rz_new = rz_new;
+    sc->apz = apz;
+    sc->beta = flexible ? (-sc->alpha * apz / sc->rz_old) : (rz_new / sc->rz_old);
+    sc->rz_old = rz_new;
 }
 
 // Neighbour masks of one level for the fused sweep (bits as rb_eval reads them).
@@ -1775,26 +1806,28 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_tiles() {
     LHI_LAUNCH_CHECK();
 }
 
-template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweeps) {
+template <class T, class TX> bool LiquidImpl<T, TX>::smooth(int level, int sweeps, bool final_dot) {
     LevelDev<T>& L = lv_[level];
     const unsigned G = tile_blocks(L, tile_grid_, 4);
-    if (L.n == 0 || sweeps <= 0 || G == 0) return;
+    if (L.n == 0 || sweeps <= 0 || G == 0) return false;
     const T w = T(sp_.smoothing_factor);
     const int cat = (level == 0) ? LHI_KERNEL_SMOOTH_FINE : LHI_KERNEL_SMOOTH_COARSE;
     if (L.fused && sp_.sweep_kernel == LHI_SWEEP_FUSED) {
         const unsigned GF = unsigned(std::min(L.ntiles, kSMs));
         for (int s = 0; s < sweeps; ++s) {
             auto ps_ = scope(cat);
+            const int fd = (final_dot && s + 1 == sweeps) ? 1 : 0;
             k_rb_fused<<<GF, rb::kThreads, rb::kSmem, cur_>>>(
                 L.tm_z, L.tm_r, L.tm_d, L.tm_cx, L.tm_cy, L.tm_cz, L.tm_m, L.nx, L.ny, L.nz, L.tiles,
                 &sc_->tile_count[level], L.tdim[1], L.tdim[2], reinterpret_cast<float*>(L.zb), float(w),
-                sp_.smoother, sc_);
+                sp_.smoother, sc_, reinterpret_cast<const float*>(ap_), partials_, counter_, fd, sp_.update_region,
+                sp_.cg_variant == LHI_CG_FLEXIBLE ? 1 : 0);
             LHI_LAUNCH_CHECK();
             std::swap(L.z, L.zb);
             std::swap(L.tm_z, L.tm_zb);
             std::swap(L.ts_z, L.ts_zb);
         }
-        return;
+        return final_dot;
     }
     const TileK tk = tile_k(L, &sc_->tile_count[level], tile_grid_, 4);
     for (int s = 0; s < sweeps; ++s)
@@ -1803,6 +1836,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::smooth(int level, int sweep
             k_sweep<T><<<G, kTileThreads, 0, cur_>>>(lk(L), tk, L.r, L.z, w, sp_.smoother, phase, &sc_->stop);
             LHI_LAUNCH_CHECK();
         }
+    return false;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::restrict_to(int level) {
@@ -1911,7 +1945,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle_levels() {
         }
         for (int l = Lc - 1; l >= 0; --l) {
             prolong_to(l);
-            smooth(l, sp_.num_post_smooth);
+            dot_fused_ |= smooth(l, sp_.num_post_smooth, l == 0 && fuse_dot_);
         }
     } else {
         for (int l = 0; l < last; ++l) {
@@ -1921,7 +1955,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_vcycle_levels() {
         smooth(last, sp_.num_final_smooth);
         for (int l = last - 1; l >= 0; --l) {
             prolong_to(l);
-            smooth(l, sp_.num_post_smooth);
+            dot_fused_ |= smooth(l, sp_.num_post_smooth, l == 0 && fuse_dot_);
         }
     }
 }
@@ -2027,11 +2061,18 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_body(unsigned long 
         }
     }
     record_snapshot();
+    // with the multigrid preconditioner the last level-0 sweep of the V-cycle
+    // also forms r.z and Ap.z (and beta), which saves k_cg_dot_rz's pass
+    fuse_dot_ = sp_.preconditioner == LHI_PRECOND_MULTIGRID;
+    dot_fused_ = false;
     enqueue_precond();
+    fuse_dot_ = false;
     {
         auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-        k_cg_dot_rz<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, L0.r, L0.z, ap_, partials_, counter_, sc_, cf);
-        LHI_LAUNCH_CHECK();
+        if (!dot_fused_) {
+            k_cg_dot_rz<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, L0.r, L0.z, ap_, partials_, counter_, sc_, cf);
+            LHI_LAUNCH_CHECK();
+        }
         k_cg_update_p<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, L0.z, p_, sc_);
         LHI_LAUNCH_CHECK();
     }
