@@ -63,6 +63,26 @@ def dist_env():
         os.environ.get("WORLD_SIZE", "1"))
 
 
+def rank_reducers(world, device):
+    """barrier() and max_over_ranks(v) over this run's process group (both
+    plain pass-throughs for one rank).  Every timed number of a multi-replica
+    run is the maximum over ranks."""
+    import torch
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -166,16 +186,7 @@ def run_ours(args):
     n_particles = ps.NumParticles()
     stream = torch.cuda.ExternalStream(model.stream_ptr())
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_reducers(world, "cuda")
 
     for _ in range(args.warmup):
         model.PreStep(spec.dt)
