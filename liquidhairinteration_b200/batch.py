@@ -82,15 +82,35 @@ class BatchRunner:
         self.log_dir = log_dir
         self.logged = 0
         self.step_index = 0
+        # a scene whose solve produced NaN/Inf is not stepped again (its
+        # particles carry no meaning any more; stepping them only wastes time)
+        self.alive = [True] * len(self.models)
+        self.diverged = {}
         if log_dir:
             os.makedirs(log_dir, exist_ok=True)
 
     def step(self):
-        """One liquid step of every scene: all enqueued, then one wait."""
-        for spec, m in zip(self.specs, self.models):
-            m.PreStep(spec.dt)
-            m.Step(spec.dt)
-        out = [stats_of(m) for m in self.models]
+        """One liquid step of every live scene: all enqueued, then one wait.
+        Returns the solve statistics of the scenes stepped."""
+        from ._lib import LhiError
+        live = [k for k, a in enumerate(self.alive) if a]
+        for k in live:
+            try:
+                self.models[k].PreStep(self.specs[k].dt)
+                self.models[k].Step(self.specs[k].dt)
+            except LhiError as e:  # synchronous mode reports a NaN solve here
+                self.alive[k] = False
+                self.diverged[k] = self.step_index
+        out = []
+        for k in live:
+            if not self.alive[k]:
+                out.append({"status": abi.LHI_E_NAN, "iterations": 0})
+                continue
+            st = stats_of(self.models[k])
+            if st["status"] == abi.LHI_E_NAN:
+                self.alive[k] = False
+                self.diverged[k] = self.step_index
+            out.append(st)
         if self.log_dir:
             self._log()
         self.step_index += 1
@@ -137,17 +157,19 @@ def main(argv=None):
     import torch
     torch.cuda.synchronize()
     t1 = time.time()
-    bad, iters = 0, []
+    bad, iters, scene_steps = 0, [], 0
     for _ in range(a.steps):
         st = runner.step()
+        scene_steps += len(st)
         bad += sum(1 for s in st if s["status"] != abi.LHI_OK)
-        iters.append(np.mean([s["iterations"] for s in st]))
+        iters.append(np.mean([s["iterations"] for s in st]) if st else 0.0)
     wall = time.time() - t1
     cells = sum(s.n ** 3 for s in specs)
     res = {"scenes": a.scenes, "steps": a.steps, "sizes": sorted({s.n for s in specs}),
-           "cells": cells, "wall_s": round(wall, 3), "scene_steps_per_s": round(a.scenes * a.steps / wall, 2),
+           "cells": cells, "wall_s": round(wall, 3), "scene_steps_per_s": round(scene_steps / wall, 2),
            "ms_per_batch_step": round(1000 * wall / a.steps, 3), "mean_cg_iterations": round(float(np.mean(iters)), 2),
-           "failed_solves": bad, "setup_s": round(setup_s, 1),
+           "failed_solves": bad, "diverged_scenes": {str(k): v for k, v in runner.diverged.items()},
+           "setup_s": round(setup_s, 1),
            "autotuned": {str(k): {"sweeps": v[0], "coarse_cells": v[1]} for k, v in runner.tuned.items()},
            "autotune_solve_ms": {str(k): v for k, v in runner.tune_tables.items()},
            "snapshots_logged": runner.logged}
