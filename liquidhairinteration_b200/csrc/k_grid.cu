@@ -162,58 +162,72 @@ struct ExtRange {
 
 // Face (x, y, z) of this thread inside the range (32-bit index arithmetic:
 // every face array has fewer than 2^31 entries).
-__device__ __forceinline__ bool ext_cell(const ExtRange& r, int& x, int& y, int& z) {
+// Faces (x, y, z .. z+3) of this thread inside the range: 4 consecutive
+// faces along z per thread (32-bit index arithmetic: every face array has
+// fewer than 2^31 entries).
+__device__ __forceinline__ bool ext_cell4(const ExtRange& r, int& x, int& y, int& z) {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ey = r.y1 - r.y0 + 1, ez = r.z1 - r.z0 + 1;
-    if (ey <= 0 || ez <= 0 || i >= unsigned(r.x1 - r.x0 + 1) * unsigned(ey) * unsigned(ez)) return false;
-    const unsigned t = i / unsigned(ez);
-    z = r.z0 + int(i - t * unsigned(ez));
+    const int ey = r.y1 - r.y0 + 1, ez4 = (r.z1 - r.z0 + 1 + 3) / 4;
+    if (ey <= 0 || ez4 <= 0 || i >= unsigned(r.x1 - r.x0 + 1) * unsigned(ey) * unsigned(ez4)) return false;
+    const unsigned t = i / unsigned(ez4);
+    z = r.z0 + 4 * int(i - t * unsigned(ez4));
     y = r.y0 + int(t % unsigned(ey));
     x = r.x0 + int(t / unsigned(ey));
     return true;
 }
+inline long long ext_threads(const ExtRange& r) {
+    return (long long)std::max(r.x1 - r.x0 + 1, 0) * std::max(r.y1 - r.y0 + 1, 0) *
+           std::max((r.z1 - r.z0 + 1 + 3) / 4, 0);
+}
 
 template <class T> __global__ void k_extrap_init(ExtRange r, const T* __restrict__ lw, uint8_t* __restrict__ valid) {
-    int x, y, z;
-    if (!ext_cell(r, x, y, z)) return;
-    long long f = ((long long)x * r.fy + y) * r.fz + z;
-    valid[((long long)x * r.ny1 + y) * r.nz1 + z] = (lw[f] > T(0)) ? 0 : 255;
+    int x, y, z0;
+    if (!ext_cell4(r, x, y, z0)) return;
+    for (int z = z0; z < z0 + 4 && z <= r.z1; ++z) {
+        long long f = ((long long)x * r.fy + y) * r.fz + z;
+        valid[((long long)x * r.ny1 + y) * r.nz1 + z] = (lw[f] > T(0)) ? 0 : 255;
+    }
 }
 
 // With t == v the sweep runs in place: it writes only faces that were not
 // valid before sweep k, and it reads only faces that were, so the values
-// equal those of the sweep into a separate buffer.
+// equal those of the sweep into a separate buffer (the same holds between
+// a thread's own 4 faces).
 template <class T>
 __global__ void k_extrap_sweep(ExtRange r, int k, const T* v, T* t, uint8_t* __restrict__ valid) {
-    int x, y, z;
-    if (!ext_cell(r, x, y, z)) return;
-    long long f = ((long long)x * r.fy + y) * r.fz + z;
-    long long vi = ((long long)x * r.ny1 + y) * r.nz1 + z;
-    if (t != v) t[f] = v[f];
-    if (valid[vi] <= k) return;
-    T sum = T(0);
-    int count = 0;
-    for (int a = -1; a <= 1; ++a)
-        for (int b = -1; b <= 1; ++b)
-            for (int c = -1; c <= 1; ++c) {
-                long long nv = ((long long)(x + a) * r.ny1 + (y + b)) * r.nz1 + (z + c);
-                if (valid[nv] <= k) {
-                    sum = X<T>::add(sum, v[((long long)(x + a) * r.fy + (y + b)) * r.fz + (z + c)]);
-                    ++count;
+    int x, y, z0;
+    if (!ext_cell4(r, x, y, z0)) return;
+    for (int z = z0; z < z0 + 4 && z <= r.z1; ++z) {
+        long long f = ((long long)x * r.fy + y) * r.fz + z;
+        long long vi = ((long long)x * r.ny1 + y) * r.nz1 + z;
+        if (t != v) t[f] = v[f];
+        if (valid[vi] <= k) continue;
+        T sum = T(0);
+        int count = 0;
+        for (int a = -1; a <= 1; ++a)
+            for (int b = -1; b <= 1; ++b)
+                for (int c = -1; c <= 1; ++c) {
+                    long long nv = ((long long)(x + a) * r.ny1 + (y + b)) * r.nz1 + (z + c);
+                    if (valid[nv] <= k) {
+                        sum = X<T>::add(sum, v[((long long)(x + a) * r.fy + (y + b)) * r.fz + (z + c)]);
+                        ++count;
+                    }
                 }
-            }
-    if (count > 0) {
-        t[f] = X<T>::div(sum, T(count));
-        valid[vi] = uint8_t(k + 1);
+        if (count > 0) {
+            t[f] = X<T>::div(sum, T(count));
+            valid[vi] = uint8_t(k + 1);
+        }
     }
 }
 
 __global__ void k_extrap_finish(ExtRange r, uint8_t* __restrict__ valid) {
-    int x, y, z;
-    if (!ext_cell(r, x, y, z)) return;
-    long long vi = ((long long)x * r.ny1 + y) * r.nz1 + z;
-    uint8_t v = valid[vi];
-    valid[vi] = (v == 255) ? 255 : 0;
+    int x, y, z0;
+    if (!ext_cell4(r, x, y, z0)) return;
+    for (int z = z0; z < z0 + 4 && z <= r.z1; ++z) {
+        long long vi = ((long long)x * r.ny1 + y) * r.nz1 + z;
+        uint8_t v = valid[vi];
+        valid[vi] = (v == 255) ? 255 : 0;
+    }
 }
 
 // LiquidModel<3>::ComputeDivergence (LiquidModel.cpp:1066-1083): per fluid
@@ -559,8 +573,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::extrapolate() {
         r.fz = nz_ + (a == 2);
         r.ny1 = ny_ + 1;
         r.nz1 = nz_ + 1;
-        long long n = (long long)std::max(r.x1 - r.x0 + 1, 0) * std::max(r.y1 - r.y0 + 1, 0) *
-                      std::max(r.z1 - r.z0 + 1, 0);
+        const long long n = ext_threads(r);  // 4 faces along z per thread
         if (n > 0) {
             k_extrap_init<T><<<blocks_for(n, 256), 256, 0, stream_>>>(r, lw_[a], valid_);
             LHI_LAUNCH_CHECK();
