@@ -32,9 +32,10 @@ sys.path.insert(0, ROOT)
 METRIC = "256³ ms/step, solve ms: learned-precond FPCG vs plain MGPCG, 1 B200, rr≤1e-6"
 UNIT = "ms/step"
 
-# The reference's PCG does not converge on this scene (fluid reaches the
-# domain's outer cell layer), so the reference arm runs its
-# solver for the iteration count our MGPCG needs on this workload.
+# The reference's PCG does not converge on this scene (once fluid reaches the
+# domain's outer cell layer its update region and smoother break down), so the
+# reference arm runs its solver for the iteration count our MGPCG needs on
+# this workload.
 REFERENCE_PCG_ITERATIONS = 24
 # The reference arm times the full reference step on the same scene at 32^3
 # (1/512 of the cells and particles) and scales the time by 512.  Every
@@ -143,9 +144,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-# Algorithmic bytes per launch of each timed category (the per-unit figures
-# of DESIGN.md): A = active cells of level 0 (active tiles x 2048 cells),
-# C = all cells, P = particles, s = bytes per scalar.
+# Algorithmic bytes per launch of each timed category: A = active cells of
+# level 0 (active tiles x 2048 cells), C = all cells, P = particles, s =
+# bytes per scalar.
 def algorithmic_bytes(cat, A, C_cells, P, scalar=4):
     s = scalar
     table = {

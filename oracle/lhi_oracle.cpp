@@ -13,7 +13,8 @@
 //   * double-literal promotion, e.g. (1. - w) * z + w * term in Smooth.
 // Built with -ffp-contract=off so no multiply-add is fused.
 //
-// The reference's own data races are replaced by deterministic
+// The reference's own data races (its OpenMP loops add into shared sums and
+// flags without ordering) are replaced by deterministic
 // semantics: serial sums in PCG; extrapolation flags either Jacobi (GPU
 // semantics) or serial x-y-z order (the reference with one OpenMP thread).
 #include "lhi_oracle.h"
