@@ -201,8 +201,10 @@ __device__ __forceinline__ int off_hi(int i, int a, int d) { return min(i == a ?
 // registers, then adds each window node once into the tile's shared-memory
 // accumulators.  The lanes of a warp own distinct cells, so at any step they
 // add to distinct nodes.  Finally each touched node goes to global memory
-// with one add.  The per-particle arithmetic is the reference's, rounded the
-// same way; only the order in which particles are summed differs.
+// with one add.  The per-axis weights and C.(x_p - x_node) terms are the
+// reference's, rounded the same way; the per-node products are regrouped
+// and fused (multiply-add), and particles are summed in another order, so
+// P2G matches the reference to rounding, not bit for bit.
 // A particle whose own truncated index (cast<Integer>, LiquidModel.cpp:629)
 // is not the cell it was sorted into (only outside the grid, where the sort
 // key is clamped) adds its window straight to global memory.
@@ -295,19 +297,23 @@ __device__ __forceinline__ void p2g_cell_component(const GridP<T>& g, const int 
             wz[s2] = ok ? qweight(e) : T(0);
             ez[s2] = X<T>::mul(C2, X<T>::sub(q[2], X<T>::add(X<T>::mul(c, g.dx[2]), g.mn[2])));
         }
+        // w (v + C.(x_p - x_node)) with the v + ex + ey part formed once per
+        // (x, y) pair and the product accumulated by fused multiply-add
 #pragma unroll
-        for (int i = 0; i < NX; ++i)
+        for (int i = 0; i < NX; ++i) {
+            const T vxi = vel + ex[i];
 #pragma unroll
             for (int j = 0; j < NY; ++j) {
-                const T wxy = X<T>::mul(wx[i], wy[j]);
+                const T wxy = wx[i] * wy[j];
+                const T vxy = vxi + ey[j];
 #pragma unroll
                 for (int k = 0; k < NZ; ++k) {
-                    const T weight = X<T>::mul(wxy, wz[k]);
-                    const T val = X<T>::mul(weight, X<T>::add(vel, X<T>::add(ex[i], X<T>::add(ey[j], ez[k]))));
-                    aw[i][j][k] = aw[i][j][k] + weight;
-                    av[i][j][k] = av[i][j][k] + val;
+                    const T weight = wxy * wz[k];
+                    aw[i][j][k] += weight;
+                    av[i][j][k] = fma(weight, vxy + ez[k], av[i][j][k]);
                 }
             }
+        }
     }
     if (p1 == p0) return;
     const int ext_y = kTile + 2 + (A == 1), ext_z = kTile + 2 + (A == 2);
