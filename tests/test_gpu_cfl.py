@@ -1,0 +1,32 @@
+"""LiquidModel<3>::GetCFL (LiquidModel.h:49-55): the reference's clamp of
+dx / max|v| over the particles' velocities, the same after a step and after
+the same particles are set again."""
+import numpy as np
+import pytest
+
+from liquidhairinteration_b200 import scenes
+
+from helpers import gpu_model
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_cfl_after_step_and_after_set_particles(lhi, prec):
+    spec = scenes.dam(32)
+    m = gpu_model(spec, prec, spec.solver_params(coarse_cells=64))
+    pos, vel = scenes.seed(spec, "fp64" if prec == "fp64" else "fp32")
+    m.GetParticleSystem().SetParticles(pos, vel)
+    for _ in range(3):
+        m.PreStep(spec.dt)
+        m.Step(spec.dt)
+    after_step = m.GetCFL()
+    p, v, a = m.GetParticleSystem().GetParticles()
+    m.GetParticleSystem().SetParticles(p, v, a)
+    full = m.GetCFL()
+    assert after_step == full
+    vmax = float(np.abs(v.astype(np.float64)).max())
+    assert vmax > 0
+    dx = 1.0 / spec.n
+    assert abs(full - min(max(dx / vmax, 0.001), 0.1)) <= 1e-6 * full
+    m.close()
