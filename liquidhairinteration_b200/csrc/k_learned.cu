@@ -536,17 +536,22 @@ __global__ void k_pool(const uint16_t* __restrict__ fine, int fny, int fnz, uint
 }
 
 // fine[v][c] = coarse[parent(v)][c] (0 beyond 2 * coarse extent)
+// fine voxel (x, y, z) = coarse voxel (x/2, y/2, z/2), 0 past the coarse
+// grid.  One thread per fine voxel and 8-channel (16-byte) chunk; C is a
+// multiple of 8 and every voxel's channels start on a 16-byte boundary.
 __global__ void k_upsample(const uint16_t* __restrict__ coarse, int cnx, int cny, int cnz, uint16_t* __restrict__ fine,
                            int fnx, int fny, int fnz, int C) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long n = (long long)fnx * fny * fnz * C;
-    if (i >= n) return;
-    const int c = int(i % C);
-    const long long v = i / C;
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned q = unsigned(C) / 8;
+    if (i >= unsigned(fnx) * unsigned(fny) * unsigned(fnz) * q) return;
+    const unsigned v = i / q, ch = i - v * q;
     int x, y, z;
-    dec3(v, fny, fnz, x, y, z);
+    idx3(v, fny, fnz, x, y, z);
     const int px = x >> 1, py = y >> 1, pz = z >> 1;
-    fine[i] = (px < cnx && py < cny && pz < cnz) ? coarse[(((long long)px * cny + py) * cnz + pz) * C + c] : uint16_t(0);
+    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+    if (px < cnx && py < cny && pz < cnz)
+        val = reinterpret_cast<const uint4*>(coarse)[((unsigned(px) * cny + py) * cnz + pz) * q + ch];
+    reinterpret_cast<uint4*>(fine)[i] = val;
 }
 
 // dcoarse[v][c] = sum of the 8 children's dfine (FP32, children in order)
@@ -868,10 +873,10 @@ void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type,
     k_pool<<<nb(b_.vox[2] * 32), 256, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[0], d2[1], d2[2], 32);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, act, b_.h2, nullptr, status_, s);
-    k_upsample<<<nb(b_.vox[1] * 64), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
+    k_upsample<<<nb(b_.vox[1] * 64 / 8), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, act, b_.u1, nullptr, status_, s);
-    k_upsample<<<nb(V0 * 32), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
+    k_upsample<<<nb(V0 * 32 / 8), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, act, b_.u0, nullptr, status_, s);
     launch_conv(b_.u0, 16, W(5), 16, Bv(5), 1, d0, 2, nullptr, 0, nullptr, b_.y, status_, s);
