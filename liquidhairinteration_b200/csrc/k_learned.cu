@@ -144,6 +144,42 @@ struct ConvParams {
     NetStatus* status;
 };
 
+// Epilogue of one output row (TMEM lane = this thread's row; warp-collective
+// loads, so every lane calls it and only valid rows store): mode 0 BF16 with
+// bias, skip and activation; mode 1 FP32, all channels; mode 2 FP32 channel 0.
+__device__ __forceinline__ void conv_store(const ConvParams& P, uint32_t trow, bool valid, long long v) {
+    if (P.mode == 2) {
+        float a[8];
+        tmem_ld8(trow, a);
+        if (valid) P.out_f[v] = a[0] + (P.bias ? P.bias[0] : 0.f);
+        return;
+    }
+    for (int c0 = 0; c0 < P.cout; c0 += 8) {
+        float a[8];
+        tmem_ld8(trow + c0, a);
+        if (!valid) continue;
+        if (P.mode == 1) {
+            float4* o = reinterpret_cast<float4*>(P.out_f + v * P.cout + c0);
+            o[0] = make_float4(a[0], a[1], a[2], a[3]);
+            o[1] = make_float4(a[4], a[5], a[6], a[7]);
+        } else {
+            uint16_t sk[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (P.skip) *reinterpret_cast<uint4*>(sk) = *reinterpret_cast<const uint4*>(P.skip + v * P.cout + c0);
+            uint16_t o[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int c = c0 + k;
+                float val = a[k];
+                if (P.bias && c < P.cout_real) val += P.bias[c];
+                if (P.skip) val += bf16_float(sk[k]);
+                if (P.relu) val = fmaxf(val, 0.f);
+                o[k] = (c < P.cout_real) ? bf16_bits(val) : uint16_t(0);
+            }
+            *reinterpret_cast<uint4*>(P.out_b + v * P.cout + c0) = *reinterpret_cast<uint4*>(o);
+        }
+    }
+}
+
 // out[v][n] = sum_tap sum_k in[v + off(tap)][k] * w[tap][n][k]
 __global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
     extern __shared__ __align__(1024) uint8_t sm[];
@@ -216,37 +252,7 @@ __global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
     __syncwarp();
     // tcgen05.ld is warp-collective: every lane loads, only valid rows store
     if (ok) {
-        const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
-        if (P.mode == 2) {
-            float a[8];
-            tmem_ld8(trow, a);
-            if (valid) P.out_f[v] = a[0] + (P.bias ? P.bias[0] : 0.f);
-        } else {
-            for (int c0 = 0; c0 < P.cout; c0 += 8) {
-                float a[8];
-                tmem_ld8(trow + c0, a);
-                if (!valid) continue;
-                if (P.mode == 1) {
-                    float4* o = reinterpret_cast<float4*>(P.out_f + v * P.cout + c0);
-                    o[0] = make_float4(a[0], a[1], a[2], a[3]);
-                    o[1] = make_float4(a[4], a[5], a[6], a[7]);
-                } else {
-                    uint16_t sk[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                    if (P.skip) *reinterpret_cast<uint4*>(sk) = *reinterpret_cast<const uint4*>(P.skip + v * P.cout + c0);
-                    uint16_t o[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int c = c0 + k;
-                        float val = a[k];
-                        if (P.bias && c < P.cout_real) val += P.bias[c];
-                        if (P.skip) val += bf16_float(sk[k]);
-                        if (P.relu) val = fmaxf(val, 0.f);
-                        o[k] = (c < P.cout_real) ? bf16_bits(val) : uint16_t(0);
-                    }
-                    *reinterpret_cast<uint4*>(P.out_b + v * P.cout + c0) = *reinterpret_cast<uint4*>(o);
-                }
-            }
-        }
+        conv_store(P, tmem + (uint32_t(warp * 32) << 16), valid, v);
     } else if (!ok && valid) {
         // keep the tensor well defined after a timeout
         if (P.mode == 2) P.out_f[v] = 0.f;
@@ -254,6 +260,103 @@ __global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
     if (!ok && tid == 0 && atomicExch(&P.status->timeout, 1) == 0) {
         P.status->pad[0] = 1;  // kernel: convolution
         P.status->pad[1] = last_tap;
+        P.status->pad[2] = int(blockIdx.x);
+    }
+    tc_fence_before();
+    __syncthreads();
+    __syncwarp();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ------------------------------------------------------ brick convolution
+// The same convolution with the 27 taps reading one staged input brick
+// instead of 27 gathers (every layer whose weights and brick fit in shared
+// memory).
+// An output tile is 128 voxels: one x plane, 16 y rows, 8 z (TMEM lane /
+// A row r = (y - y0) * 8 + (z - z0)).  Its input brick, grown by one voxel
+// (3 x 18 x 10), sits in shared memory as one plane per 8-channel chunk with
+// z fastest, so for any tap the 8 z of a y row are one contiguous 8 x 16-byte
+// core matrix: the tap's A operand is the brick at offset (dx, dy, dz), with
+// M-direction stride one brick row (160 bytes) and K-direction stride one
+// plane.  CTAs are persistent and keep all 27 weight tiles resident.
+constexpr int kBrX = 3, kBrY = 18, kBrZ = 10;
+constexpr int kBrVox = kBrX * kBrY * kBrZ;  // 540
+constexpr int kBrPlane = kBrVox * 16;       // bytes of one 8-channel plane
+constexpr size_t kBrickSmemMax = 227 * 1024;
+
+__global__ void __launch_bounds__(kConvM) k_conv_brick(ConvParams P) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int kc = P.cin / 8;
+    const int wbytes = P.cout * P.cin * 2;  // one tap's B tile
+    uint8_t* Bs = sm;
+    uint8_t* Ab = sm + 27 * wbytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ab + kc * kBrPlane);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = P.cout < 32 ? 32u : uint32_t(P.cout);
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(tslot, ncols);
+    for (int i = tid; i < 27 * wbytes / 16; i += kConvM)
+        reinterpret_cast<uint4*>(Bs)[i] = reinterpret_cast<const uint4*>(P.w)[i];
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const int tyn = (P.ny + 15) / 16, tzn = (P.nz + 7) / 8;
+    const long long ntiles = (long long)P.nx * tyn * tzn;
+    const uint32_t idesc = idesc_bf16(kConvM, P.cout, 0, 0);
+    const uint32_t bsbo = uint32_t(kc) * 128;
+    unsigned phase = 0;
+    bool ok = true;
+    long long t = blockIdx.x;
+    for (; t < ntiles; t += gridDim.x) {
+        const int tzi = int(t % tzn);
+        const long long rest = t / tzn;
+        const int tyi = int(rest % tyn), x0 = int(rest / tyn);
+        const int y0 = tyi * 16, z0 = tzi * 8;
+        for (int e = tid; e < kBrVox * kc; e += kConvM) {
+            const int c = e / kBrVox, vb = e - c * kBrVox;
+            const int bx = vb / (kBrY * kBrZ), r2 = vb - bx * (kBrY * kBrZ);
+            const int by = r2 / kBrZ, bz = r2 - by * kBrZ;
+            const int xx = x0 - 1 + bx, yy = y0 - 1 + by, zz = z0 - 1 + bz;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (xx >= 0 && xx < P.nx && yy >= 0 && yy < P.ny && zz >= 0 && zz < P.nz)
+                val = *reinterpret_cast<const uint4*>(P.in + (((long long)xx * P.ny + yy) * P.nz + zz) * P.cin + c * 8);
+            *reinterpret_cast<uint4*>(Ab + c * kBrPlane + vb * 16) = val;
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(Ab), b0 = smem_u32(Bs);
+            for (int tap = 0; tap < kNetTaps; ++tap) {
+                int dx, dy, dz;
+                tap_offset(tap, dx, dy, dz);
+                const uint32_t at = a0 + uint32_t((((dx + 1) * kBrY + (dy + 1)) * kBrZ + (dz + 1)) * 16);
+                const uint32_t bt = b0 + uint32_t(tap * wbytes);
+                for (int k = 0; k < P.cin / 16; ++k)
+                    umma_bf16(tmem, sdesc(at + uint32_t(2 * k * kBrPlane), kBrPlane, kBrZ * 16),
+                              sdesc(bt + k * 256, 128, bsbo), idesc, (tap > 0 || k > 0) ? 1u : 0u);
+            }
+            umma_commit(&bar[0]);
+        }
+        ok = mbar_wait(&bar[0], phase);
+        phase ^= 1u;
+        tc_fence_after();
+        __syncwarp();
+        const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
+        const bool valid = y < P.ny && z < P.nz;
+        if (ok) conv_store(P, tmem + (uint32_t(warp * 32) << 16), valid, ((long long)x0 * P.ny + y) * P.nz + z);
+        tc_fence_before();
+        // the brick and TMEM are free for the next tile; a timeout ends the CTA
+        if (!__syncthreads_and(ok)) break;
+    }
+    if (t < ntiles && tid == 0 && atomicExch(&P.status->timeout, 1) == 0) {
+        P.status->pad[0] = 3;  // kernel: brick convolution
         P.status->pad[2] = int(blockIdx.x);
     }
     tc_fence_before();
@@ -813,6 +916,24 @@ void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const
     P.out_f = out_f;
     P.status = st;
     if (P.nvox == 0) return;
+    // the brick kernel keeps all 27 weight tiles and the brick in shared
+    // memory: every layer but the 64 -> 64 input gradient fits
+    const size_t brick_smem = size_t(27) * cout * cin * 2 + size_t(cin / 8) * kBrPlane + 16;
+    if (brick_smem <= kBrickSmemMax) {
+        const size_t smem = brick_smem;
+        static bool attr = false;
+        if (!attr) {
+            LHI_CUDA(cudaFuncSetAttribute(k_conv_brick, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(kBrickSmemMax)));
+            attr = true;
+        }
+        const long long ntiles = (long long)d[0] * ((d[1] + 15) / 16) * ((d[2] + 7) / 8);
+        const long long per_sm = std::max<long long>(1, (200LL * 1024) / (long long)smem);
+        const unsigned grid = unsigned(std::min<long long>(ntiles, kSMs * per_sm));
+        k_conv_brick<<<grid, kConvM, smem, s>>>(P);
+        LHI_LAUNCH_CHECK();
+        return;
+    }
     const size_t smem = size_t(2) * kConvM * cin * 2 + size_t(2) * cout * cin * 2 + 32;
     k_conv<<<unsigned((P.nvox + kConvM - 1) / kConvM), kConvM, smem, s>>>(P);
     LHI_LAUNCH_CHECK();
