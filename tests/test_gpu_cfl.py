@@ -14,7 +14,9 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
 def test_cfl_after_step_and_after_set_particles(lhi, prec):
     spec = scenes.dam(32)
-    m = gpu_model(spec, prec, spec.solver_params(coarse_cells=64))
+    # FP32 keeps x in float: its true residual stalls near 1e-5 relative, so
+    # the FP32 solve stops on the recursive residual alone
+    m = gpu_model(spec, prec, spec.solver_params(coarse_cells=64, true_residual_every=0 if prec == "fp32" else 10))
     pos, vel = scenes.seed(spec, "fp64" if prec == "fp64" else "fp32")
     m.GetParticleSystem().SetParticles(pos, vel)
     for _ in range(3):
