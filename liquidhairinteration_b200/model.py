@@ -219,11 +219,22 @@ class ParticleSystem:
     def WriteToFile(self, filename, isAppend=False):
         """ParticleSystem::WriteToFile (ParticleSystem.cpp:67-85): count line
         then comma-separated positions, std::ostream default formatting."""
-        pos = self.GetPositions()
-        with open(filename, "a" if isAppend else "w") as f:
-            f.write(f"{pos.shape[0]}\n")
-            f.write("".join("%.6g," % float(v) for v in pos.reshape(-1)))
-            f.write("\n")
+        from . import snapshots
+        snapshots.write_frame(filename, self.GetPositions(), append=isAppend)
+
+    def SaveCheckpoint(self, filename, **counters):
+        """Binary checkpoint of the whole particle state (exact bits) plus
+        the caller's counters, e.g. step and time."""
+        from . import snapshots
+        pos, vel, aff = self.GetParticles()
+        snapshots.save_checkpoint(filename, pos, vel, aff, **counters)
+
+    def LoadCheckpoint(self, filename):
+        """Restores a SaveCheckpoint file; returns its counters."""
+        from . import snapshots
+        c = snapshots.load_checkpoint(filename)
+        self.SetParticles(c.pop("pos"), c.pop("vel"), c.pop("affine"))
+        return c
 
 
 class CGSolver:

@@ -1,6 +1,7 @@
-"""LiquidModel<3>::GetCFL (LiquidModel.h:49-55): the reference's clamp of
-dx / max|v| over the particles' velocities, the same after a step and after
-the same particles are set again."""
+"""Around the step: LiquidModel<3>::GetCFL (LiquidModel.h:49-55), the
+reference's clamp of dx / max|v| over the particles' velocities, the same
+after a step and after the same particles are set again; and the particle
+checkpoint, which restores the exact particle state in a fresh model."""
 import numpy as np
 import pytest
 
@@ -32,3 +33,27 @@ def test_cfl_after_step_and_after_set_particles(lhi, prec):
     dx = 1.0 / spec.n
     assert abs(full - min(max(dx / vmax, 0.001), 0.1)) <= 1e-6 * full
     m.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_checkpoint_restores_particles(lhi, prec, tmp_path):
+    """ParticleSystem SaveCheckpoint / LoadCheckpoint through the C-ABI: a
+    fresh model loaded from a checkpoint holds the same particle bits, in
+    the caller's order, and gets the counters back."""
+    spec = scenes.dam(16)
+    m = gpu_model(spec, prec, spec.solver_params(coarse_cells=64, true_residual_every=0 if prec == "fp32" else 10))
+    pos, vel = scenes.seed(spec, "fp64" if prec == "fp64" else "fp32")
+    m.GetParticleSystem().SetParticles(pos, vel)
+    for _ in range(2):
+        m.PreStep(spec.dt)
+        m.Step(spec.dt)
+    path = tmp_path / "ck.npz"
+    m.GetParticleSystem().SaveCheckpoint(path, step=2, time=2 * spec.dt)
+    saved = m.GetParticleSystem().GetParticles()
+    m2 = gpu_model(spec, prec)
+    counters = m2.GetParticleSystem().LoadCheckpoint(path)
+    assert counters == {"step": 2, "time": 2 * spec.dt}
+    for a, b in zip(m2.GetParticleSystem().GetParticles(), saved):
+        assert np.array_equal(a, b)
+    m.close()
+    m2.close()
