@@ -5,6 +5,8 @@ any change to them.
 
 - Fused red-black sweep (k_rb_fused): the indices of rb_eval for every cell
   of both colour phases lie inside the Z, R/D/CZ, CX, CY and mask boxes.
+- TMA SpMV and restriction (k_spmv_tma, k_restrict_tma): every box index a
+  thread forms, and the restriction's 8 children per coarse cell.
 - Brick convolution (k_conv_brick): for every tap and K step, each 8-row
   core matrix the tensor-core instruction reads (16 along M, 2 along K) lies
   inside the input brick and is the intended brick row of 8 z voxels, and
@@ -103,3 +105,33 @@ def test_brick_convolution_operands_inside_tiles(cin, cout):
                 for j in range(2):
                     start = b0 + g * kc * 128 + j * 128
                     assert bt <= start and start + 128 <= bt + wbytes
+
+
+def test_spmv_and_restriction_indices_inside_boxes():
+    """k_spmv_tma and k_restrict_tma: thread (warp wp = x, lane = z) and row
+    ly of a tile read p / z (grown by one cell, z from z0 - 4), diag, the
+    coefficients with the -x / -y / -z faces and the mask; the restriction's
+    coarse cells read their 8 children from the residual tile."""
+    p_box = _const("k_solver.cu", "kP")
+    d_box = _const("k_solver.cu", "kD")
+    cx_box, cy_box, cz_box = (_const("k_solver.cu", n) for n in ("kCX", "kCY", "kCZ"))
+    assert (p_box, d_box, cx_box, cy_box, cz_box) == (10 * 10 * 40, 8 * 8 * 32, 9 * 8 * 32, 8 * 9 * 32, 8 * 8 * 36)
+    for wp in range(8):
+        for ly in range(8):
+            for lane in range(32):
+                pi = ((wp + 1) * 10 + (ly + 1)) * 40 + (lane + 4)
+                ci = (wp * 8 + ly) * 32 + lane
+                for off in (0, 400, -400, 40, -40, 1, -1):
+                    assert 0 <= pi + off < p_box
+                assert 0 <= ci < d_box and 0 <= ci + 256 < cx_box
+                assert 0 <= (wp * 9 + ly + 1) * 32 + lane < cy_box and 0 <= (wp * 9 + ly) * 32 + lane < cy_box
+                assert 0 <= (wp * 8 + ly) * 36 + lane + 3 and (wp * 8 + ly) * 36 + lane + 4 < cz_box
+    seen = set()
+    for t in range(256):  # one coarse cell per thread
+        i, j, k = t >> 6, (t >> 4) & 3, t & 15
+        for c8 in range(8):
+            a, b, c = (c8 >> 2) & 1, (c8 >> 1) & 1, c8 & 1
+            idx = ((2 * i + a) * 8 + (2 * j + b)) * 32 + 2 * k + c
+            assert 0 <= idx < d_box
+            seen.add(idx)
+    assert len(seen) == d_box  # the 256 coarse cells cover the fine tile exactly once
