@@ -2,7 +2,7 @@
 // the checker for the CUDA path, never part of it.
 //
 // Restates the reference's 3D liquid path in plain C++ (float = the
-// reference's Scalar, or double), single-threaded and deterministic.  The
+// reference's Scalar, or double), deterministic.  The
 // arithmetic follows the reference expression by expression, including:
 //   * Eigen's fixed-size reductions: squaredNorm/dot of a 3-vector evaluate
 //     as a0 + (a1 + a2) (Eigen redux_novec_unroller splits the range in half);
@@ -17,7 +17,22 @@
 // flags without ordering) are replaced by deterministic
 // semantics: serial sums in PCG; extrapolation flags either Jacobi (GPU
 // semantics) or serial x-y-z order (the reference with one OpenMP thread).
+//
+// Threads: only loops whose result cannot depend on the thread count run in
+// parallel (OpenMP, lho_set_threads):
+//   * loops whose iterations write disjoint cells, faces, nodes or particles
+//     (one colour of a red-black sweep, restriction, prolongation, matrix and
+//     right-hand side, G2P, advection, Jacobi extrapolation, ...);
+//   * scatters (P2G sums, the liquid SDF's minimum) split into x slabs of the
+//     target grid: each thread walks every particle in the serial order and
+//     keeps the window nodes of its own slab, so every node receives the same
+//     terms in the same order as in the serial loop;
+//   * every reduction (dot products, residual norms) is a serial pass in the
+//     serial loop's order over values the parallel pass stored.
+// So the results are bit-identical for any thread count.
 #include "lhi_oracle.h"
+
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -25,9 +40,18 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <string>
 #include <vector>
 
 namespace {
+
+int g_threads = 0;  // 0: every processor
+inline int nthreads() { return g_threads > 0 ? g_threads : omp_get_num_procs(); }
+// [lo, hi) of n split into nt near-equal parts, part t
+inline void slab(int n, int t, int nt, int& lo, int& hi) {
+    lo = int((long long)n * t / nt);
+    hi = int((long long)n * (t + 1) / nt);
+}
 
 template <class S> S eps_of() { return S(1e-8); }  // EPSILON (Definition.h:88)
 
@@ -176,7 +200,7 @@ template <class S> struct Model {
     lhi_solver_params sp;
     int maxLevel;
     S tolerance, smoothFactor;
-    Field<S> rhs, p, x;
+    Field<S> rhs, p, x, tmp;  // tmp: the true residual when r is not overwritten
     std::vector<Field<S>> r, z, Adiag;
     std::vector<std::vector<S>> Acoef;  // 6 per cell
     std::vector<Dims> ldims;
@@ -237,6 +261,7 @@ template <class S> struct Model {
         rhs.resize(nx, ny, nz);
         p.resize(nx, ny, nz);
         x.resize(nx, ny, nz);
+        tmp.resize(nx, ny, nz);
     }
 
     // ---------------------------------------------------------- Grid helpers
@@ -322,6 +347,7 @@ template <class S> struct Model {
 
     // ------------------------------------------------------- solid / liquid
     void set_boundary(const lhi_boundary_node* nodes, int32_t count, int32_t root) {
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 0; xi < nx + 1; ++xi)
             for (int yi = 0; yi < ny + 1; ++yi)
                 for (int zi = 0; zi < nz + 1; ++zi) {
@@ -335,14 +361,17 @@ template <class S> struct Model {
     // LiquidModel<3>::ComputeSolidPhi face fractions (LiquidModel.cpp:574-610):
     // liquidWx uses the y-edge, liquidWy and liquidWz both use the x-edge.
     void compute_face_fractions() {
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 0; xi < nx + 1; ++xi)
             for (int yi = 0; yi < ny; ++yi)
                 for (int zi = 0; zi < nz; ++zi)
                     lwx(xi, yi, zi) = open_fraction(solidPhi(xi, yi, zi), solidPhi(xi, yi + 1, zi));
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 0; xi < nx; ++xi)
             for (int yi = 0; yi < ny + 1; ++yi)
                 for (int zi = 0; zi < nz; ++zi)
                     lwy(xi, yi, zi) = open_fraction(solidPhi(xi, yi, zi), solidPhi(xi + 1, yi, zi));
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 0; xi < nx; ++xi)
             for (int yi = 0; yi < ny; ++yi)
                 for (int zi = 0; zi < nz + 1; ++zi)
@@ -360,11 +389,20 @@ template <class S> struct Model {
         int dX = int(std::ceil(radius / dx[0]));
         int dY = int(std::ceil(radius / dx[1]));
         int dZ = int(std::ceil(radius / dx[2]));
+        // x slabs of the cells; every thread walks all particles in order
+#pragma omp parallel num_threads(nthreads())
+        {
+            int xlo, xhi;
+            slab(nx, omp_get_thread_num(), omp_get_num_threads(), xlo, xhi);
+            liquid_phi_slab(dX, dY, dZ, xlo, xhi);
+        }
+    }
+    void liquid_phi_slab(int dX, int dY, int dZ, int xlo, int xhi) {
         for (int64_t pi = 0; pi < np; ++pi) {
             const S* q = &pos[3 * pi];
             int c[3];
             point2index(q, c);
-            for (int xi = std::max(0, c[0] - dX); xi <= std::min(nx - 1, c[0] + dX); ++xi)
+            for (int xi = std::max(xlo, c[0] - dX); xi <= std::min(xhi - 1, c[0] + dX); ++xi)
                 for (int yi = std::max(0, c[1] - dY); yi <= std::min(ny - 1, c[1] + dY); ++yi)
                     for (int zi = std::max(0, c[2] - dZ); zi <= std::min(nz - 1, c[2] + dZ); ++zi) {
                         // Index2Point: (index + 0.5) * dx + minCoord
@@ -382,11 +420,14 @@ template <class S> struct Model {
     // LiquidModel<3>::Particle2Grid (LiquidModel.cpp:614-721), serial
     // particle order; zero-weight nodes add +-0 and are skipped.
     template <int A>
-    void p2g_component(const S* q, const S* v, const S* C, const S g[3], const int ci[3], const int del[3]) {
+    void p2g_component(const S* q, const S* v, const S* C, const S g[3], const int ci[3], const int del[3],
+                       int xlo, int xhi) {
         Field<S>& wf = (A == 0) ? wx : (A == 1) ? wy : wz;
         Field<S>& vf = (A == 0) ? vx : (A == 1) ? vy : vz;
         int hx = nx - 1 + (A == 0), hy = ny - 1 + (A == 1), hz = nz - 1 + (A == 2);
-        for (int ddx = -del[0]; ddx <= del[0]; ++ddx)
+        // window columns in this thread's slab, in the serial order
+        const int d0 = std::max(-del[0], xlo - ci[0]), d1 = std::min(del[0], xhi - 1 - ci[0]);
+        for (int ddx = d0; ddx <= d1; ++ddx)
             for (int ddy = -del[1]; ddy <= del[1]; ++ddy)
                 for (int ddz = -del[2]; ddz <= del[2]; ++ddz) {
                     int xi = ci[0] + ddx, yi = ci[1] + ddy, zi = ci[2] + ddz;
@@ -411,31 +452,45 @@ template <class S> struct Model {
         if (np == 0) return;
         int del[3];
         for (int i = 0; i < 3; ++i) del[i] = int(std::ceil(radius / dx[i]));
-        for (int64_t pi = 0; pi < np; ++pi) {
-            const S* q = &pos[3 * pi];
-            const S* v = &vel[3 * pi];
-            const S* C = &aff[9 * pi];
-            S g[3];
-            int ci[3];
-            for (int i = 0; i < 3; ++i) {
-                g[i] = (q[i] - minc[i]) / dx[i];  // cwiseQuotient
-                ci[i] = int(g[i]);                // cast<Integer>
+        // x slabs of each component's faces; every thread walks all particles in order
+#pragma omp parallel num_threads(nthreads())
+        {
+            const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+            int lo[3], hi[3];
+            slab(nx + 1, t, nt, lo[0], hi[0]);
+            slab(nx, t, nt, lo[1], hi[1]);
+            slab(nx, t, nt, lo[2], hi[2]);
+            const int lmin = std::min(lo[0], lo[1]), hmax = std::max(hi[0], hi[1]);
+            for (int64_t pi = 0; pi < np; ++pi) {
+                const S* q = &pos[3 * pi];
+                const S* v = &vel[3 * pi];
+                const S* C = &aff[9 * pi];
+                S g[3];
+                int ci[3];
+                for (int i = 0; i < 3; ++i) {
+                    g[i] = (q[i] - minc[i]) / dx[i];  // cwiseQuotient
+                    ci[i] = int(g[i]);                // cast<Integer>
+                }
+                if (ci[0] + del[0] < lmin || ci[0] - del[0] >= hmax) continue;  // no node in this slab
+                p2g_component<0>(q, v, C, g, ci, del, lo[0], hi[0]);
+                p2g_component<1>(q, v, C, g, ci, del, lo[1], hi[1]);
+                p2g_component<2>(q, v, C, g, ci, del, lo[2], hi[2]);
             }
-            p2g_component<0>(q, v, C, g, ci, del);
-            p2g_component<1>(q, v, C, g, ci, del);
-            p2g_component<2>(q, v, C, g, ci, del);
         }
         normalize(vx, wx);
         normalize(vy, wy);
         normalize(vz, wz);
     }
     void normalize(Field<S>& v, const Field<S>& w) {
-        for (size_t i = 0; i < v.d.size(); ++i) v.d[i] = !is_small(w.d[i]) ? v.d[i] / w.d[i] : S(0.0);
+        const long long n = (long long)v.d.size();
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+        for (long long i = 0; i < n; ++i) v.d[i] = !is_small(w.d[i]) ? v.d[i] / w.d[i] : S(0.0);
     }
 
     // LiquidModel<3>::ApplyGravity (LiquidModel.cpp:899-910)
     void apply_gravity(S dt) {
         S gdt = gravity * dt;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 1; xi < nx - 1; ++xi)
             for (int yi = 1; yi < ny; ++yi)
                 for (int zi = 1; zi < nz - 1; ++zi) vy(xi, yi, zi) += gdt;
@@ -473,6 +528,7 @@ template <class S> struct Model {
         if (np == 0) return;
         int del[3];
         for (int i = 0; i < 3; ++i) del[i] = int(std::ceil(radius / dx[i]));
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int64_t pi = 0; pi < np; ++pi) {
             const S* q = &pos[3 * pi];
             S g[3];
@@ -495,6 +551,7 @@ template <class S> struct Model {
     // velocity is never stored by the reference, so only positions change.
     void advect(S dt) {
         if (np == 0) return;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int64_t pi = 0; pi < np; ++pi) {
             S* q = &pos[3 * pi];
             const S* v = &vel[3 * pi];
@@ -520,13 +577,18 @@ template <class S> struct Model {
         int x0 = 1, x1 = (A == 0) ? nx : nx - 1;  // exclusive upper bounds
         int y0 = 1, y1 = (A == 1) ? ny : ny - 1;
         int z0 = 1, z1 = (A == 2) ? nz : nz - 1;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = x0; xi < x1; ++xi)
             for (int yi = y0; yi < y1; ++yi)
                 for (int zi = z0; zi < z1; ++zi) isValid(xi, yi, zi) = (lw(xi, yi, zi) > S(0.0)) ? 1 : 0;
         Field<uint8_t> prev;
+        // Jacobi flags: every face reads the previous sweep's flags only, so
+        // x planes are independent; serial flags keep the x-y-z order.
+        const int nt = (mode == LHO_EXTRAP_JACOBI) ? nthreads() : 1;
         for (int iter = 0; iter < extrap_iters; ++iter) {
             if (mode == LHO_EXTRAP_JACOBI) prev = isValid;
             const Field<uint8_t>& rv = (mode == LHO_EXTRAP_JACOBI) ? prev : isValid;
+#pragma omp parallel for num_threads(nt) schedule(static)
             for (int xi = x0; xi < x1; ++xi)
                 for (int yi = y0; yi < y1; ++yi)
                     for (int zi = z0; zi < z1; ++zi) {
@@ -605,6 +667,7 @@ template <class S> struct Model {
     }
 
     void build_rhs() {  // PressureSolver.cpp:682-698
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 0; xi < nx; ++xi)
             for (int yi = 0; yi < ny; ++yi)
                 for (int zi = 0; zi < nz; ++zi) {
@@ -660,6 +723,7 @@ template <class S> struct Model {
             S ldx[3] = {S(factor) * dx[0], S(factor) * dx[1], S(factor) * dx[2]};
             Field<S>& D = Adiag[level];
             std::vector<S>& Cf = Acoef[level];
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
             for (int xi = 0; xi < d.nx; ++xi)
                 for (int yi = 0; yi < d.ny; ++yi)
                     for (int zi = 0; zi < d.nz; ++zi) {
@@ -716,6 +780,8 @@ template <class S> struct Model {
     void smooth(int level, int phase) {
         const Dims& d = ldims[level];
         Field<S>& zl = z[level];
+        // one colour: its cells are not each other's neighbours
+#pragma omp parallel for num_threads(d.nx >= 16 ? nthreads() : 1) schedule(static)
         for (int xi = 0; xi < d.nx; ++xi)
             for (int yi = 0; yi < d.ny; ++yi)
                 for (int zi = 0; zi < d.nz; ++zi) {
@@ -735,6 +801,7 @@ template <class S> struct Model {
     void restrict_(int toLevel) {
         int from = toLevel - 1;
         const Dims& d = ldims[toLevel];
+#pragma omp parallel for num_threads(d.nx >= 8 ? nthreads() : 1) schedule(static)
         for (int xi = 0; xi < d.nx; ++xi)
             for (int yi = 0; yi < d.ny; ++yi)
                 for (int zi = 0; zi < d.nz; ++zi) {
@@ -756,6 +823,7 @@ template <class S> struct Model {
     void prolong(int toLevel) {
         int from = toLevel + 1;
         const Dims& d = ldims[from];
+#pragma omp parallel for num_threads(d.nx >= 8 ? nthreads() : 1) schedule(static)
         for (int xi = 0; xi < d.nx; ++xi)
             for (int yi = 0; yi < d.ny; ++yi)
                 for (int zi = 0; zi < d.nz; ++zi) {
@@ -821,13 +889,20 @@ template <class S> struct Model {
 
     // ||b - A x|| over interior fluid cells; optionally stores it into r[0].
     S true_residual(bool store) {
+        Field<S>& out = store ? r[0] : tmp;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+        for (int xi = lo(); xi < hx(); ++xi)
+            for (int yi = lo(); yi < hy(); ++yi)
+                for (int zi = lo(); zi < hz(); ++zi) {
+                    if (!interior_fluid(xi, yi, zi)) continue;
+                    out(xi, yi, zi) = rhs(xi, yi, zi) - get_ax(x, xi, yi, zi, 0);
+                }
         S acc = S(0.0);
         for (int xi = lo(); xi < hx(); ++xi)
             for (int yi = lo(); yi < hy(); ++yi)
                 for (int zi = lo(); zi < hz(); ++zi) {
                     if (!interior_fluid(xi, yi, zi)) continue;
-                    S rr = rhs(xi, yi, zi) - get_ax(x, xi, yi, zi, 0);
-                    if (store) r[0](xi, yi, zi) = rr;
+                    S rr = out(xi, yi, zi);
                     acc += rr * rr;
                 }
         return std::sqrt(acc);
@@ -839,37 +914,51 @@ template <class S> struct Model {
         solver_init();
         build_rhs();
         build_lhs(rho, dt);
-        for (size_t i = 0; i < rhs.d.size(); ++i)
+        const long long ncells = (long long)rhs.d.size();
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+        for (long long i = 0; i < ncells; ++i)
             if (!(liquidPhi.d[i] > S(0.0))) r[0].d[i] = rhs.d[i];
         apply_preconditioner();
-        for (size_t i = 0; i < p.d.size(); ++i)
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+        for (long long i = 0; i < ncells; ++i)
             if (!(liquidPhi.d[i] > S(0.0))) p.d[i] = z[0].d[i];
         oldRZ = reduce(r[0], z[0]);
         S residual = std::sqrt(reduce(r[0], r[0]));
         S residual0 = residual;
         S threshold = (sp.tolerance_mode == LHI_TOL_RELATIVE) ? S(tolerance * residual0) : tolerance;
         int iters = 0;
-        Field<S> Ap;
-        if (sp.cg_variant == LHI_CG_FLEXIBLE) Ap.resize(nx, ny, nz);
+        Field<S> Ap;  // A p of the iteration (p does not change between its two uses)
+        Ap.resize(nx, ny, nz);
         for (int iter = 0; iter < sp.max_iterations; ++iter) {
             if (residual < threshold) break;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+            for (int xi = lo(); xi < hx(); ++xi)
+                for (int yi = lo(); yi < hy(); ++yi)
+                    for (int zi = lo(); zi < hz(); ++zi) {
+                        if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
+                        Ap(xi, yi, zi) = get_ax(p, xi, yi, zi, 0);
+                    }
             S denom = S(0.0);
             for (int xi = lo(); xi < hx(); ++xi)
                 for (int yi = lo(); yi < hy(); ++yi)
                     for (int zi = lo(); zi < hz(); ++zi) {
                         if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
-                        S ap = get_ax(p, xi, yi, zi, 0);
-                        if (sp.cg_variant == LHI_CG_FLEXIBLE) Ap(xi, yi, zi) = ap;
-                        denom += p(xi, yi, zi) * ap;
+                        denom += p(xi, yi, zi) * Ap(xi, yi, zi);
                     }
             alpha = oldRZ / denom;
-            residual = S(0.0);
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
             for (int xi = lo(); xi < hx(); ++xi)
                 for (int yi = lo(); yi < hy(); ++yi)
                     for (int zi = lo(); zi < hz(); ++zi) {
                         if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
                         x(xi, yi, zi) += alpha * p(xi, yi, zi);
-                        r[0](xi, yi, zi) -= alpha * get_ax(p, xi, yi, zi, 0);
+                        r[0](xi, yi, zi) -= alpha * Ap(xi, yi, zi);
+                    }
+            residual = S(0.0);
+            for (int xi = lo(); xi < hx(); ++xi)
+                for (int yi = lo(); yi < hy(); ++yi)
+                    for (int zi = lo(); zi < hz(); ++zi) {
+                        if (liquidPhi(xi, yi, zi) > S(0.0)) continue;
                         residual += r[0](xi, yi, zi) * r[0](xi, yi, zi);
                     }
             residual = std::sqrt(residual);
@@ -890,7 +979,8 @@ template <class S> struct Model {
             } else {
                 beta = newRZ / oldRZ;
             }
-            for (size_t i = 0; i < p.d.size(); ++i)
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+            for (long long i = 0; i < ncells; ++i)
                 if (!(liquidPhi.d[i] > S(0.0))) p.d[i] = z[0].d[i] + beta * p.d[i];
             oldRZ = newRZ;
         }
@@ -907,6 +997,7 @@ template <class S> struct Model {
     // LiquidModel<3>::SolvePressure velocity update (LiquidModel.cpp:834-889)
     void velocity_update(S dt) {
         S rho = density;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
         for (int xi = 1; xi < nx - 1; ++xi)
             for (int yi = 1; yi < ny - 1; ++yi)
                 for (int zi = 1; zi < nz - 1; ++zi) {
@@ -1039,6 +1130,16 @@ int64_t spawn_t(const double mn[3], const double mx[3], double defr, int64_t max
 }  // namespace
 
 extern "C" {
+
+// Error text of the scene generator compiled into this library (the CUDA
+// library keeps its own copy of the same function).
+static thread_local std::string g_scene_error;
+extern "C" void lhi_set_error_message(const char* msg) { g_scene_error = msg ? msg : ""; }
+const char* lho_last_error(void) { return g_scene_error.c_str(); }
+
+void lho_set_threads(int32_t n) { g_threads = n > 0 ? n : 0; }
+
+int32_t lho_get_threads(void) { return nthreads(); }
 
 lho_model* lho_create(const lhi_grid_desc* grid, const lhi_solver_params* solver,
                       const lhi_liquid_params* liquid, int32_t dbl) {

@@ -4,8 +4,12 @@
  * A plain C++ restatement of the reference's 3D liquid path
  * (LiquidModel.cpp:476-1134, PressureSolver.cpp:420-936, Grid.cpp:84-193,
  * Kernel.h:12-31, MathUtils.h:8-33, MathUtils.cpp:29-35,75-88,
- * Boundary.h:38-90, ParticleSystem.cpp:7-64), single-threaded and
- * deterministic, in float (the reference's Scalar) or double.
+ * Boundary.h:38-90, ParticleSystem.cpp:7-64), deterministic (bit-identical
+ * for any thread count), in float (the reference's Scalar) or double.
+ *
+ * The library also carries the scene generator (lhi_scene_seed_particles and
+ * friends, built from liquidhairinteration_b200/csrc/scene.cpp), so CPU-only
+ * runs of the reference arm seed their particles without the CUDA library.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
  * load this library, and only as the checker.  The product never calls it.
@@ -33,6 +37,14 @@ extern "C" {
                                run with one OpenMP thread (LiquidModel.cpp:964-975) */
 
 typedef struct lho_model lho_model;
+
+/* Threads of the oracle's parallel loops (0: every processor, the default).
+   Results are bit-identical for any count: only loops whose iterations write
+   disjoint data run in parallel, and every sum is taken serially. */
+LHO_API void lho_set_threads(int32_t n);
+LHO_API int32_t lho_get_threads(void);
+/* Message of the last failed scene-generator call in this library. */
+LHO_API const char* lho_last_error(void);
 
 /* dbl = 0: Scalar float; dbl = 1: Scalar double.  Host buffers use Scalar. */
 LHO_API lho_model* lho_create(const lhi_grid_desc* grid, const lhi_solver_params* solver,

@@ -57,6 +57,11 @@ def _load_oracle():
     lib.lho_solver_get_ax.argtypes = [_vp, C.c_int32, _vp, _vp]
     lib.lho_cell_keys.argtypes = [_vp, _vp]
     lib.lho_sort_by_cell.argtypes = [_vp, _vp, _vp]
+    lib.lho_set_threads.argtypes = [C.c_int32]
+    lib.lho_get_threads.restype = C.c_int32
+    lib.lhi_scene_seed_particles.argtypes = [C.POINTER(abi.GridDesc), C.POINTER(abi.BoundaryNode), C.c_int32,
+                                             C.c_int32, C.POINTER(abi.FluidPrim), C.c_int32, C.c_uint64,
+                                             C.c_int32, C.POINTER(C.c_int64), _vp, _vp]
     lib.lho_spawn_lattice.restype = C.c_int64
     lib.lho_spawn_lattice.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
                                       C.c_int64, C.c_int32, _vp]
@@ -240,6 +245,39 @@ class Oracle:
         cs = np.empty(self.n[0] * self.n[1] * self.n[2] + 1, np.int32)
         self.lib.lho_sort_by_cell(self.h, _ptr(ids), _ptr(cs))
         return ids, cs
+
+
+def set_threads(n):
+    """Threads of the oracle's parallel loops (0: every processor).  Results
+    do not depend on it."""
+    oracle_lib().lho_set_threads(int(n))
+
+
+def get_threads():
+    return int(oracle_lib().lho_get_threads())
+
+
+def seed_scene(spec, precision="fp32"):
+    """(positions, velocities) of a scene's seeded particles from the scene
+    generator compiled into the oracle library: the same particles as the
+    CUDA library's lhi_scene_seed_particles, with no CUDA library loaded."""
+    lib = oracle_lib()
+    prec = {"fp32": abi.PRECISION_FP32, "mixed": abi.PRECISION_MIXED, "fp64": abi.PRECISION_FP64}[precision]
+    dt = np.float64 if precision == "fp64" else np.float32
+    grid = spec.grid_desc()
+    nodes = abi.boundary_array(spec.boundary)
+    prims = abi.fluid_array(spec.prims)
+    n = C.c_int64()
+    args = (C.byref(grid), nodes, len(spec.boundary), 0, prims, len(spec.prims), int(spec.seed), prec, C.byref(n))
+    rc = lib.lhi_scene_seed_particles(*args, None, None)
+    if rc:
+        raise RuntimeError(f"lhi_scene_seed_particles failed ({rc})")
+    pos = np.empty((n.value, 3), dt)
+    vel = np.empty((n.value, 3), dt)
+    rc = lib.lhi_scene_seed_particles(*args, _ptr(pos), _ptr(vel))
+    if rc:
+        raise RuntimeError(f"lhi_scene_seed_particles failed ({rc})")
+    return pos, vel
 
 
 def spawn_lattice(min_coord, max_coord, default_radius, max_count, dbl=False):
