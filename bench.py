@@ -15,7 +15,14 @@ steps, and downloads it again.
 
 The reference arm (--impl reference) times the reference's own CPU code
 (oracle/_ref/libref.so, its sources compiled from the reference tree) on
-this workload with all host threads; see reference_step_sample().
+this very workload: the 256^3 scene with its 32M particles, one full
+PreStep + Step per timed step, with the OpenMP thread count that a short
+calibration on the 32^3 scene finds fastest.  It loads no CUDA library: the
+particles come from the scene generator compiled into the oracle library.
+
+error_vs_fp64_oracle (our arm, after every timed region): one projection of
+the scene's current state on the GPU against the FP64 CPU oracle solved to
+||r||/||b|| <= 1e-12 on the same float inputs.
 """
 import argparse
 import ctypes as C
@@ -36,12 +43,14 @@ UNIT = "ms/step"
 # domain's outer cell layer its update region and smoother break down), so the
 # reference arm runs its solver for the iteration count our MGPCG needs on
 # this workload.
-REFERENCE_PCG_ITERATIONS = 24
-# The reference arm times the full reference step on the same scene at 32^3
-# (1/512 of the cells and particles) and scales the time by 512.  Every
+REFERENCE_PCG_ITERATIONS = 21
+# cpu_baseline of our arm: a bounded sample, the full reference step on the
+# same scene at 32^3 (1/512 of the cells and particles), time x512.  Every
 # reference loop is linear in cells or particles and the small grid is
 # cache-resident, so the extrapolation favours the reference.
 REFERENCE_SAMPLE_N = 32
+# the grid inputs of a pressure solve, shared by the GPU and the oracle check
+GRID_INPUTS = ("vx", "vy", "vz", "liquidPhi", "liquidWx", "liquidWy", "liquidWz")
 
 
 def parse():
@@ -49,13 +58,17 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "replica-check"],
+                    help="replica-check: the launcher and rank plumbing alone (gloo on CPU, no GPU work)")
     ap.add_argument("--scene", default="dam256")
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eager", action="store_true", help="host-driven PCG loop instead of the solve graph")
     ap.add_argument("--no-fpcg", action="store_true", help="skip the learned-preconditioner FPCG leg")
+    ap.add_argument("--no-oracle-check", action="store_true", help="skip error_vs_fp64_oracle")
+    ap.add_argument("--ref-steps", type=int, default=1,
+                    help="reference arm: full-size reference steps timed (each takes minutes)")
     return ap.parse_args()
 
 
@@ -306,6 +319,12 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(spec)
 
+    # ---- the checker, after every timed region: one projection against the
+    # FP64 oracle (rank 0 of a single-replica run)
+    check = None
+    if rank == 0 and world == 1 and not args.no_oracle_check:
+        check = oracle_check(model, spec)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(ms_step, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -326,6 +345,7 @@ def run_ours(args):
             "particles_per_s": round(n_particles / (ms_step * 1e-3), 1),
             "scenes_per_s": round(world * 1000.0 / ms_step, 3),
             "fpcg": fpcg,
+            "error_vs_fp64_oracle": check,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clock_info,
             "kernel_ms_per_step": {k: round(v[1] / prof_steps, 3) for k, v in prof.items()},
@@ -376,30 +396,82 @@ def run_fpcg(args, spec, stream_of, steps=None):
     return out
 
 
+# ------------------------------------------------------------- checker
+def oracle_check(model, spec):
+    """Error of one projection against the FP64 oracle.
+
+    From the model's current state (after the timed steps): PreStep, P2G and
+    gravity on the GPU; the GPU's float grid inputs then go to both the GPU
+    projection (the handle's own precision and stopping rule) and the FP64
+    CPU oracle, which solves the same system to ||r||/||b|| <= 1e-12
+    (CGSolver<3>::Solve, PressureSolver.cpp:839-934) and applies the same
+    velocity update.  Reports the pressure's relative L2 error and the
+    post-projection divergence max-norm of both (LiquidModel.cpp:1066-1083,
+    max-norm over the cells whose six faces the update touches)."""
+    import numpy as np
+    from oracle import pyoracle as po
+    po.set_threads(0)
+    t0 = time.perf_counter()
+    dt = spec.dt
+    model.PreStep(dt)
+    model.Particle2Grid()
+    model.ApplyGravity(dt)
+    fields = {f: model.field(f) for f in GRID_INPUTS}
+    div_before = model.ComputeDivergenceMax()
+    model.Projection(dt)
+    st = model.GetSolver().Stats()
+    p_gpu = model.field("pressure").astype(np.float64)
+    div_gpu = model.ComputeDivergenceMax()
+    o = po.Oracle(spec.grid_desc(), spec.solver_params(tolerance=1e-12, max_iterations=400), spec.liquid_params(),
+                  dbl=True)
+    o.set_boundary(spec.boundary)
+    for f, v in fields.items():
+        o.set_field(f, v.astype(np.float64))
+    st_o = o.solve(spec.density, dt)  # the oracle holds no particles: solve + velocity update by hand
+    o.velocity_update(dt)
+    p_o = o.field("pressure")
+    _, div_o = o.divergence()
+    nrm = float(np.linalg.norm(p_o))
+    rel = float(np.linalg.norm(p_gpu - p_o) / (nrm if nrm > 0 else 1.0))
+    return {"pressure_rel_l2": rel, "pressure_tolerance": 1e-5,
+            "gpu_true_residual_rel": st["true_residual"] / st["initial_residual"] if st["initial_residual"] else 0.0,
+            "gpu_iterations": st["iterations"], "oracle_iterations": st_o["iterations"],
+            "oracle_rel_residual": st_o["true_residual"] / st_o["initial_residual"] if st_o["initial_residual"] else 0.0,
+            "div_max_before": div_before, "div_max_after_gpu": div_gpu, "div_max_after_oracle": div_o,
+            "oracle_threads": po.get_threads(), "check_s": round(time.perf_counter() - t0, 1),
+            "what": "one projection of the scene's state after the timed steps; the same float inputs; oracle FP64 "
+                    "solved to 1e-12; positions: tests/test_gpu_configs.py (64^3, 100 FP64 steps)"}
+
+
 # --------------------------------------------------------- reference arm
-def reference_model(po, spec_small, iterations):
+def reference_model(po, spec, iterations):
     """The reference's LiquidModel<3> on the scene (Scene<3> built from the
     reference JSON schema), PCG capped at ``iterations``."""
-    from liquidhairinteration_b200 import abi
-    solver = spec_small.solver_params(robust=False, max_iterations=iterations, tolerance=1e-30,
-                                      num_level=5, num_pre_smooth=2, num_post_smooth=2, num_final_smooth=20)
-    ref = po.Reference(spec_small.config_json(solver))
-    ref.set_boundary(spec_small.boundary)
+    solver = spec.solver_params(robust=False, max_iterations=iterations, tolerance=1e-30,
+                                num_level=5, num_pre_smooth=2, num_post_smooth=2, num_final_smooth=20)
+    ref = po.Reference(spec.config_json(solver))
+    ref.set_boundary(spec.boundary)
     return ref
 
 
-def reference_step_sample(po, spec, n_small):
-    """One reference step on the scene's layout at n_small^3; returns
-    (seconds, particles).  Each timed step restarts from the seeded state so
-    the reference's own (non-converging) PCG cannot accumulate NaN."""
+def scaled_scene(n):
+    """dam256's layout (block, walls one cell thick, the two solid boxes) on an n^3 grid."""
     from liquidhairinteration_b200 import scenes
     small = scenes.dam256()
-    small.n = n_small
-    small.boundary = [dict(small.boundary[0]), scenes.walls(n_small)] + [dict(b) for b in small.boundary[2:]]
-    pos, vel = scenes.seed(small, "fp32")
-    ref = reference_model(po, small, REFERENCE_PCG_ITERATIONS)
+    small.n = n
+    small.boundary = [dict(small.boundary[0]), scenes.walls(n)] + [dict(b) for b in small.boundary[2:]]
+    return small
+
+
+def reference_stepper(po, spec):
+    """A function that times one reference PreStep + Step on the scene and
+    returns seconds, and the particle count.  Each timed step restarts from
+    the seeded state so the reference's own (non-converging) PCG cannot
+    accumulate NaN from step to step."""
     import numpy as np
-    dt = np.float32(small.dt)
+    pos, vel = po.seed_scene(spec, "fp32")
+    ref = reference_model(po, spec, REFERENCE_PCG_ITERATIONS)
+    dt = np.float32(spec.dt)
 
     def step():
         ref.set_particles(pos, vel)
@@ -411,58 +483,137 @@ def reference_step_sample(po, spec, n_small):
     return step, pos.shape[0]
 
 
+def fastest_reference_threads(po, spec):
+    """OpenMP thread count with the fastest reference step on the scene's
+    layout at 32^3.  The reference's ComputeLiquidPhi takes an omp critical
+    section per (particle, cell) pair (LiquidModel.cpp:540-560), so more
+    threads can make it slower; the arm gives the reference its best count."""
+    cores = os.cpu_count() or 1
+    cands = sorted({c for c in (1, 2, 4, 8, 16, 32, 64, cores) if c <= cores})
+    step, _ = reference_stepper(po, scaled_scene(REFERENCE_SAMPLE_N))
+    times = {}
+    for c in cands:
+        po.set_reference_threads(c)
+        step()
+        times[c] = min(step() for _ in range(2))
+    best = min(times, key=times.get)
+    return best, {str(c): round(t * 1e3, 1) for c, t in times.items()}
+
+
 def cpu_baseline(spec, steps=3):
-    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     from oracle import pyoracle as po
     if not po.reference_available():
         return None
-    step, npart = reference_step_sample(po, spec, REFERENCE_SAMPLE_N)
+    cores = os.cpu_count() or 1
+    po.set_reference_threads(cores)
+    step, npart = reference_stepper(po, scaled_scene(REFERENCE_SAMPLE_N))
     step()  # warm-up
     secs = [step() for _ in range(steps)]
     scale = (spec.n / REFERENCE_SAMPLE_N) ** 3
     ms = sum(secs) / len(secs) * 1e3 * scale
-    return {"value": round(ms, 1), "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
-            "sample": f"reference LiquidModel<3>::PreStep+Step (OpenMP, {os.environ['OMP_NUM_THREADS']} threads) on "
-                      f"the same scene at {REFERENCE_SAMPLE_N}^3 ({npart} particles), PCG capped at "
-                      f"{REFERENCE_PCG_ITERATIONS} iterations, {steps} steps, time x{scale:.0f}"}
+    return {"value": round(ms, 1), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"bounded sample: reference LiquidModel<3>::PreStep+Step (OpenMP, {cores} threads) on the same "
+                      f"scene layout at {REFERENCE_SAMPLE_N}^3 ({npart} particles), PCG capped at "
+                      f"{REFERENCE_PCG_ITERATIONS} iterations, {steps} steps, time x{scale:.0f}; the full-size "
+                      f"measurement is the --impl reference arm"}
 
 
 def run_reference(args):
+    """The reference's own CPU step on the full workload (see the module
+    docstring).  Rank 0 alone runs it; the other ranks exit at once."""
     rank, _, world = dist_env()
     if rank != 0:
         return
-    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     from oracle import pyoracle as po
     from liquidhairinteration_b200 import scenes
     if not po.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so was not built"}))
         return
     spec = scenes.get(args.scene)
-    step, npart = reference_step_sample(po, spec, REFERENCE_SAMPLE_N)
-    for _ in range(args.warmup):
-        step()
-    secs = [step() for _ in range(args.steps)]
-    scale = (spec.n / REFERENCE_SAMPLE_N) ** 3
-    ms = sum(secs) / len(secs) * 1e3 * scale
-    cores = int(os.environ["OMP_NUM_THREADS"])
-    sample = (f"reference LiquidModel<3>::PreStep+Step (OpenMP, {cores} threads) on the same scene at "
-              f"{REFERENCE_SAMPLE_N}^3 ({npart} particles), PCG capped at {REFERENCE_PCG_ITERATIONS} iterations, "
-              f"time x{scale:.0f}")
+    t0 = time.perf_counter()
+    threads, calib = fastest_reference_threads(po, spec)
+    po.set_reference_threads(threads)
+    step, npart = reference_stepper(po, spec)
+    setup_s = time.perf_counter() - t0
+    k = max(1, args.ref_steps)
+    secs = [step() for _ in range(k)]
+    ms = sum(secs) / len(secs) * 1e3
+    sample = (f"reference LiquidModel<3>::PreStep+Step (its own sources, OpenMP, {threads} threads: the fastest of a "
+              f"32^3 calibration) on the full {spec.n}^3 scene, {npart} particles, PCG capped at "
+              f"{REFERENCE_PCG_ITERATIONS} iterations (the GPU's count; the reference's own PCG does not converge on "
+              f"this scene), {k} step(s) timed, no warm-up step (each takes minutes)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(ms, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{spec.name} (reference CPU path, bounded sample)", "parallelism": "OpenMP"},
-        "cpu_baseline": {"value": round(ms, 1), "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "config": {"workload": f"{spec.name}: the same {spec.n}^3 scene and particles as our arm (reference CPU path)",
+                   "parallelism": f"OpenMP x{threads}"},
+        "ref_steps_timed": k, "step_seconds": [round(s, 2) for s in secs], "setup_s": round(setup_s, 1),
+        "thread_calibration_ms_at_32": calib,
+        "cpu_baseline": {"value": round(ms, 1), "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": round(ms, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
+# ------------------------------------------------------- replica launch
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_replicas(n, argv, visible_gpus):
+    """Runs this script as n ranks of one node under torch.distributed.run
+    (one replica of the scene per GPU) and returns its exit code.  Fails
+    loudly when fewer than n GPUs are visible."""
+    if n > visible_gpus:
+        print(f"bench.py: --gpus {n} needs {n} visible GPUs, {visible_gpus} found", file=sys.stderr, flush=True)
+        return 2
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(__file__)] + list(argv)
+    return subprocess.call(cmd)
+
+
+def run_replica_check(args):
+    """Every rank joins a gloo group, takes the bench's barrier and
+    max-over-ranks, and rank 0 prints the run's rank count and the maximum
+    of the ranks' values (rank r contributes r + 1)."""
+    import datetime
+    import torch
+    rank, _, world = dist_env()
+    if world > 1:
+        torch.distributed.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    barrier, max_over_ranks = rank_reducers(world, "cpu")
+    barrier()
+    v = max_over_ranks(float(rank + 1))
+    barrier()
+    if rank == 0:
+        print(json.dumps({"impl": "replica-check", "n_ranks": world, "max_over_ranks": v}), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
+    if args.impl != "reference" and args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not under a launcher yet: start one rank per GPU
+        if args.impl == "replica-check":
+            visible = args.gpus
+        else:
+            import torch
+            visible = torch.cuda.device_count()
+        sys.exit(launch_replicas(args.gpus, sys.argv[1:], visible))
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "replica-check":
+        run_replica_check(args)
     else:
+        world = dist_env()[2]
+        if world != args.gpus:
+            print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr, flush=True)
+            sys.exit(2)
         run_ours(args)
 
 

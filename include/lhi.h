@@ -199,7 +199,8 @@ typedef struct lhi_fluid_prim {
                                    particle index                             */
 #define LHI_FIELD_CELL_START 25 /* int32, ncells + 1: first sorted particle of
                                    each cell                                  */
-#define LHI_FIELD_COUNT 26
+#define LHI_FIELD_AP 26         /* CG's A p of level 0 (lhi_solver_spmv)       */
+#define LHI_FIELD_COUNT 27
 
 typedef struct lhi_liquid lhi_liquid;  /* opaque handle: owns all device memory */
 
@@ -270,6 +271,13 @@ LHI_API int lhi_solver_get_stats(lhi_liquid* h, lhi_solve_stats* stats);
 /* CGSolver<3>::GetAx (PressureSolver.cpp:700-717) applied to a whole level:
    out = A_level * x (host buffers, ncells(level) host scalars). */
 LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void* out);
+/* One SpMV of the PCG body (the Ap = A p and p.Ap of PressureSolver.cpp:874-880)
+   with the kernel the solve itself runs: the TMA-staged tile kernel on FP32
+   grids the fused sweep takes, the row kernel elsewhere.  Reads the
+   handle's p (LHI_FIELD_P), writes Ap (LHI_FIELD_AP) on every cell of the
+   active tiles and returns p.Ap over the update region; *tma_kernel (may be
+   NULL) is 1 when the TMA kernel ran.  Needs a BuildLHS first. */
+LHI_API int lhi_solver_spmv(lhi_liquid* h, double* p_dot_ap, int32_t* tma_kernel);
 /* Active tiles of one MG level after the last BuildLHS: tiles of 8 x 8 x 32
    cells (x, y, z) holding a cell with phi <= 0 or covering an active tile of
    the next finer level; the V-cycle and PCG kernels visit only these.
@@ -395,14 +403,15 @@ LHI_API int lhi_net_backward_host(lhi_net* net, const int32_t dims[3], const flo
 /* ------------------------------------------- no-allocation divergence */
 /* No counterpart in the reference: an added entry point for callers that
    cannot allocate device memory -- a host that owns all device memory in its
-   own pool, a frame loop that must not stall on cudaMalloc/cudaFree (which
-   may synchronise the device), or code recording into a stream capture.
+   own pool, or a frame loop that must not stall on cudaMalloc/cudaFree
+   (which may synchronise the device).
    Computes what lhi_liquid_compute_divergence computes (mean over fluid
    cells, max-norm over fluid cells of [1, N-3]^3), but from DEVICE pointers
    the caller already holds, with no handle and no allocation of any kind.
    Fields are float for LHI_PRECISION_FP32 / MIXED and double for FP64, in
    the layouts listed at the top of this file; dx is the grid spacing of the
-   x axis; stream is a cudaStream_t (NULL = the legacy default stream).
+   x axis; stream is a cudaStream_t of the current device (NULL = the legacy
+   default stream).
    Scratch is a fixed device array inside the library (about 192 KB, held by
    every GPU that loads the library until the process exits), so grids above
    LHI_NOALLOC_MAX_CELLS cells are rejected with LHI_E_INVALID_ARG.  The first

@@ -83,6 +83,7 @@ FIELD_ACOEF = 22
 FIELD_CELL_KEY = 23
 FIELD_PARTICLE_ID = 24
 FIELD_CELL_START = 25
+FIELD_AP = 26
 
 KERNEL_CATEGORIES = ["sort", "liquid_phi", "p2g", "g2p", "extrapolate", "grid", "lhs", "smooth_fine",
                      "smooth_coarse", "restrict", "prolong", "spmv", "cg_vector"]
@@ -96,6 +97,7 @@ FIELD_NAMES = {
     "isValid": FIELD_IS_VALID, "rhs": FIELD_RHS, "x": FIELD_X, "p": FIELD_P,
     "r": FIELD_R, "z": FIELD_Z, "Adiag": FIELD_ADIAG, "Acoef": FIELD_ACOEF,
     "cell_key": FIELD_CELL_KEY, "particle_id": FIELD_PARTICLE_ID, "cell_start": FIELD_CELL_START,
+    "Ap": FIELD_AP,
 }
 
 

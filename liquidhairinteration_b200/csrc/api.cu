@@ -531,6 +531,17 @@ LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void*
     });
 }
 
+LHI_API int lhi_solver_spmv(lhi_liquid* h, double* p_dot_ap, int32_t* tma_kernel) {
+    NEED_HANDLE(h);
+    if (!p_dot_ap) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        int tma = 0;
+        *p_dot_ap = h->impl->spmv_p(&tma);
+        if (tma_kernel) *tma_kernel = tma;
+        return LHI_OK;
+    });
+}
+
 LHI_API int lhi_solver_active_tiles(lhi_liquid* h, int32_t level, int32_t* active, int32_t* total,
                                     int32_t* coarse) {
     NEED_HANDLE(h);

@@ -213,6 +213,7 @@ public:
     virtual void set_async(bool on) = 0;
     virtual const std::string& graph_error() const = 0;
     virtual void get_ax(int level, const void* x, void* out) = 0;
+    virtual double spmv_p(int* tma) = 0;
     virtual void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) = 0;
     virtual void set_network(LearnedNet* net, int fallback_iterations) = 0;
     virtual void learned_stats(int32_t* net_iters, int32_t* fallback_at) = 0;
@@ -270,6 +271,7 @@ public:
     const std::string& graph_error() const override { return graph_error_; }
     void finish_stats();
     void get_ax(int level, const void* x, void* out) override;
+    double spmv_p(int* tma) override;
     void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) override;
     void set_network(LearnedNet* net, int fallback_iterations) override;
     void learned_stats(int32_t* net_iters, int32_t* fallback_at) override {

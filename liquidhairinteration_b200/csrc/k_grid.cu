@@ -653,7 +653,8 @@ template <class T, class TX> int LiquidImpl<T, TX>::field_size(int f, int level,
         case LHI_FIELD_LIQUID_PHI:
         case LHI_FIELD_RHS:
         case LHI_FIELD_X:
-        case LHI_FIELD_P: *count = ncell_; return 0;
+        case LHI_FIELD_P:
+        case LHI_FIELD_AP: *count = ncell_; return 0;
         case LHI_FIELD_SOLID_PHI: *count = nnode_; return 0;
         case LHI_FIELD_IS_VALID:
             *count = nnode_;
@@ -698,6 +699,7 @@ template <class T, class TX> static T* grid_ptr(LiquidImpl<T, TX>& s, int f, int
         case LHI_FIELD_SOLID_PHI: return s.solid_phi_;
         case LHI_FIELD_RHS: return s.rhs_;
         case LHI_FIELD_P: return s.p_;
+        case LHI_FIELD_AP: return s.ap_;
         case LHI_FIELD_R: return s.lv_[level].r;
         case LHI_FIELD_Z: return s.lv_[level].z;
         case LHI_FIELD_ADIAG: return s.lv_[level].diag;

@@ -2262,6 +2262,35 @@ template <class T, class TX> void LiquidImpl<T, TX>::spmv(int level, const T* x,
     LHI_LAUNCH_CHECK();
 }
 
+// One SpMV of the PCG body on the handle's p, through the same launch as
+// enqueue_body's (so the same kernel and tile order); p.Ap comes back from
+// the device scalars.
+template <class T, class TX> double LiquidImpl<T, TX>::spmv_p(int* tma) {
+    LevelDev<T>& L0 = lv_[0];
+    if (L0.n == 0) return 0.0;
+    cur_ = stream_;
+    LHI_CUDA(cudaMemsetAsync(&sc_->stop, 0, sizeof(int), stream_));  // a finished solve leaves stop set
+    const TileK tk = tile_k(L0, &sc_->tile_count[0], tile_grid_);
+    const unsigned G = std::max(1u, tile_blocks(L0, tile_grid_));
+    const CgConf cf = make_conf(sp_, 0, 0);
+    const bool use_tma = spmv_tma_ && sp_.sweep_kernel == LHI_SWEEP_FUSED;
+    {
+        auto ps_ = scope(LHI_KERNEL_SPMV);
+        if (use_tma)
+            k_spmv_tma<<<std::min(G, unsigned(2 * kSMs)), kTileThreads, sp::kSmem, cur_>>>(
+                tm_sp_[0], tm_sp_[1], tm_sp_[2], tm_sp_[3], tm_sp_[4], tm_sp_[5], L0.nx, L0.ny, L0.nz, L0.tiles,
+                &sc_->tile_count[0], L0.tdim[1], L0.tdim[2], reinterpret_cast<float*>(ap_), partials_, counter_, sc_,
+                cf);
+        else
+            k_cg_spmv<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, p_, ap_, partials_, counter_, sc_, cf);
+        LHI_LAUNCH_CHECK();
+    }
+    read_scalars();
+    if (sc_host_->timeout) throw std::runtime_error("SpMV: a bounded wait on a staging copy timed out");
+    if (tma) *tma = use_tma ? 1 : 0;
+    return sc_host_->denom;
+}
+
 template <class T, class TX> void LiquidImpl<T, TX>::get_ax(int level, const void* x, void* out) {
     if (level < 0 || level >= nlev_) throw std::invalid_argument("bad level");
     LevelDev<T>& L = lv_[level];

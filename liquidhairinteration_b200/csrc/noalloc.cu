@@ -3,18 +3,21 @@
 // memory.
 //
 // Who needs it: a host that owns every byte of device memory itself (an
-// engine with a fixed memory budget and its own pool), a frame loop that must
-// not stall (cudaMalloc / cudaFree may synchronise the whole device), or a
-// caller that records its work into a CUDA stream capture (allocation calls
-// are not allowed while a capture is open).  Such a caller passes device
-// pointers to fields it already holds and gets the same mean and max-norm as
-// lhi_liquid_compute_divergence, without a handle and without any allocation.
+// engine with a fixed memory budget and its own pool), or a frame loop that
+// must not stall (cudaMalloc / cudaFree may synchronise the whole device).
+// Such a caller passes device pointers to fields it already holds and gets
+// the same mean and max-norm as lhi_liquid_compute_divergence, without a
+// handle and without any allocation.  The call synchronises the stream it is
+// given, to return the two values.
 //
 // Scratch lives in one file-scope __device__ array (below): every GPU that
 // loads the library holds it until the process exits.  In host code the
 // array's name is only a host-side stand-in, so its device address is looked
 // up once per device with cudaGetSymbolAddress and passed to the kernel.
+// The stream must belong to the current device, whose copy of the array the
+// kernel is given.
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "lhi.h"
@@ -37,17 +40,18 @@ constexpr int kNaScratchDoubles = kNaResultSlot + 3;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNaScratchDoubles];
 
-constexpr int kNaMaxDevices = 64;
 std::mutex g_na_mutex;
-double* g_na_ptr[kNaMaxDevices] = {};
+std::vector<double*> g_na_ptr;  // per device ordinal, sized by the device count on first use
 
 // Device address of the scratch array on the current device; looked up on
 // the first call per device.
 double* scratch_on_current_device() {
-    int dev = 0;
+    int dev = 0, count = 0;
     LHI_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNaMaxDevices) throw std::invalid_argument("device ordinal above 63");
+    LHI_CUDA(cudaGetDeviceCount(&count));
     std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (int(g_na_ptr.size()) < count) g_na_ptr.resize(size_t(count), nullptr);
+    if (dev < 0 || dev >= int(g_na_ptr.size())) throw std::invalid_argument("current device ordinal out of range");
     if (!g_na_ptr[dev]) {
         void* p = nullptr;
         LHI_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));

@@ -271,6 +271,14 @@ class CGSolver:
         call("lhi_solver_get_ax", self._m._h, int(level), _ptr(x), _ptr(out))
         return out
 
+    def SpMV(self):
+        """One SpMV of the PCG body on the solver's p (field "p") with the
+        solve's own kernel; writes field "Ap" and returns (p.Ap over the
+        update region, True when the TMA-staged tile kernel ran)."""
+        d, t = C.c_double(), C.c_int32()
+        call("lhi_solver_spmv", self._m._h, C.byref(d), C.byref(t))
+        return d.value, bool(t.value)
+
     def SetNetwork(self, net, fallbackIterations=0):
         """The learned preconditioner's network (handle created with
         preconditionerType "Learned"); the handle keeps a reference."""
@@ -478,7 +486,8 @@ class LiquidModel:
         f = abi.FIELD_NAMES[name] if isinstance(name, str) else int(name)
         cnt, eb = C.c_int64(), C.c_int32()
         call("lhi_liquid_field_size", self._h, f, int(level), C.byref(cnt), C.byref(eb))
-        dt = {1: np.uint8, 4: (np.int32 if f >= abi.FIELD_CELL_KEY else np.float32), 8: np.float64}[eb.value]
+        ints = (abi.FIELD_CELL_KEY, abi.FIELD_PARTICLE_ID, abi.FIELD_CELL_START)
+        dt = {1: np.uint8, 4: (np.int32 if f in ints else np.float32), 8: np.float64}[eb.value]
         out = np.empty(cnt.value, dt)
         if cnt.value:
             call("lhi_liquid_get_field", self._h, f, int(level), _ptr(out))

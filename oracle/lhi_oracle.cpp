@@ -1139,6 +1139,10 @@ const char* lho_last_error(void) { return g_scene_error.c_str(); }
 
 void lho_set_threads(int32_t n) { g_threads = n > 0 ? n : 0; }
 
+void lho_set_omp_default_threads(int32_t n) {
+    if (n > 0) omp_set_num_threads(n);
+}
+
 int32_t lho_get_threads(void) { return nthreads(); }
 
 lho_model* lho_create(const lhi_grid_desc* grid, const lhi_solver_params* solver,

@@ -43,6 +43,9 @@ typedef struct lho_model lho_model;
    disjoint data run in parallel, and every sum is taken serially. */
 LHO_API void lho_set_threads(int32_t n);
 LHO_API int32_t lho_get_threads(void);
+/* OpenMP's default thread count for parallel regions the calling thread
+   opens without a num_threads clause: the reference build's own loops. */
+LHO_API void lho_set_omp_default_threads(int32_t n);
 /* Message of the last failed scene-generator call in this library. */
 LHO_API const char* lho_last_error(void);
 

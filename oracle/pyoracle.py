@@ -59,6 +59,7 @@ def _load_oracle():
     lib.lho_sort_by_cell.argtypes = [_vp, _vp, _vp]
     lib.lho_set_threads.argtypes = [C.c_int32]
     lib.lho_get_threads.restype = C.c_int32
+    lib.lho_set_omp_default_threads.argtypes = [C.c_int32]
     lib.lhi_scene_seed_particles.argtypes = [C.POINTER(abi.GridDesc), C.POINTER(abi.BoundaryNode), C.c_int32,
                                              C.c_int32, C.POINTER(abi.FluidPrim), C.c_int32, C.c_uint64,
                                              C.c_int32, C.POINTER(C.c_int64), _vp, _vp]
@@ -255,6 +256,12 @@ def set_threads(n):
 
 def get_threads():
     return int(oracle_lib().lho_get_threads())
+
+
+def set_reference_threads(n):
+    """OpenMP threads of the reference build's own parallel loops (they
+    take OpenMP's default, which this sets for the calling thread)."""
+    oracle_lib().lho_set_omp_default_threads(int(n))
 
 
 def seed_scene(spec, precision="fp32"):

@@ -11,7 +11,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_TREE = "/root/reference"
+# the reference source tree, where this machine has one (LHI_REFERENCE_TREE overrides)
+REFERENCE_TREE = os.environ.get("LHI_REFERENCE_TREE", "/root/reference")
 
 
 def pytest_configure(config):

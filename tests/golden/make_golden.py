@@ -27,7 +27,8 @@ sys.path.insert(0, ROOT)
 from liquidhairinteration_b200 import abi, scenes  # noqa: E402
 from oracle import pyoracle as po  # noqa: E402
 
-REFERENCE_TREE = "/root/reference"
+# the reference source tree, where this machine has one (LHI_REFERENCE_TREE overrides)
+REFERENCE_TREE = os.environ.get("LHI_REFERENCE_TREE", "/root/reference")
 
 # solver settings of the fixture run: the reference's own PCG and stopping rule
 DAM16_SOLVER = dict(robust=False, max_iterations=100, tolerance=1e-4, num_level=4, num_pre_smooth=5,

@@ -63,3 +63,23 @@ def test_reference_arm_idle_on_other_ranks(monkeypatch):
     monkeypatch.setenv("WORLD_SIZE", "2")
     # rank 1 returns before importing or running anything of the reference
     assert bench.run_reference(None) is None
+
+
+def test_bench_launches_its_own_replicas():
+    """`bench.py --gpus 2` outside a launcher starts two ranks itself (the
+    same torch.distributed.run command the GPU run uses); the replica-check
+    mode does only the rank plumbing, over gloo on CPU."""
+    import json
+    import subprocess
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "replica-check", "--gpus", "2"],
+                       capture_output=True, text=True, timeout=240, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    assert json.loads(lines[0]) == {"impl": "replica-check", "n_ranks": 2, "max_over_ranks": 2.0}
+
+
+def test_bench_refuses_more_gpus_than_visible():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.launch_replicas(4, ["--steps", "1"], visible_gpus=1) == 2

@@ -1,7 +1,7 @@
 """lhi_divergence_noalloc: the divergence diagnostic for callers that cannot
 allocate device memory (a host that owns every device byte in its own pool,
-a frame loop that must not stall on cudaMalloc/cudaFree, code recording into
-a stream capture).  It must give what the handle's
+or a frame loop that must not stall on cudaMalloc/cudaFree).  It must give
+what the handle's
 lhi_liquid_compute_divergence gives on the same fields: the max-norm exactly
 (a maximum does not depend on order) and the mean within 1e-9 of the
 max-norm (both are double sums of the same per-cell values, taken in another
