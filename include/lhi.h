@@ -128,8 +128,21 @@ typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> *
     double gravity;                  /* gravity along y                        */
     double particle_radius;          /* 0 => 2 * dx.x (ParticleSystem.cpp:8)   */
     int32_t extrapolate_iterations;  /* 0 => 5 (LiquidModel.cpp:948)           */
-    int32_t reserved[7];
+    int32_t correct_volume;          /* 1: Step ends with CorrectVolume, the call
+                                        the reference's Step has commented out
+                                        (LiquidModel.cpp:527); 0 (default): off */
+    int32_t correct_cycle;           /* 0 => 8 (m_correctCycle, LiquidModel.cpp:486) */
+    int32_t reserved[5];
 } lhi_liquid_params;
+
+/* Headless particle render (LiquidModel<3>::Render, LiquidModel.cpp:1138-1159,
+   and Shader/Scene3D_vertex.glsl), lhi_liquid_render. */
+typedef struct lhi_render_params {
+    int32_t width, height;  /* viewport in pixels (main.cpp:11: 480 x 480)        */
+    float point_size;       /* gl_PointSize in pixels (LiquidModel.cpp:1149: 5)   */
+    uint8_t color[4];       /* RGBA of the points (Color::Blue: 0, 0, 255, 255)   */
+    uint8_t background[4];  /* clear colour (main.cpp:12: Color::White)           */
+} lhi_render_params;
 
 typedef struct lhi_solve_stats {
     int32_t iterations;        /* PCG iterations taken                        */
@@ -259,6 +272,34 @@ LHI_API int lhi_liquid_advect_particles(lhi_liquid* h, double dt);/* LiquidModel
 LHI_API int lhi_liquid_compute_divergence(lhi_liquid* h, double* mean, double* max_abs);
 /* LiquidModel<3>::GetCFL (LiquidModel.h:49-55) */
 LHI_API int lhi_liquid_get_cfl(lhi_liquid* h, double* dt_out);
+/* LiquidModel<3>::CorrectVolume (LiquidModel.cpp:1086-1132) with the
+   neighbour search of HashNeighborSearch (NeighborSearch.h:22-108) done on
+   the handle's cell-sorted particles.  The particles whose index (caller
+   order) is step mod cycle move by the repulsion of their neighbours within
+   one radius (every other particle keeps its position), then step advances.
+   Off unless called, or unless lhi_liquid_params.correct_volume is set,
+   which makes Step end with it (the reference's Step has the call commented
+   out).  Where the reference differs: its neighbour table is the one built
+   at the end of the previous call, not the current positions, and a hash
+   collision can list a particle twice; here the neighbours are those of the
+   current positions, each counted once per cell its 3x3x3 region shares
+   with the particle's region, as the table lists it once per region cell.
+   Coincident particles (distance <= 1e-4 radius) take a seeded counter-based
+   uniform number (SplitMix64 of the two indices, the call count and the
+   axis) where the reference draws from an unseeded std::mt19937. */
+LHI_API int lhi_liquid_correct_volume(lhi_liquid* h, double dt);
+/* LiquidModel<3>::Render without a graphics API: the vertex shader's
+   normalised device coordinates, point = (pos - minCoord) / (maxCoord -
+   minCoord) * 2 - 1 in float (Shader/Scene3D_vertex.glsl:9), per particle in
+   the caller's order (ndc, n x 3, may be NULL), and the points drawn as GL
+   draws them into an RGBA image (rgba, height x width x 4 bytes, row 0 at
+   the bottom as in GL window coordinates, may be NULL): points outside
+   [-1, 1]^3 are clipped, the viewport maps x to (x + 1) * width / 2, each
+   point covers the pixels whose centres lie in the square of side
+   point_size around it (left and bottom edges included), and every covered
+   pixel takes the point colour (one uniform colour, no depth test, no
+   blending: Scene3D_fragment.glsl), the rest the background. */
+LHI_API int lhi_liquid_render(lhi_liquid* h, const lhi_render_params* params, float* ndc, uint8_t* rgba);
 
 /* -------------------------------------------------------------- solver */
 LHI_API int lhi_solver_init(lhi_liquid* h);                               /* PressureSolver.cpp:666 */

@@ -89,6 +89,7 @@ struct LiquidParameter {
     Scalar surfaceTension = Scalar(0.0728);  // parsed, unused
     int correctCycle = 8;
     Scalar gravity = Scalar(-9.81);
+    bool correctVolume = false;  // Step ends with CorrectVolume (off, as in the reference's Step)
 };
 
 template <int DIM> class ParticleSystem;
@@ -282,8 +283,10 @@ public:
     void ApplyGravity(Scalar dt) { Check(lhi_liquid_apply_gravity(h_, dt), "lhi_liquid_apply_gravity"); }
     void AdvectParticle(Scalar dt) { Check(lhi_liquid_advect_particles(h_, dt), "lhi_liquid_advect_particles"); }
     void Extrapolate() { Check(lhi_liquid_extrapolate(h_), "lhi_liquid_extrapolate"); }
-    // disabled in the reference's 3D step (LiquidModel.cpp:527)
-    void CorrectVolume(Scalar) { throw std::runtime_error("CorrectVolume is disabled in the 3D liquid step"); }
+    // LiquidModel<3>::CorrectVolume (LiquidModel.cpp:1086-1132); the reference's
+    // Step has the call commented out (LiquidModel.cpp:527), so it runs only
+    // when called (or with LiquidParameter::correctVolume set)
+    void CorrectVolume(Scalar dt) { Check(lhi_liquid_correct_volume(h_, dt), "lhi_liquid_correct_volume"); }
     Scalar ComputeDivergence() const {
         double mean = 0, mx = 0;
         Check(lhi_liquid_compute_divergence(h_, &mean, &mx), "lhi_liquid_compute_divergence");
@@ -358,6 +361,8 @@ private:
         lhi_liquid_params lp{};
         lp.density = liquid.density;
         lp.gravity = liquid.gravity;
+        lp.correct_volume = liquid.correctVolume ? 1 : 0;
+        lp.correct_cycle = liquid.correctCycle;
         lhi_liquid* h = nullptr;
         Check(lhi_liquid_create(&g, &sp, &lp, precision, &h), "lhi_liquid_create");
         return h;

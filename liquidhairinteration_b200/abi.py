@@ -101,6 +101,19 @@ FIELD_NAMES = {
 }
 
 
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("point_size", C.c_float),
+                ("color", C.c_uint8 * 4), ("background", C.c_uint8 * 4)]
+
+
+def make_render_params(width=480, height=480, point_size=5.0, color=(0, 0, 255, 255),
+                       background=(255, 255, 255, 255)):
+    """The reference's defaults: a 480 x 480 window (main.cpp:11), white
+    background (main.cpp:12), blue points of 5 pixels (LiquidModel.cpp:1140-1149)."""
+    return RenderParams(int(width), int(height), float(point_size), (C.c_uint8 * 4)(*color),
+                        (C.c_uint8 * 4)(*background))
+
+
 class GridDesc(C.Structure):
     _fields_ = [("dim", C.c_int32 * 3), ("reserved", C.c_int32),
                 ("min_coord", C.c_double * 3), ("max_coord", C.c_double * 3)]
@@ -120,7 +133,7 @@ class SolverParams(C.Structure):
 class LiquidParams(C.Structure):
     _fields_ = [("density", C.c_double), ("gravity", C.c_double),
                 ("particle_radius", C.c_double), ("extrapolate_iterations", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("correct_volume", C.c_int32), ("correct_cycle", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class SolveStats(C.Structure):
@@ -176,12 +189,15 @@ def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECON
     return s
 
 
-def make_liquid_params(density=1000.0, gravity=-9.81, particle_radius=0.0, extrapolate_iterations=5):
+def make_liquid_params(density=1000.0, gravity=-9.81, particle_radius=0.0, extrapolate_iterations=5,
+                       correct_volume=0, correct_cycle=8):
     p = LiquidParams()
     p.density = float(density)
     p.gravity = float(gravity)
     p.particle_radius = float(particle_radius)
     p.extrapolate_iterations = int(extrapolate_iterations)
+    p.correct_volume = int(correct_volume)
+    p.correct_cycle = int(correct_cycle)
     return p
 
 

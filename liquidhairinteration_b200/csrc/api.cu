@@ -531,6 +531,23 @@ LHI_API int lhi_solver_get_ax(lhi_liquid* h, int32_t level, const void* x, void*
     });
 }
 
+LHI_API int lhi_liquid_correct_volume(lhi_liquid* h, double dt) {
+    NEED_HANDLE(h);
+    return guarded([&]() -> int {
+        h->impl->correct_volume(dt);
+        return LHI_OK;
+    });
+}
+
+LHI_API int lhi_liquid_render(lhi_liquid* h, const lhi_render_params* params, float* ndc, uint8_t* rgba) {
+    NEED_HANDLE(h);
+    if (!params) return fail(LHI_E_INVALID_ARG, "null argument");
+    return guarded([&]() -> int {
+        h->impl->render(*params, ndc, rgba);
+        return LHI_OK;
+    });
+}
+
 LHI_API int lhi_solver_spmv(lhi_liquid* h, double* p_dot_ap, int32_t* tma_kernel) {
     NEED_HANDLE(h);
     if (!p_dot_ap) return fail(LHI_E_INVALID_ARG, "null argument");

@@ -214,6 +214,8 @@ public:
     virtual const std::string& graph_error() const = 0;
     virtual void get_ax(int level, const void* x, void* out) = 0;
     virtual double spmv_p(int* tma) = 0;
+    virtual void render(const lhi_render_params& rp, float* ndc_host, uint8_t* rgba_host) = 0;
+    virtual void correct_volume(double dt) = 0;
     virtual void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) = 0;
     virtual void set_network(LearnedNet* net, int fallback_iterations) = 0;
     virtual void learned_stats(int32_t* net_iters, int32_t* fallback_at) = 0;
@@ -272,6 +274,8 @@ public:
     void finish_stats();
     void get_ax(int level, const void* x, void* out) override;
     double spmv_p(int* tma) override;
+    void render(const lhi_render_params& rp, float* ndc_host, uint8_t* rgba_host) override;
+    void correct_volume(double dt) override;
     void active_tiles(int level, int32_t* active, int32_t* total, int32_t* coarse) override;
     void set_network(LearnedNet* net, int fallback_iterations) override;
     void learned_stats(int32_t* net_iters, int32_t* fallback_at) override {
@@ -338,6 +342,10 @@ public:
     T min_[3], max_[3], dx_[3];
     T radius_, density_, gravity_;
     int extrap_iters_;
+    // CorrectVolume (LiquidModel.cpp:1086-1132): on in Step, cycle, current step, calls so far
+    bool correct_in_step_ = false;
+    int correct_cycle_ = 8, correct_step_ = 0;
+    unsigned long long correct_calls_ = 0;
     long long ncell_, nface_[3], nnode_;
     T* v_[3] = {};    // current vx, vy, vz
     T* tv_[3] = {};   // current tempVx, tempVy, tempVz
@@ -363,6 +371,11 @@ public:
     long long hist_cap_ = 0;
     int32_t* cell_count_ = nullptr;  // ncell + 1
     int32_t* cell_start_ = nullptr;  // ncell + 1
+    // headless render: RGBA image and normalised device coordinates, sized on first use
+    void* image_ = nullptr;
+    long long image_cap_ = 0;
+    float* ndc_ = nullptr;
+    long long ndc_cap_ = 0;
     void* scan_tmp_ = nullptr;
     long long scan_tmp_bytes_ = 0;
 

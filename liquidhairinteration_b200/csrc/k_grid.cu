@@ -324,6 +324,8 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     density_ = T(lp.density);
     gravity_ = T(lp.gravity);
     extrap_iters_ = lp.extrapolate_iterations > 0 ? lp.extrapolate_iterations : 5;
+    correct_in_step_ = lp.correct_volume != 0;
+    correct_cycle_ = lp.correct_cycle > 0 ? lp.correct_cycle : 8;
     if (extrap_iters_ > 250) throw std::invalid_argument("extrapolate_iterations must be <= 250");
     sp_ = sp;
     if (sp.max_iterations < 0 || sp.num_pre_smooth < 0 || sp.num_post_smooth < 0 || sp.num_final_smooth < 0)
@@ -447,6 +449,8 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
         F(w_[a]);
         F(lw_[a]);
     }
+    F(image_);
+    F(ndc_);
     F(pressure_);
     F(liquid_phi_);
     F(solid_phi_);
@@ -630,6 +634,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::step(double dt) {
     int st = projection(dt);
     extrapolate();
     g2p(true, T(dt));  // Grid2Particle + AdvectParticle
+    if (correct_in_step_) correct_volume(dt);
     return st;
 }
 

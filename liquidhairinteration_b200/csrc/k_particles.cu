@@ -243,92 +243,6 @@ __device__ void p2g_particle_global(const GridP<T>& g, const int d[3], const T q
     }
 }
 
-template <class T, int A>
-__device__ __forceinline__ void p2g_cell_component(const GridP<T>& g, const int d[3], const int ci[3], int p0, int p1,
-                                                   const T* __restrict__ pd, long long cap, T* sw, T* sv, int lox,
-                                                   int loy, int loz, T* __restrict__ gw, T* __restrict__ gv) {
-    constexpr int NX = (A == 0) ? 4 : 3, NY = (A == 1) ? 4 : 3, NZ = (A == 2) ? 4 : 3;
-    T aw[NX][NY][NZ], av[NX][NY][NZ];
-#pragma unroll
-    for (int i = 0; i < NX; ++i)
-#pragma unroll
-        for (int j = 0; j < NY; ++j)
-#pragma unroll
-            for (int k = 0; k < NZ; ++k) aw[i][j][k] = av[i][j][k] = T(0);
-    // node coordinate (grid units) of window slot s on axis i, and its validity
-    auto node_c = [&](int i, int s) -> T {
-        const int node = ci[i] + s - 1;
-        return (i == A) ? T(node) : X<T>::add(T(node), T(0.5));
-    };
-    for (int p = p0; p < p1; ++p) {
-        const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
-        const T vel = pd[(3 + A) * cap + p];
-        const T C0 = pd[(6 + 3 * A) * cap + p], C1 = pd[(7 + 3 * A) * cap + p], C2 = pd[(8 + 3 * A) * cap + p];
-        T g3[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) g3[i] = X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]);  // cwiseQuotient
-        if (int(g3[0]) != ci[0] || int(g3[1]) != ci[1] || int(g3[2]) != ci[2]) {
-            p2g_particle_global<T, A>(g, d, q, g3, vel, C0, C1, C2, gw, gv);
-            continue;
-        }
-        // per-axis weights and C_a . (x_p - x_node) terms (Eigen dot order a0 + (a1 + a2))
-        T wx[NX], wy[NY], wz[NZ], ex[NX], ey[NY], ez[NZ];
-#pragma unroll
-        for (int s2 = 0; s2 < NX; ++s2) {
-            const T c = node_c(0, s2), e = X<T>::sub(g3[0], c);
-            const int o = s2 - 1;
-            const bool ok = o >= max(-1, -d[0]) && o <= min(A == 0 ? 2 : 1, d[0]) && !(fabs(e) >= T(1.5f));
-            wx[s2] = ok ? qweight(e) : T(0);
-            ex[s2] = X<T>::mul(C0, X<T>::sub(q[0], X<T>::add(X<T>::mul(c, g.dx[0]), g.mn[0])));
-        }
-#pragma unroll
-        for (int s2 = 0; s2 < NY; ++s2) {
-            const T c = node_c(1, s2), e = X<T>::sub(g3[1], c);
-            const int o = s2 - 1;
-            const bool ok = o >= max(-1, -d[1]) && o <= min(A == 1 ? 2 : 1, d[1]) && !(fabs(e) >= T(1.5f));
-            wy[s2] = ok ? qweight(e) : T(0);
-            ey[s2] = X<T>::mul(C1, X<T>::sub(q[1], X<T>::add(X<T>::mul(c, g.dx[1]), g.mn[1])));
-        }
-#pragma unroll
-        for (int s2 = 0; s2 < NZ; ++s2) {
-            const T c = node_c(2, s2), e = X<T>::sub(g3[2], c);
-            const int o = s2 - 1;
-            const bool ok = o >= max(-1, -d[2]) && o <= min(A == 2 ? 2 : 1, d[2]) && !(fabs(e) >= T(1.5f));
-            wz[s2] = ok ? qweight(e) : T(0);
-            ez[s2] = X<T>::mul(C2, X<T>::sub(q[2], X<T>::add(X<T>::mul(c, g.dx[2]), g.mn[2])));
-        }
-        // w (v + C.(x_p - x_node)) with the v + ex + ey part formed once per
-        // (x, y) pair and the product accumulated by fused multiply-add
-#pragma unroll
-        for (int i = 0; i < NX; ++i) {
-            const T vxi = vel + ex[i];
-#pragma unroll
-            for (int j = 0; j < NY; ++j) {
-                const T wxy = wx[i] * wy[j];
-                const T vxy = vxi + ey[j];
-#pragma unroll
-                for (int k = 0; k < NZ; ++k) {
-                    const T weight = wxy * wz[k];
-                    aw[i][j][k] += weight;
-                    av[i][j][k] = fma(weight, vxy + ez[k], av[i][j][k]);
-                }
-            }
-        }
-    }
-    if (p1 == p0) return;
-    const int ext_y = kTile + 2 + (A == 1), ext_z = kTile + 2 + (A == 2);
-#pragma unroll
-    for (int i = 0; i < NX; ++i)
-#pragma unroll
-        for (int j = 0; j < NY; ++j)
-#pragma unroll
-            for (int k = 0; k < NZ; ++k) {
-                const int idx = ((ci[0] + i - 1 - lox) * ext_y + (ci[1] + j - 1 - loy)) * ext_z + (ci[2] + k - 1 - loz);
-                atomicAdd(&sw[idx], aw[i][j][k]);
-                atomicAdd(&sv[idx], av[i][j][k]);
-            }
-}
-
 template <class T> struct P2GOut {
     T* v[3];
     T* w[3];
@@ -338,70 +252,212 @@ __host__ __device__ constexpr int p2g_region(int a) {
     return (kTile + 2 + (a == 0)) * (kTile + 2 + (a == 1)) * (kTile + 2 + (a == 2));
 }
 
+// Staged particle record of the P2G warp loop (values of T):
+//   [0, 12)   face weights wf[axis][4], window slots -1..2 (node = cell + slot)
+//   [12, 21)  centre weights wc[axis][3], slots -1..1 (node centre = cell + slot + 0.5)
+//   [21, 33)  tf[a][4] = C_aa * (x_a - face node a)          (component a, its own axis)
+//   [33, 51)  tc[a][j][3] = C_ab * (x_b - centre node b), b the j-th other axis of a
+//   [51, 54)  v
+//   [54]      z offset of the particle's cell in its row (bits of an int), -1: skip
+// A weight outside the reference's window (+-d) or with |e| >= 1.5 is 0.
+constexpr int kP2GRec = 55;
+constexpr int kP2GWarps = 8;
+
+__device__ __forceinline__ void p2g_other_axes(int a, int& b, int& c) {
+    b = (a == 0) ? 1 : 0;
+    c = (a == 2) ? 1 : 2;
+}
+
+// Computes the record of one particle (one lane per particle).  Returns the
+// z offset of its cell in the row, or -1 when its own truncated index
+// (cast<Integer>, LiquidModel.cpp:629) is not the cell it was sorted into
+// (outside the grid, where the sort key is clamped): then its window goes
+// straight to global memory here, component by component.
 template <class T>
-__global__ void __launch_bounds__(256) k_p2g(GridP<T> g, const int32_t* __restrict__ cs, const T* __restrict__ pd,
-                                             long long cap, int d0, int d1, int d2, P2GOut<T> out) {
+__device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __restrict__ pd, long long cap, long long p,
+                         int rx, int ry, int z0, int zend, T* rec, T* __restrict__ gw0, T* __restrict__ gv0,
+                         T* __restrict__ gw1, T* __restrict__ gv1, T* __restrict__ gw2, T* __restrict__ gv2) {
+    const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
+    const T v[3] = {pd[3 * cap + p], pd[4 * cap + p], pd[5 * cap + p]};
+    T C[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) C[k] = pd[(6 + k) * cap + p];  // column-major: C[3a + i] = C(i, a)
+    T g3[3];
+    int ci[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        g3[i] = X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]);  // cwiseQuotient
+        ci[i] = int(g3[i]);                                     // cast<Integer>
+    }
+    if (ci[0] != rx || ci[1] != ry || ci[2] < z0 || ci[2] >= zend) {
+        const int d[3] = {d0, d1, d2};
+        p2g_particle_global<T, 0>(g, d, q, g3, v[0], C[0], C[1], C[2], gw0, gv0);
+        p2g_particle_global<T, 1>(g, d, q, g3, v[1], C[3], C[4], C[5], gw1, gv1);
+        p2g_particle_global<T, 2>(g, d, q, g3, v[2], C[6], C[7], C[8], gw2, gv2);
+        return -1;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int di = (i == 0) ? d0 : (i == 1) ? d1 : d2;
+#pragma unroll
+        for (int s2 = 0; s2 < 4; ++s2) {  // face nodes: component i's own axis
+            const int o = s2 - 1;
+            const T c = T(ci[i] + o);
+            const T e = X<T>::sub(g3[i], c);
+            const bool ok = o >= -di && o <= di && !(fabs(e) >= T(1.5f));
+            rec[i * 4 + s2] = ok ? qweight(e) : T(0);
+            const T df = X<T>::sub(q[i], X<T>::add(X<T>::mul(c, g.dx[i]), g.mn[i]));
+            rec[21 + i * 4 + s2] = X<T>::mul(C[4 * i], df);  // C(i, i)
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < 3; ++s2) {  // cell-centre nodes: the other two components
+            const int o = s2 - 1;
+            const T c = X<T>::add(T(ci[i] + o), T(0.5));
+            const T e = X<T>::sub(g3[i], c);
+            const bool ok = o >= -di && o <= di && !(fabs(e) >= T(1.5f));
+            rec[12 + i * 3 + s2] = ok ? qweight(e) : T(0);
+            const T dc = X<T>::sub(q[i], X<T>::add(X<T>::mul(c, g.dx[i]), g.mn[i]));
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a == i) continue;
+                int b, c2;
+                p2g_other_axes(a, b, c2);
+                rec[33 + a * 6 + (b == i ? 0 : 3) + s2] = X<T>::mul(C[3 * a + i], dc);
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) rec[51 + a] = v[a];
+    return ci[2] - z0;
+}
+
+// LiquidModel<3>::Particle2Grid accumulation (LiquidModel.cpp:614-701).
+// One CTA per 8^3-cell tile, shared-memory accumulators for the tile's
+// window nodes of the three face components.  A warp takes whole z rows of
+// the tile: the particles of a row are contiguous in the sorted order.  The
+// row's particles are staged 32 at a time (one lane per particle computes
+// its per-axis weights and C.(x_p - x_node) terms once, for all three
+// components), then the warp walks them in order: lane l < 27 owns one
+// column of 4 window nodes of one component (component l / 9, along that
+// component's own axis; the 3 x 3 columns across it) and sums the weights
+// and APIC values of the current cell's particles in registers.  When the
+// walk reaches the next cell each lane adds its 4 nodes once into the
+// tile's accumulators; at the end every touched node goes to global memory
+// with one add.  The per-axis weights are the reference's, rounded the same
+// way; the per-node products are regrouped and fused and particles are
+// summed in another order, so P2G matches the reference to rounding, not
+// bit for bit.  No per-particle global atomics.
+template <class T>
+__global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_t* __restrict__ cs,
+                                                        const T* __restrict__ pd, long long cap, int d0, int d1,
+                                                        int d2, P2GOut<T> out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
     __shared__ int any;
     const int x0 = blockIdx.z * kTile, y0 = blockIdx.y * kTile, z0 = blockIdx.x * kTile;
-    // the tile's two cells of this thread and their particle ranges
-    int cnt[2], beg[2], cc[2][3];
-    int mine = 0;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int t = threadIdx.x + h * 256;
-        cc[h][0] = x0 + (t >> 6);
-        cc[h][1] = y0 + ((t >> 3) & 7);
-        cc[h][2] = z0 + (t & 7);
-        beg[h] = 0;
-        cnt[h] = 0;
-        if (cc[h][0] < g.nx && cc[h][1] < g.ny && cc[h][2] < g.nz) {
-            const long long c = ((long long)cc[h][0] * g.ny + cc[h][1]) * g.nz + cc[h][2];
-            beg[h] = cs[c];
-            cnt[h] = cs[c + 1] - beg[h];
-        }
-        mine += cnt[h];
-    }
-    if (threadIdx.x == 0) any = 0;
-    __syncthreads();
-    if (mine) any = 1;
-    __syncthreads();
-    if (!any) return;
+    const int zend = min(z0 + kTile, g.nz);
     const int R0 = p2g_region(0), R1 = p2g_region(1), R2 = p2g_region(2);
     const int ntot = 2 * (R0 + R1 + R2);
+    T* stage = acc + ntot + (threadIdx.x >> 5) * 32 * kP2GRec;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    if (threadIdx.x < kTile * kTile) {  // row (x0 + t / 8, y0 + t % 8)
+        const int rx = x0 + (threadIdx.x >> 3), ry = y0 + (threadIdx.x & 7);
+        if (rx < g.nx && ry < g.ny) {
+            const long long c = ((long long)rx * g.ny + ry) * g.nz + z0;
+            if (cs[c + (zend - z0)] > cs[c]) any = 1;
+        }
+    }
+    __syncthreads();
+    if (!any) return;
     for (int i = threadIdx.x; i < ntot; i += blockDim.x) acc[i] = T(0);
     __syncthreads();
-    T* sw[3] = {acc, acc + 2 * R0, acc + 2 * (R0 + R1)};
-    T* sv[3] = {acc + R0, acc + 2 * R0 + R1, acc + 2 * (R0 + R1) + R2};
-    const int d[3] = {d0, d1, d2};
-#pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
-        const int p0 = beg[h], p1 = beg[h] + cnt[h];
-        p2g_cell_component<T, 0>(g, d, cc[h], p0, p1, pd, cap, sw[0], sv[0], x0 - 1, y0 - 1, z0 - 1, out.w[0],
-                                   out.v[0]);
-        p2g_cell_component<T, 1>(g, d, cc[h], p0, p1, pd, cap, sw[1], sv[1], x0 - 1, y0 - 1, z0 - 1, out.w[1],
-                                   out.v[1]);
-        p2g_cell_component<T, 2>(g, d, cc[h], p0, p1, pd, cap, sw[2], sv[2], x0 - 1, y0 - 1, z0 - 1, out.w[2],
-                                   out.v[2]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // this lane's column: component a, centre slots s (axis b) and t (axis c), face slots k along a
+    const int a = lane / 9, s = (lane % 9) / 3, t = lane % 3;
+    int b = 0, c = 0;
+    p2g_other_axes(a < 3 ? a : 0, b, c);
+    const bool col = lane < 27;
+    const int ey = kTile + 2 + (a == 1), ez = kTile + 2 + (a == 2);
+    const int astride = (a == 0) ? ey * ez : (a == 1) ? ez : 1;
+    // the column's first node relative to its cell, per axis (slot - 1, plus 1 for the halo): face slot 0
+    // along a, centre slot s along b, t along c (b < c)
+    const int ox = (a == 0) ? 0 : s;
+    const int oy = (a == 1) ? 0 : (b == 1 ? s : t);
+    const int oz = (a == 2) ? 0 : t;
+    // component a's weight and value accumulators: [w_0 | v_0 | w_1 | v_1 | w_2 | v_2]
+    T* aw_s = acc + ((a == 1) ? 2 * R0 : (a == 2) ? 2 * (R0 + R1) : 0);
+    T* av_s = aw_s + ((a == 1) ? R1 : (a == 2) ? R2 : R0);
+    for (int row = warp; row < kTile * kTile; row += kP2GWarps) {
+        const int rx = x0 + (row >> 3), ry = y0 + (row & 7);
+        if (rx >= g.nx || ry >= g.ny) continue;
+        const long long c0 = ((long long)rx * g.ny + ry) * g.nz + z0;
+        const int pbeg = cs[c0], pend = cs[c0 + (zend - z0)];
+        if (pend == pbeg) continue;
+        int cur = -1;  // z offset of the cell being summed
+        T aw[4] = {T(0), T(0), T(0), T(0)}, av[4] = {T(0), T(0), T(0), T(0)};
+        auto flush = [&]() {
+            if (cur < 0 || !col) return;
+            // window node of slot (k, s, t) of cell (rx, ry, z0 + cur), local to the tile region
+            const int base = (((rx - x0) + ox) * ey + (ry - y0) + oy) * ez + cur + oz;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                atomicAdd(&aw_s[base + k * astride], aw[k]);
+                atomicAdd(&av_s[base + k * astride], av[k]);
+                aw[k] = T(0);
+                av[k] = T(0);
+            }
+        };
+        for (int chunk = pbeg; chunk < pend; chunk += 32) {
+            const int n = min(32, pend - chunk);
+            __syncwarp();
+            if (lane < n) {
+                const int zo = p2g_stage<T>(g, d0, d1, d2, pd, cap, chunk + lane, rx, ry, z0, zend, stage + lane * kP2GRec,
+                                            out.w[0], out.v[0], out.w[1], out.v[1], out.w[2], out.v[2]);
+                stage[lane * kP2GRec + 54] = T(0);
+                reinterpret_cast<int*>(stage + lane * kP2GRec + 54)[0] = zo;
+            }
+            __syncwarp();
+            for (int j = 0; j < n; ++j) {
+                const T* r = stage + j * kP2GRec;
+                const int zo = reinterpret_cast<const int*>(r + 54)[0];
+                if (zo < 0) continue;
+                if (zo != cur) {
+                    flush();
+                    cur = zo;
+                }
+                if (!col) continue;
+                const T wbc = r[12 + b * 3 + s] * r[12 + c * 3 + t];
+                const T base = r[51 + a] + r[33 + a * 6 + s] + r[33 + a * 6 + 3 + t];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const T w = wbc * r[a * 4 + k];
+                    aw[k] += w;
+                    av[k] = fma(w, base + r[21 + a * 4 + k], av[k]);
+                }
+            }
+        }
+        flush();
     }
     __syncthreads();
     // flush: one global add per touched node
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int ey = kTile + 2 + (a == 1), ez = kTile + 2 + (a == 2);
-        const int R = (a == 0) ? R0 : (a == 1) ? R1 : R2;
-        const int fy = g.ny + (a == 1), fz = g.nz + (a == 2);
-        const int hx = g.nx - 1 + (a == 0);
+    for (int a2 = 0; a2 < 3; ++a2) {
+        const int fy2 = kTile + 2 + (a2 == 1), fz2 = kTile + 2 + (a2 == 2);
+        const int R = (a2 == 0) ? R0 : (a2 == 1) ? R1 : R2;
+        const T* sw_a = acc + ((a2 == 1) ? 2 * R0 : (a2 == 2) ? 2 * (R0 + R1) : 0);
+        const T* sv_a = sw_a + R;
+        const int fy = g.ny + (a2 == 1), fz = g.nz + (a2 == 2);
+        const int hx = g.nx - 1 + (a2 == 0);
         for (int i = threadIdx.x; i < R; i += blockDim.x) {
-            T wv = sw[a][i], vv = sv[a][i];
+            T wv = sw_a[i], vv = sv_a[i];
             if (wv == T(0) && vv == T(0)) continue;
-            int lz = i % ez, ly = (i / ez) % ey, lx = i / (ey * ez);
+            int lz = i % fz2, ly = (i / fz2) % fy2, lx = i / (fy2 * fz2);
             int xi = x0 - 1 + lx, yi = y0 - 1 + ly, zi = z0 - 1 + lz;
             if (xi < 0 || xi > hx || yi < 0 || yi >= fy || zi < 0 || zi >= fz) continue;
             long long gi = ((long long)xi * fy + yi) * fz + zi;
-            atomicAdd(&out.w[a][gi], wv);
-            atomicAdd(&out.v[a][gi], vv);
+            atomicAdd(&out.w[a2][gi], wv);
+            atomicAdd(&out.v[a2][gi], vv);
         }
     }
 }
@@ -636,6 +692,113 @@ __global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, lon
     }
 }
 
+// ------------------------------------------------------- CorrectVolume
+// Uniform number in [0, 1) for the coincident-particle branch of
+// CorrectVolume: SplitMix64 (Steele, Lea and Flood, 2014) of the call count,
+// both particles' indices, the visit and the axis; the top 24 bits.
+__host__ __device__ __forceinline__ float cv_uniform(unsigned long long call, long long i, long long j, int visit,
+                                                     int axis) {
+    unsigned long long z = call * 0x9E3779B97F4A7C15ull + (unsigned long long)i * 0xBF58476D1CE4E5B9ull +
+                           (unsigned long long)j * 0x94D049BB133111EBull + (unsigned long long)(visit * 3 + axis);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return float(z >> 40) * (1.0f / 16777216.0f);
+}
+
+// HashNeighborSearch::GetImpactRegion (NeighborSearch.h:87-95): the cells
+// within one of the particle's own (unclamped) cell index, clamped to the grid.
+template <class T>
+__device__ __forceinline__ void cv_region(const GridP<T>& g, const T q[3], int lo[3], int hi[3]) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int c = int(X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]));
+        lo[i] = min(max(c - 1, 0), n[i] - 1);
+        hi[i] = min(max(c + 1, 0), n[i] - 1);
+    }
+}
+
+// LiquidModel<3>::CorrectVolume (LiquidModel.cpp:1086-1124) for the
+// particles with caller index = step (mod cycle): the repulsion of every
+// other particle within one radius, visited once per cell that the two
+// particles' impact regions share (as the hash table lists a particle once
+// per cell of its region and the query walks the cells of the particle's
+// region), then the move and the solid push-out.  Candidates come from the
+// cell-sorted particles of the cells within one of the region; cells in x,
+// y, z order, particles in sorted order.  New positions go to out (3 x cap).
+template <class T>
+__global__ void __launch_bounds__(256)
+    k_correct_volume(GridP<T> g, const T* __restrict__ pd, long long cap, const int32_t* __restrict__ pid,
+                     const int32_t* __restrict__ cs, long long n, T radius, T wfac, T dt, int cycle, int step,
+                     unsigned long long call, const T* __restrict__ sp, T* __restrict__ out) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int id = pid[k];
+    if (id % cycle != step) return;
+    const T p[3] = {pd[k], pd[cap + k], pd[2 * cap + k]};
+    const T r2 = X<T>::mul(radius, radius);
+    int lo[3], hi[3];
+    cv_region(g, p, lo, hi);
+    T rep[3] = {T(0), T(0), T(0)};
+    for (int cx = max(lo[0] - 1, 0); cx <= min(hi[0] + 1, g.nx - 1); ++cx)
+        for (int cy = max(lo[1] - 1, 0); cy <= min(hi[1] + 1, g.ny - 1); ++cy)
+            for (int cz = max(lo[2] - 1, 0); cz <= min(hi[2] + 1, g.nz - 1); ++cz) {
+                const long long c = ((long long)cx * g.ny + cy) * g.nz + cz;
+                for (int j = cs[c]; j < cs[c + 1]; ++j) {
+                    if (j == k) continue;
+                    const T q[3] = {pd[j], pd[cap + j], pd[2 * cap + j]};
+                    const T dir[3] = {X<T>::sub(p[0], q[0]), X<T>::sub(p[1], q[1]), X<T>::sub(p[2], q[2])};
+                    const T d2 = sqnorm3(dir[0], dir[1], dir[2]);
+                    if (d2 >= r2) continue;
+                    int lj[3], hj[3];
+                    cv_region(g, q, lj, hj);
+                    int mult = 1;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) mult *= max(0, min(hi[i], hj[i]) - max(lo[i], lj[i]) + 1);
+                    if (mult == 0) continue;
+                    const T dist = X<T>::sqrt(d2);
+                    const T w = X<T>::mul(wfac, qweight(X<T>::div(dist, radius)));
+                    if (double(dist) > 1e-4 * double(radius)) {
+                        const T wr = X<T>::mul(w, radius);
+                        const T t[3] = {X<T>::mul(wr, X<T>::div(dir[0], dist)), X<T>::mul(wr, X<T>::div(dir[1], dist)),
+                                        X<T>::mul(wr, X<T>::div(dir[2], dist))};
+                        for (int v = 0; v < mult; ++v)
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) rep[i] = X<T>::add(rep[i], t[i]);
+                    } else {
+                        const T rdt = X<T>::div(radius, dt);
+                        for (int v = 0; v < mult; ++v)
+#pragma unroll
+                            for (int i = 0; i < 3; ++i)
+                                rep[i] = X<T>::add(rep[i], X<T>::mul(rdt, T(cv_uniform(call, id, pid[j], v, i))));
+                    }
+                }
+            }
+    T np_[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) np_[i] = X<T>::add(p[i], X<T>::mul(rep[i], dt));
+    const T sphi = solid_phi_at(g, sp, np_[0], np_[1], np_[2]);
+    if (sphi < T(0)) {
+        T gr[3];
+        solid_grad_at(g, sp, np_[0], np_[1], np_[2], gr);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) np_[i] = X<T>::sub(np_[i], X<T>::mul(sphi, gr[i]));
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) out[i * cap + k] = np_[i];
+}
+
+// SetPosition(pi, GetBuffer(pi)) for the moved particles (LiquidModel.cpp:1126-1129)
+template <class T>
+__global__ void k_correct_apply(T* __restrict__ pd, long long cap, const int32_t* __restrict__ pid, long long n,
+                                int cycle, int step, const T* __restrict__ buf) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || pid[k] % cycle != step) return;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) pd[i * cap + k] = buf[i * cap + k];
+}
+
 // max |v| over particles for GetCFL (LiquidModel.h:49-55)
 template <class T>
 __global__ void k_vmax(const T* __restrict__ pd, long long cap, long long n, double* __restrict__ partials,
@@ -798,11 +961,13 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
         out.v[a] = v_[a];
         out.w[a] = w_[a];
     }
-    size_t smem = sizeof(T) * 2 * (p2g_region(0) + p2g_region(1) + p2g_region(2));
+    // tile accumulators, then one 32-particle staging buffer per warp
+    size_t smem = sizeof(T) * (2 * (p2g_region(0) + p2g_region(1) + p2g_region(2)) + kP2GWarps * 32 * kP2GRec);
     LHI_CUDA(cudaFuncSetAttribute(k_p2g<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid(unsigned((nz_ + kTile - 1) / kTile), unsigned((ny_ + kTile - 1) / kTile),
               unsigned((nx_ + kTile - 1) / kTile));
-    k_p2g<T><<<grid, 256, smem, stream_>>>(gridp(*this), cell_start_, pdata_[pcur_], pcap_, d0, d1, d2, out);
+    k_p2g<T><<<grid, kP2GWarps * 32, smem, stream_>>>(gridp(*this), cell_start_, pdata_[pcur_], pcap_, d0, d1, d2,
+                                                       out);
     LHI_LAUNCH_CHECK();
 }
 
@@ -814,6 +979,27 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_normalize(bool with_gra
             v_[a], w_[a], fx, fy, fz, (with_gravity && a == 1) ? 1 : 0, gdt, nx_, ny_, nz_);
         LHI_LAUNCH_CHECK();
     }
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::correct_volume(double dt) {
+    if (np_ == 0) return;
+    ensure_sorted();  // cell lists of the current positions
+    auto ps_ = scope(LHI_KERNEL_G2P);
+    // weightFactor = sqrt(dx.x * dx.y * dx.z) (LiquidModel.cpp:1089)
+    const T wfac = std::sqrt(dx_[0] * dx_[1] * dx_[2]);
+    T* buf = pdata_[pcur_ ^ 1];  // the permutation's other buffer, free between sorts
+    k_correct_volume<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(
+        gridp(*this), pdata_[pcur_], pcap_, pid_[pcur_], cell_start_, np_, radius_, wfac, T(dt), correct_cycle_,
+        correct_step_, correct_calls_, solid_phi_, buf);
+    LHI_LAUNCH_CHECK();
+    k_correct_apply<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pcap_, pid_[pcur_], np_,
+                                                                 correct_cycle_, correct_step_, buf);
+    LHI_LAUNCH_CHECK();
+    correct_step_ = (correct_step_ + 1) % correct_cycle_;
+    ++correct_calls_;
+    // positions moved: the next sort recomputes the keys
+    sorted_ = false;
+    keys_fresh_ = false;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::particle_to_grid() {

@@ -412,8 +412,11 @@ class LiquidModel:
         call("lhi_liquid_extrapolate", self._h)
 
     def CorrectVolume(self, dt):
-        """Disabled in the reference's 3D step (LiquidModel.cpp:527)."""
-        raise NotImplementedError("CorrectVolume is disabled in the reference's 3D liquid step")
+        """LiquidModel<3>::CorrectVolume (LiquidModel.cpp:1086-1132) on the GPU
+        (lhi_liquid_correct_volume).  The reference's Step has the call
+        commented out (LiquidModel.cpp:527); Step makes it only when the
+        handle was created with correct_volume set."""
+        call("lhi_liquid_correct_volume", self._h, float(dt))
 
     def ComputeDivergence(self):
         m, mx = C.c_double(), C.c_double()
@@ -429,6 +432,18 @@ class LiquidModel:
         d = C.c_double()
         call("lhi_liquid_get_cfl", self._h, C.byref(d))
         return d.value
+
+    def Render(self, width=480, height=480, pointSize=5.0, color=(0, 0, 255, 255),
+               background=(255, 255, 255, 255), ndc=False):
+        """LiquidModel<3>::Render without a display (lhi_liquid_render): the
+        particles drawn as the reference's shaders draw them into an RGBA
+        image (height x width x 4, row 0 at the bottom as in GL).  With
+        ndc=True also returns the vertex shader's coordinates (n x 3)."""
+        rp = abi.make_render_params(width, height, pointSize, color, background)
+        img = np.empty((height, width, 4), np.uint8)
+        out = np.empty((self.GetParticleSystem().NumParticles(), 3), np.float32) if ndc else None
+        call("lhi_liquid_render", self._h, C.byref(rp), _ptr(out), _ptr(img))
+        return (img, out) if ndc else img
 
     def SetBoundary(self, boundary):
         self.m_boundary = boundary

@@ -196,6 +196,10 @@ template <class S> struct Model {
     // parameters
     S density, gravity;
     int extrap_iters;
+    // CorrectVolume (LiquidModel.cpp:1086-1132)
+    int correct_cycle = 8, correct_step = 0;
+    bool correct_in_step = false;
+    unsigned long long correct_calls = 0;
     // solver (PressureSolver.h:121-145)
     lhi_solver_params sp;
     int maxLevel;
@@ -239,6 +243,8 @@ template <class S> struct Model {
         density = S(lp.density);
         gravity = S(lp.gravity);
         extrap_iters = lp.extrapolate_iterations > 0 ? lp.extrapolate_iterations : 5;
+        correct_cycle = lp.correct_cycle > 0 ? lp.correct_cycle : 8;
+        correct_in_step = lp.correct_volume != 0;
         // CGSolver<3>::CGSolver (PressureSolver.cpp:422-447)
         sp = s;
         tolerance = S(s.tolerance);
@@ -564,6 +570,116 @@ template <class S> struct Model {
                 for (int i = 0; i < 3; ++i) q[i] -= s * g[i];
             }
         }
+    }
+
+    // ------------------------------------------------------- CorrectVolume
+    // Uniform number in [0, 1): SplitMix64 (Steele, Lea and Flood, 2014) of
+    // the call count, both particles' indices, the visit and the axis; top
+    // 24 bits.  Stands in for the reference's unseeded std::mt19937.
+    static float cv_uniform(unsigned long long call, long long i, long long j, int visit, int axis) {
+        unsigned long long z = call * 0x9E3779B97F4A7C15ull + (unsigned long long)i * 0xBF58476D1CE4E5B9ull +
+                               (unsigned long long)j * 0x94D049BB133111EBull + (unsigned long long)(visit * 3 + axis);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return float(z >> 40) * (1.0f / 16777216.0f);
+    }
+    // HashNeighborSearch::GetImpactRegion (NeighborSearch.h:87-95)
+    void cv_region(const S* q, int lo[3], int hi[3]) const {
+        int c[3];
+        point2index(q, c);
+        const int n[3] = {nx, ny, nz};
+        for (int i = 0; i < 3; ++i) {
+            lo[i] = std::min(std::max(c[i] - 1, 0), n[i] - 1);
+            hi[i] = std::min(std::max(c[i] + 1, 0), n[i] - 1);
+        }
+    }
+    // LiquidModel<3>::CorrectVolume (LiquidModel.cpp:1086-1132) with the
+    // neighbour lists of the current positions: a neighbour within one
+    // radius counts once per cell its impact region shares with the
+    // particle's (HashNeighborSearch lists a particle once per cell of its
+    // region, NeighborSearch.h:62-83, and the query walks the cells of the
+    // particle's region, :22-50).  Neighbours are visited cell by cell (x, y,
+    // z over the region grown by one cell), in caller order within a cell.
+    void correct_volume(S dt) {
+        if (np == 0) return;
+        const S weightFactor = std::sqrt(dx[0] * dx[1] * dx[2]);
+        // cell lists, stable in caller order
+        const int64_t ncell = int64_t(nx) * ny * nz;
+        std::vector<int32_t> start(ncell + 1, 0), ids(np);
+        std::vector<int64_t> key(np);
+        for (int64_t i = 0; i < np; ++i) {
+            int c[3];
+            point2index(&pos[3 * i], c);
+            c[0] = std::min(std::max(c[0], 0), nx - 1);
+            c[1] = std::min(std::max(c[1], 0), ny - 1);
+            c[2] = std::min(std::max(c[2], 0), nz - 1);
+            key[i] = (int64_t(c[0]) * ny + c[1]) * nz + c[2];
+            start[key[i] + 1]++;
+        }
+        for (int64_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
+        {
+            std::vector<int32_t> fill(start.begin(), start.end() - 1);
+            for (int64_t i = 0; i < np; ++i) ids[fill[key[i]]++] = int32_t(i);
+        }
+        std::vector<S> buffer(3 * np);
+#pragma omp parallel for num_threads(nthreads()) schedule(dynamic, 256)
+        for (int64_t pi = 0; pi < np; ++pi) {
+            if (pi % correct_cycle != correct_step) continue;
+            const S* p = &pos[3 * pi];
+            const S r = radius, r2 = r * r;
+            int lo[3], hi[3];
+            cv_region(p, lo, hi);
+            S repel[3] = {S(0), S(0), S(0)};
+            for (int cx = std::max(lo[0] - 1, 0); cx <= std::min(hi[0] + 1, nx - 1); ++cx)
+                for (int cy = std::max(lo[1] - 1, 0); cy <= std::min(hi[1] + 1, ny - 1); ++cy)
+                    for (int cz = std::max(lo[2] - 1, 0); cz <= std::min(hi[2] + 1, nz - 1); ++cz) {
+                        const int64_t c = (int64_t(cx) * ny + cy) * nz + cz;
+                        for (int32_t s = start[c]; s < start[c + 1]; ++s) {
+                            const int64_t npi = ids[s];
+                            if (npi == pi) continue;
+                            const S* q = &pos[3 * npi];
+                            const S dir[3] = {S(p[0] - q[0]), S(p[1] - q[1]), S(p[2] - q[2])};
+                            const S d2 = sqnorm3(dir[0], dir[1], dir[2]);
+                            if (d2 >= r2) continue;
+                            int lj[3], hj[3];
+                            cv_region(q, lj, hj);
+                            int mult = 1;
+                            for (int i = 0; i < 3; ++i)
+                                mult *= std::max(0, std::min(hi[i], hj[i]) - std::max(lo[i], lj[i]) + 1);
+                            if (mult == 0) continue;
+                            const S dist = std::sqrt(d2);
+                            const S weight = weightFactor * qweight(S(dist / r));
+                            if (double(dist) > 1e-4 * double(r)) {
+                                const S wr = weight * r;
+                                const S t[3] = {S(wr * S(dir[0] / dist)), S(wr * S(dir[1] / dist)),
+                                                S(wr * S(dir[2] / dist))};
+                                for (int v = 0; v < mult; ++v)
+                                    for (int i = 0; i < 3; ++i) repel[i] += t[i];
+                            } else {
+                                const S rdt = r / dt;
+                                for (int v = 0; v < mult; ++v)
+                                    for (int i = 0; i < 3; ++i)
+                                        repel[i] += rdt * S(cv_uniform(correct_calls, pi, npi, v, i));
+                            }
+                        }
+                    }
+            S np3[3];
+            for (int i = 0; i < 3; ++i) np3[i] = p[i] + repel[i] * dt;
+            const S sphi = solid_phi_at(np3[0], np3[1], np3[2]);
+            if (sphi < S(0.0)) {
+                S g[3];
+                solid_gradient(np3[0], np3[1], np3[2], g);
+                for (int i = 0; i < 3; ++i) np3[i] -= sphi * g[i];
+            }
+            for (int i = 0; i < 3; ++i) buffer[3 * pi + i] = np3[i];
+        }
+        for (int64_t pi = 0; pi < np; ++pi) {
+            if (pi % correct_cycle != correct_step) continue;
+            for (int i = 0; i < 3; ++i) pos[3 * pi + i] = buffer[3 * pi + i];
+        }
+        correct_step = (correct_step + 1) % correct_cycle;
+        ++correct_calls;
     }
 
     // --------------------------------------------------------- extrapolation
@@ -1139,6 +1255,45 @@ const char* lho_last_error(void) { return g_scene_error.c_str(); }
 
 void lho_set_threads(int32_t n) { g_threads = n > 0 ? n : 0; }
 
+// LiquidModel<3>::Render (LiquidModel.cpp:1138-1159) restated without GL:
+// Shader/Scene3D_vertex.glsl:9 in float, then the fixed-function point
+// rasterisation the reference relies on (clip to [-1, 1]^3, viewport
+// x_w = (x + 1) * width / 2, pixels whose centres lie in the square of side
+// pointSize around the point, one colour, no depth test).
+int lho_render(const float* pos, int64_t n, const float mn[3], const float mx[3], const lhi_render_params* rp,
+               float* ndc, uint8_t* rgba) {
+    if (!rp || rp->width < 1 || rp->height < 1) return LHI_E_INVALID_ARG;
+    const int64_t npix = int64_t(rp->width) * rp->height;
+    if (rgba)
+        for (int64_t i = 0; i < npix; ++i) std::memcpy(rgba + 4 * i, rp->background, 4);
+    auto cover = [](float v, int extent, float size, int& lo, int& hi) {
+        const float xw = (v + 1.0f) * (0.5f * float(extent));
+        const float h = size * 0.5f;
+        lo = int(std::ceil((xw - h) - 0.5f));
+        hi = int(std::ceil((xw + h) - 0.5f)) - 1;
+        lo = std::max(lo, 0);
+        hi = std::min(hi, extent - 1);
+    };
+    for (int64_t k = 0; k < n; ++k) {
+        float p[3];
+        for (int i = 0; i < 3; ++i) {
+            const float a = pos[3 * k + i] - mn[i];
+            const float b = mx[i] - mn[i];
+            p[i] = (a / b) * 2.0f - 1.0f;
+        }
+        if (ndc)
+            for (int i = 0; i < 3; ++i) ndc[3 * k + i] = p[i];
+        if (!rgba) continue;
+        if (!(p[0] >= -1.f && p[0] <= 1.f && p[1] >= -1.f && p[1] <= 1.f && p[2] >= -1.f && p[2] <= 1.f)) continue;
+        int x0, x1, y0, y1;
+        cover(p[0], rp->width, rp->point_size, x0, x1);
+        cover(p[1], rp->height, rp->point_size, y0, y1);
+        for (int j = y0; j <= y1; ++j)
+            for (int i = x0; i <= x1; ++i) std::memcpy(rgba + 4 * (int64_t(j) * rp->width + i), rp->color, 4);
+    }
+    return LHI_OK;
+}
+
 void lho_set_omp_default_threads(int32_t n) {
     if (n > 0) omp_set_num_threads(n);
 }
@@ -1310,8 +1465,13 @@ int lho_step(lho_model* m, double dt, int32_t extrap_mode, lhi_solve_stats* stat
         M->extrapolate(extrap_mode);
         M->grid_to_particle();
         M->advect(sdt);
+        if (M->correct_in_step) M->correct_volume(sdt);
         if (stats) *stats = M->last;
     });
+    return 0;
+}
+int lho_correct_volume(lho_model* m, double dt) {
+    DISPATCH(m, M->correct_volume(S(dt)));
     return 0;
 }
 int lho_compute_divergence(lho_model* m, double* mean, double* max_abs) {

@@ -82,6 +82,7 @@ LHO_API int lho_grid_to_particle(lho_model* m);
 LHO_API int lho_advect_particles(lho_model* m, double dt);
 LHO_API int lho_pre_step(lho_model* m, double dt);
 LHO_API int lho_step(lho_model* m, double dt, int32_t extrap_mode, lhi_solve_stats* stats);
+LHO_API int lho_correct_volume(lho_model* m, double dt);
 LHO_API int lho_compute_divergence(lho_model* m, double* mean, double* max_abs);
 LHO_API int lho_get_cfl(lho_model* m, double* dt_out);
 
@@ -96,6 +97,12 @@ LHO_API int lho_solver_get_ax(lho_model* m, int32_t level, const void* x, void* 
    sorted_ids[k] = caller index of the k-th particle, cell_start[ncells+1]. */
 LHO_API int lho_cell_keys(lho_model* m, int32_t* keys);
 LHO_API int lho_sort_by_cell(lho_model* m, int32_t* sorted_ids, int32_t* cell_start);
+
+/* LiquidModel<3>::Render restated without a graphics API (see
+   lhi_liquid_render in lhi.h): float positions (n x 3) -> the vertex
+   shader's coordinates and the RGBA image (row 0 at the bottom). */
+LHO_API int lho_render(const float* pos, int64_t n, const float mn[3], const float mx[3],
+                       const lhi_render_params* params, float* ndc, uint8_t* rgba);
 
 /* ParticleSystem<3>::SpawnParticles restated (ParticleSystem.cpp:45-64). */
 LHO_API int64_t lho_spawn_lattice(const double min_coord[3], const double max_coord[3],

@@ -50,6 +50,7 @@ def _load_oracle():
     lib.lho_projection.argtypes = [_vp, C.c_double, C.POINTER(abi.SolveStats)]
     lib.lho_extrapolate.argtypes = [_vp, C.c_int32]
     lib.lho_step.argtypes = [_vp, C.c_double, C.c_int32, C.POINTER(abi.SolveStats)]
+    lib.lho_correct_volume.argtypes = [_vp, C.c_double]
     lib.lho_compute_divergence.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.lho_get_cfl.argtypes = [_vp, C.POINTER(C.c_double)]
     lib.lho_solver_build_lhs.argtypes = [_vp, C.c_double, C.c_double]
@@ -63,6 +64,8 @@ def _load_oracle():
     lib.lhi_scene_seed_particles.argtypes = [C.POINTER(abi.GridDesc), C.POINTER(abi.BoundaryNode), C.c_int32,
                                              C.c_int32, C.POINTER(abi.FluidPrim), C.c_int32, C.c_uint64,
                                              C.c_int32, C.POINTER(C.c_int64), _vp, _vp]
+    lib.lho_render.argtypes = [_vp, C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                               C.POINTER(abi.RenderParams), _vp, _vp]
     lib.lho_spawn_lattice.restype = C.c_int64
     lib.lho_spawn_lattice.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
                                       C.c_int64, C.c_int32, _vp]
@@ -207,6 +210,9 @@ class Oracle:
         self.lib.lho_compute_divergence(self.h, C.byref(m), C.byref(mx))
         return m.value, mx.value
 
+    def correct_volume(self, dt):
+        self.lib.lho_correct_volume(self.h, dt)
+
     def cfl(self):
         d = C.c_double()
         self.lib.lho_get_cfl(self.h, C.byref(d))
@@ -285,6 +291,22 @@ def seed_scene(spec, precision="fp32"):
     if rc:
         raise RuntimeError(f"lhi_scene_seed_particles failed ({rc})")
     return pos, vel
+
+
+def render(pos, min_coord, max_coord, width=480, height=480, point_size=5.0, color=(0, 0, 255, 255),
+           background=(255, 255, 255, 255)):
+    """(image height x width x 4, ndc n x 3) of LiquidModel<3>::Render restated."""
+    lib = oracle_lib()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    mn = (C.c_float * 3)(*min_coord)
+    mx = (C.c_float * 3)(*max_coord)
+    rp = abi.make_render_params(width, height, point_size, color, background)
+    img = np.empty((height, width, 4), np.uint8)
+    ndc = np.empty_like(p)
+    rc = lib.lho_render(_ptr(p), p.shape[0], mn, mx, C.byref(rp), _ptr(ndc), _ptr(img))
+    if rc:
+        raise ValueError("lho_render: bad parameters")
+    return img, ndc
 
 
 def spawn_lattice(min_coord, max_coord, default_radius, max_count, dbl=False):

@@ -28,5 +28,5 @@ def test_cpp_scene_loop_runs_on_gpu(lhi):
     res = json.loads(out.stdout.strip().splitlines()[-1])
     print(res)
     assert res["particles"] > 10000
-    assert res["correct_volume_throws"]
+    assert res["correct_volume_moved"] > 0
     assert 0.0 < res["ymin"] < res["ymax"] < 0.6

@@ -52,3 +52,20 @@ def test_checkpoint_restores_exact_bits(tmp_path, dtype):
     for k, want in (("pos", pos), ("vel", vel), ("affine", aff)):
         assert c[k].dtype == dtype and np.array_equal(c[k].view(np.uint8), want.view(np.uint8))
     assert c["step"] == 17 and c["time"] == 0.0354
+
+
+def test_render_oracle_pixel_rule(oracle_mod):
+    """The oracle's point rasterisation on a 16 x 16 image with 5-pixel
+    points: a point at the domain centre covers pixels 5..9 on both axes, a
+    point on the min corner the 2 x 2 pixels it overlaps, and a point beyond
+    the max face is clipped."""
+    import numpy as np
+    pos = np.array([[0.5, 0.5, 0.5], [0.0, 0.0, 0.0], [1.2, 0.5, 0.5]], np.float32)
+    img, ndc = oracle_mod.render(pos, (0, 0, 0), (1, 1, 1), 16, 16, 5.0)
+    assert np.array_equal(ndc[:2], [[0, 0, 0], [-1, -1, -1]])
+    covered = img[..., 0] == 0
+    want = np.zeros((16, 16), bool)
+    want[5:10, 5:10] = True
+    want[0:2, 0:2] = True
+    assert np.array_equal(covered, want)
+    assert (img[covered] == [0, 0, 255, 255]).all() and (img[~covered] == 255).all()
