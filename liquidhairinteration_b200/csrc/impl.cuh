@@ -367,8 +367,6 @@ public:
     bool keys_fresh_ = false;  // keys_[0]/vals_[0] hold (cell key, identity) of the current order
     uint32_t* keys_[2] = {nullptr, nullptr};
     int32_t* vals_[2] = {nullptr, nullptr};
-    uint32_t* hist_ = nullptr;  // radix histograms
-    long long hist_cap_ = 0;
     int32_t* cell_count_ = nullptr;  // ncell + 1
     int32_t* cell_start_ = nullptr;  // ncell + 1
     // headless render: RGBA image and normalised device coordinates, sized on first use
@@ -432,12 +430,9 @@ public:
     T* p_ptr(int k) const { return pdata_[pcur_] + size_t(k) * size_t(pcap_); }
 };
 
-// radix-sort / scan helpers (k_sort.cu)
+// device-wide exclusive scan (k_sort.cu)
 void device_exclusive_scan_i32(const int32_t* in, int32_t* out, long long n, void* tmp, long long tmp_bytes,
                                cudaStream_t s);
 long long scan_tmp_bytes(long long n);
-void radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], int& cur, long long n, int key_bits, uint32_t* hist,
-                      void* tmp, long long tmp_bytes, cudaStream_t s);
-long long radix_hist_entries(long long n);
 
 }  // namespace lhi

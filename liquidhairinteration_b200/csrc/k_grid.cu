@@ -459,7 +459,6 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
     F(cell_count_);
     F(cell_start_);
     F(scan_tmp_);
-    F(hist_);
     for (int b = 0; b < 2; ++b) {
         F(pdata_[b]);
         F(pid_[b]);

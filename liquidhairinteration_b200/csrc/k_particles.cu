@@ -56,6 +56,72 @@ __global__ void k_cell_count(const uint32_t* __restrict__ keys, long long n, int
     if (valid && (peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&count[key], int(__popc(peers)));
 }
 
+// Counting-sort scatter: particle i goes to cell_start[key] + its rank among
+// the particles of its cell.  Lanes of a warp with the same key take
+// consecutive ranks in lane order from one atomic add; warps take their
+// blocks of ranks in whatever order the atomics land, so k_cell_order then
+// sorts every cell's indices, which makes the whole order the stable one.
+__global__ void k_rank_scatter(const uint32_t* __restrict__ keys, long long n, const int32_t* __restrict__ cs,
+                               int32_t* __restrict__ cursor, uint32_t* __restrict__ skeys,
+                               int32_t* __restrict__ order) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t key = valid ? keys[i] : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const unsigned lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (valid && int(lane) == leader) base = atomicAdd(&cursor[key], int(__popc(peers)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!valid) return;
+    const long long pos = (long long)cs[key] + base + __popc(peers & ((1u << lane) - 1u));
+    skeys[pos] = key;
+    order[pos] = int32_t(i);
+}
+
+// Sorts the indices of every cell ascending (insertion sort for the usual
+// handful, heap sort for a crowded cell), so equal keys keep their input
+// order: the result is the stable sort by cell key.
+__global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, int32_t* __restrict__ order) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const int s = cs[c], e = cs[c + 1];
+    const int len = e - s;
+    if (len <= 1) return;
+    int32_t* a = order + s;
+    if (len <= 64) {
+        for (int i = 1; i < len; ++i) {
+            const int32_t v = a[i];
+            int j = i - 1;
+            while (j >= 0 && a[j] > v) {
+                a[j + 1] = a[j];
+                --j;
+            }
+            a[j + 1] = v;
+        }
+        return;
+    }
+    auto sift = [&](int root, int end) {  // max-heap on a[0, end)
+        while (true) {
+            int ch = 2 * root + 1;
+            if (ch >= end) return;
+            if (ch + 1 < end && a[ch + 1] > a[ch]) ++ch;
+            if (a[root] >= a[ch]) return;
+            const int32_t t = a[root];
+            a[root] = a[ch];
+            a[ch] = t;
+            root = ch;
+        }
+    };
+    for (int r = len / 2 - 1; r >= 0; --r) sift(r, len);
+    for (int end = len - 1; end > 0; --end) {
+        const int32_t t = a[0];
+        a[0] = a[end];
+        a[end] = t;
+        sift(0, end);
+    }
+}
+
 __global__ void k_occupancy(const int32_t* __restrict__ cs, int nx, int ny, int nz, uint8_t* __restrict__ occ,
                             int ox, int oy, int oz) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -577,7 +643,13 @@ template <class T> __device__ void solid_grad_at(const GridP<T>& g, const T* sp,
 // consecutive nodes; the sum visits that run in the reference's ascending
 // order.  The x.y weight products are formed once per (x, y) pair: the same
 // products as the reference's (wX * wY) * wZ, so every term is bit-identical.
-template <class T, int A>
+// FACTORED (the mixed-precision handles): the weights are separable, so the
+// sums are taken axis by axis -- per (x, y) column S = sum wZ v and
+// T = sum gZ v, then per x A = sum wY S, B = sum gY S, D = sum wY T, then
+// v = sum wX A, C = (sum gX A, sum wX B, sum wX D) -- with fused
+// multiply-adds: about a third of the arithmetic, the same value up to
+// rounding.
+template <class T, int A, bool FACTORED>
 __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3], const T g3[3], const int ci[3],
                                               const T* __restrict__ vf, T& velA, T col[3]) {
     const int hmax[3] = {g.nx - 1 + (A == 0), g.ny - 1 + (A == 1), g.nz - 1 + (A == 2)};
@@ -610,6 +682,33 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
             eg[i][j] = j < cnt[i] ? gqweight(e) : T(0);
         }
     }
+    if constexpr (FACTORED) {
+#pragma unroll
+        for (int jx = 0; jx < 3; ++jx) {
+            if (jx >= cnt[0]) break;
+            T a = T(0), b = T(0), dd = T(0);
+#pragma unroll
+            for (int jy = 0; jy < 3; ++jy) {
+                if (jy >= cnt[1]) break;
+                const T* row = vf + ((long long)(first[0] + jx) * fy + (first[1] + jy)) * fz + first[2];
+                T s = T(0), t = T(0);
+#pragma unroll
+                for (int jz = 0; jz < 3; ++jz) {
+                    if (jz >= cnt[2]) break;
+                    const T val = row[jz];
+                    s = fma(ew[2][jz], val, s);
+                    t = fma(eg[2][jz], val, t);
+                }
+                a = fma(ew[1][jy], s, a);
+                b = fma(eg[1][jy], s, b);
+                dd = fma(ew[1][jy], t, dd);
+            }
+            velA = fma(ew[0][jx], a, velA);
+            col[0] = fma(eg[0][jx], a, col[0]);
+            col[1] = fma(ew[0][jx], b, col[1]);
+            col[2] = fma(ew[0][jx], dd, col[2]);
+        }
+    } else {
 #pragma unroll
     for (int jx = 0; jx < 3; ++jx) {
         if (jx >= cnt[0]) break;
@@ -636,11 +735,12 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
             }
         }
     }
+    }
 }
 
 // LiquidModel<3>::Grid2Particle (LiquidModel.cpp:724-823) fused with
 // AdvectParticle (LiquidModel.cpp:913-935) and the next step's cell key.
-template <class T>
+template <class T, bool FACTORED>
 __global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, long long cap, long long n, int d0,
                                              int d1, int d2, const T* __restrict__ vx, const T* __restrict__ vy,
                                              const T* __restrict__ vz, int do_g2p, int do_advect, T dt,
@@ -663,9 +763,9 @@ __global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, lon
         vel[0] = vel[1] = vel[2] = T(0);
 #pragma unroll
         for (int k = 0; k < 9; ++k) C[k] = T(0);
-        g2p_component<T, 0>(g, d, g3, ci, vx, vel[0], &C[0]);
-        g2p_component<T, 1>(g, d, g3, ci, vy, vel[1], &C[3]);
-        g2p_component<T, 2>(g, d, g3, ci, vz, vel[2], &C[6]);
+        g2p_component<T, 0, FACTORED>(g, d, g3, ci, vx, vel[0], &C[0]);
+        g2p_component<T, 1, FACTORED>(g, d, g3, ci, vy, vel[1], &C[3]);
+        g2p_component<T, 2, FACTORED>(g, d, g3, ci, vz, vel[2], &C[6]);
 #pragma unroll
         for (int k = 0; k < 3; ++k) pd[(3 + k) * cap + i] = vel[k];
 #pragma unroll
@@ -853,18 +953,6 @@ template <class T, class TX> void LiquidImpl<T, TX>::alloc_particles(int64_t cap
         LHI_CUDA(cudaMalloc(&keys_[b], sizeof(uint32_t) * size_t(cap)));
         LHI_CUDA(cudaMalloc(&vals_[b], sizeof(int32_t) * size_t(cap)));
     }
-    long long he = radix_hist_entries(cap);
-    if (he > hist_cap_) {
-        if (hist_) cudaFree(hist_);
-        LHI_CUDA(cudaMalloc(&hist_, sizeof(uint32_t) * size_t(he)));
-        hist_cap_ = he;
-    }
-    long long need = std::max(scan_tmp_bytes(he), scan_tmp_bytes(ncell_ + 1));
-    if (need > scan_tmp_bytes_) {
-        if (scan_tmp_) cudaFree(scan_tmp_);
-        LHI_CUDA(cudaMalloc(&scan_tmp_, size_t(need)));
-        scan_tmp_bytes_ = need;
-    }
     pcap_ = cap;
     pcur_ = 0;
 }
@@ -909,25 +997,30 @@ template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
                                                                  vals_[0]);
             LHI_LAUNCH_CHECK();
         }
-        int kbits = 1;
-        while ((1LL << kbits) < ncell_) ++kbits;
-        int kc = 0;
-        radix_sort_pairs(keys_, vals_, kc, np_, kbits, hist_, scan_tmp_, scan_tmp_bytes_, stream_);
-        k_permute<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_,
-                                                                pid_[pcur_], pid_[pcur_ ^ 1], vals_[kc], np_);
-        LHI_LAUNCH_CHECK();
-        pcur_ ^= 1;
-        if (kc != 0) {  // keep the sorted keys in keys_[0]
-            std::swap(keys_[0], keys_[1]);
-            std::swap(vals_[0], vals_[1]);
-        }
     }
+    // counting sort by cell key: per-cell counts, their exclusive scan (the
+    // cell ranges), a scatter by atomic ranks, then each cell's indices in
+    // input order -- the stable sort, one read of the keys per pass
     LHI_CUDA(cudaMemsetAsync(cell_count_, 0, sizeof(int32_t) * size_t(ncell_ + 1), stream_));
     if (np_ > 0) {
         k_cell_count<<<blocks_for(np_, 256), 256, 0, stream_>>>(keys_[0], np_, cell_count_);
         LHI_LAUNCH_CHECK();
     }
     device_exclusive_scan_i32(cell_count_, cell_start_, ncell_ + 1, scan_tmp_, scan_tmp_bytes_, stream_);
+    if (np_ > 0) {
+        LHI_CUDA(cudaMemsetAsync(cell_count_, 0, sizeof(int32_t) * size_t(ncell_), stream_));  // rank cursors
+        k_rank_scatter<<<blocks_for(np_, 256), 256, 0, stream_>>>(keys_[0], np_, cell_start_, cell_count_, keys_[1],
+                                                                 vals_[1]);
+        LHI_LAUNCH_CHECK();
+        k_cell_order<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, ncell_, vals_[1]);
+        LHI_LAUNCH_CHECK();
+        k_permute<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_,
+                                                                pid_[pcur_], pid_[pcur_ ^ 1], vals_[1], np_);
+        LHI_LAUNCH_CHECK();
+        pcur_ ^= 1;
+        std::swap(keys_[0], keys_[1]);  // the sorted keys in keys_[0]
+        std::swap(vals_[0], vals_[1]);
+    }
     LHI_CUDA(cudaMemsetAsync(occ_, 0, size_t(occ_dim_[0]) * occ_dim_[1] * occ_dim_[2], stream_));
     k_occupancy<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, nx_, ny_, nz_, occ_, occ_dim_[0],
                                                               occ_dim_[1], occ_dim_[2]);
@@ -1012,9 +1105,10 @@ template <class T, class TX> void LiquidImpl<T, TX>::g2p(bool do_advect, T dt) {
     if (np_ == 0) return;
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
     auto ps_ = scope(LHI_KERNEL_G2P);
-    k_g2p<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
-                                                        v_[1], v_[2], 1, do_advect ? 1 : 0, dt, solid_phi_,
-                                                        keys_[0], vals_[0]);
+    // mixed precision takes the factored sums; FP32 and FP64 keep the reference's order bit for bit
+    auto kern = precision_ == LHI_PRECISION_MIXED ? k_g2p<T, true> : k_g2p<T, false>;
+    kern<<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0], v_[1],
+                                                    v_[2], 1, do_advect ? 1 : 0, dt, solid_phi_, keys_[0], vals_[0]);
     LHI_LAUNCH_CHECK();
     if (do_advect) {
         sorted_ = false;
@@ -1028,8 +1122,9 @@ template <class T, class TX> void LiquidImpl<T, TX>::advect(double dt) {
     if (np_ == 0) return;
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
     auto ps_ = scope(LHI_KERNEL_G2P);
-    k_g2p<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
-                                                        v_[1], v_[2], 0, 1, T(dt), solid_phi_, keys_[0], vals_[0]);
+    k_g2p<T, false><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2,
+                                                               v_[0], v_[1], v_[2], 0, 1, T(dt), solid_phi_, keys_[0],
+                                                               vals_[0]);
     LHI_LAUNCH_CHECK();
     sorted_ = false;
     keys_fresh_ = true;

@@ -193,3 +193,30 @@ def test_divergence_vs_oracle(po, lhi, prec, projected):
     assert abs(mean_g - vals.mean()) <= 1e-12 * scale, (mean_g, vals.mean())
     # the oracle sums in the grid's type, as the reference does
     assert abs(mean_o - vals.mean()) <= (1e-12 if prec == "fp64" else 1e-4) * scale, (mean_o, vals.mean())
+
+
+def test_g2p_factored_mixed_close(po, lhi):
+    """Mixed-precision handles gather with the factored (axis-by-axis, fused)
+    sums: velocity and affine matrix within rounding of the oracle's
+    per-node sums (LiquidModel.cpp:724-823), positions after advection too."""
+    spec = obstacle_scene(32)
+    g = gpu_model(spec, "mixed")
+    o = oracle_model(po, spec, "fp32")
+    pos, vel = scenes.seed(spec, "fp32")
+    g.GetParticleSystem().SetParticles(pos, vel)
+    o.set_particles(pos, vel)
+    rng = np.random.default_rng(17)
+    for f in ("vx", "vy", "vz"):
+        v = (rng.standard_normal(o.field(f).size) * 2).astype(np.float32)
+        o.set_field(f, v)
+        g.set_field(f, v)
+    o.grid_to_particle()
+    g.Grid2Particle()
+    _, v_g, a_g = g.GetParticleSystem().GetParticles()
+    _, v_o, a_o = o.get_particles()
+    assert_close(v_g, v_o, 1e-5, 1e-5 * np.abs(v_o).max(), "velocity")
+    assert_close(a_g, a_o, 1e-5, 1e-5 * np.abs(a_o).max(), "affine")
+    o.advect_particles(spec.dt)
+    g.AdvectParticle(spec.dt)
+    d = np.abs(g.GetParticleSystem().GetPositions() - o.get_particles()[0]).max()
+    assert d < 1e-5 * spec.dx, d / spec.dx
