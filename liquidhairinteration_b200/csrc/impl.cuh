@@ -10,6 +10,7 @@
 #pragma once
 
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -417,6 +418,15 @@ public:
     float* train_e_ = nullptr;
     double* train_red_ = nullptr;    // [0] sum e^2, [1] sum r^2, [2] loss accumulator
     T* rhs_ = nullptr;
+    // mixed mode (T = float, TX = double): the finest level's right-hand side
+    // and matrix assembled in FP64 from the same float fields, for the outer
+    // CG's true residual and final check, so the iteration converges to the
+    // FP64 system's solution; the V-cycle and the loop's SpMV stay FP32
+    static constexpr bool kHiResidual = std::is_same<T, float>::value && std::is_same<TX, double>::value;
+    double dxd_[3] = {0, 0, 0};  // grid spacing in double, as an FP64 model of the same grid computes it
+    double* rhs_hi_ = nullptr;
+    double* diag_hi_ = nullptr;
+    double* cf_hi_[3] = {nullptr, nullptr, nullptr};
     TX* x_ = nullptr;
     T* p_ = nullptr;
     T* ap_ = nullptr;

@@ -319,6 +319,7 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
         T interval = max_[i] - min_[i];
         dx_[i] = T(interval / T(dims[i]));
         if (!(dx_[i] > T(0))) throw std::invalid_argument("max_coord must exceed min_coord");
+        dxd_[i] = (g.max_coord[i] - g.min_coord[i]) / double(dims[i]);
     }
     radius_ = lp.particle_radius > 0 ? T(lp.particle_radius) : T(2 * dx_[0]);
     density_ = T(lp.density);
@@ -425,6 +426,16 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     LHI_CUDA(cudaMemsetAsync(x_, 0, sizeof(TX) * ncell_, stream_));
     LHI_CUDA(cudaMemsetAsync(p_, 0, sizeof(T) * ncell_, stream_));
     LHI_CUDA(cudaMemsetAsync(ap_, 0, sizeof(T) * ncell_, stream_));
+    if constexpr (kHiResidual) {
+        LHI_CUDA(cudaMalloc(&rhs_hi_, sizeof(double) * ncell_));
+        LHI_CUDA(cudaMalloc(&diag_hi_, sizeof(double) * ncell_));
+        LHI_CUDA(cudaMemsetAsync(rhs_hi_, 0, sizeof(double) * ncell_, stream_));
+        LHI_CUDA(cudaMemsetAsync(diag_hi_, 0, sizeof(double) * ncell_, stream_));
+        for (int a = 0; a < 3; ++a) {
+            LHI_CUDA(cudaMalloc(&cf_hi_[a], sizeof(double) * ncell_));
+            LHI_CUDA(cudaMemsetAsync(cf_hi_[a], 0, sizeof(double) * ncell_, stream_));
+        }
+    }
     setup_spmv();
     LHI_CUDA(cudaMalloc(&sc_, sizeof(SolveScalars)));
     LHI_CUDA(cudaMemsetAsync(sc_, 0, sizeof(SolveScalars), stream_));
@@ -489,6 +500,9 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
     F(train_red_);
     if (side_) cudaStreamDestroy(side_);
     F(rhs_);
+    F(rhs_hi_);
+    F(diag_hi_);
+    for (int a = 0; a < 3; ++a) F(cf_hi_[a]);
     F(x_);
     F(p_);
     F(ap_);

@@ -49,6 +49,12 @@ template <class T> LevelK<T> lk(const LevelDev<T>& L) {
     return LevelK<T>{L.nx, L.ny, L.nz, L.diag, L.cf[0], L.cf[1], L.cf[2], L.type};
 }
 
+// the mixed mode's FP64 finest-level matrix with the level's cell types
+template <class T, class TX> LevelK<double> lk_hi(const LiquidImpl<T, TX>& s) {
+    const LevelDev<T>& L = s.lv_[0];
+    return LevelK<double>{L.nx, L.ny, L.nz, s.diag_hi_, s.cf_hi_[0], s.cf_hi_[1], s.cf_hi_[2], L.type};
+}
+
 __device__ __forceinline__ void decode(long long i, int ny, int nz, int& x, int& y, int& z) { idx3(i, ny, nz, x, y, z); }
 
 // CGSolver<3>::GetAx (PressureSolver.cpp:700-717), computed in C
@@ -180,10 +186,12 @@ __global__ void k_level_phi(LevelGeom g, const T* __restrict__ fine_phi, T* __re
     if (t != 0) tile_flag[((long long)(x / kTileX) * tdy + y / kTileY) * tdz + z / kTileZ] = 1;
 }
 
-// CGSolver<3>::BuildLHS for one level (PressureSolver.cpp:544-664).
-template <class T>
-__global__ void k_level_matrix(LevelGeom g, const T* __restrict__ phi, const T* __restrict__ lwx,
-                               const T* __restrict__ lwy, const T* __restrict__ lwz, T h0, T h1, T h2, T dt, T rho,
+// CGSolver<3>::BuildLHS for one level (PressureSolver.cpp:544-664), in T
+// from fields of type TI (TI = float, T = double: the FP64 finest-level
+// matrix the mixed mode's outer residual uses).
+template <class T, class TI = T>
+__global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI* __restrict__ lwx,
+                               const TI* __restrict__ lwy, const TI* __restrict__ lwz, T h0, T h1, T h2, T dt, T rho,
                                T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy, T* __restrict__ cz) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)g.nx * g.ny * g.nz;
@@ -191,7 +199,7 @@ __global__ void k_level_matrix(LevelGeom g, const T* __restrict__ phi, const T* 
     int x, y, z;
     decode(i, g.ny, g.nz, x, y, z);
     const long long sy = g.nz, sx = (long long)g.ny * g.nz;
-    const T* lw[3] = {lwx, lwy, lwz};
+    const TI* lw[3] = {lwx, lwy, lwz};
     const T hh[3] = {h0, h1, h2};
     auto term_of = [&](int a, T w) -> T {
         return X<T>::div(X<T>::mul(w, dt), X<T>::mul(X<T>::mul(rho, hh[a]), hh[a]));
@@ -203,7 +211,7 @@ __global__ void k_level_matrix(LevelGeom g, const T* __restrict__ phi, const T* 
         int dd[3] = {g.nx, g.ny, g.nz};
         for (int a = 0; a < 3; ++a) {
             if (cc[a] + 1 < dd[a]) {
-                T w = approx_w(lw[a], g, a, x + (a == 0), y + (a == 1), z + (a == 2));
+                T w = T(approx_w(lw[a], g, a, x + (a == 0), y + (a == 1), z + (a == 2)));
                 if (w > T(0)) c[a] = -term_of(a, w);
             }
         }
@@ -211,7 +219,7 @@ __global__ void k_level_matrix(LevelGeom g, const T* __restrict__ phi, const T* 
     cx[i] = c[0];
     cy[i] = c[1];
     cz[i] = c[2];
-    const T center = phi[i];
+    const T center = T(phi[i]);
     T d = T(0);
     if (!(center > T(0))) {
         // right, left, top, bottom, front, back
@@ -224,10 +232,10 @@ __global__ void k_level_matrix(LevelGeom g, const T* __restrict__ phi, const T* 
         for (int k = 0; k < 6; ++k) {
             if (!exists[k]) continue;
             const int a = ax[k];
-            T w = approx_w(lw[a], g, a, xs[k], ys[k], zs[k]);
+            T w = T(approx_w(lw[a], g, a, xs[k], ys[k], zs[k]));
             if (w > T(0)) {
                 T term = term_of(a, w);
-                T nphi = phi[i + off[k]];
+                T nphi = T(phi[i + off[k]]);
                 if (nphi < T(0)) d = X<T>::add(d, term);
                 else d = X<T>::add(d, X<T>::div(term, frac_floor(fraction_in_region(center, nphi))));
             }
@@ -237,27 +245,29 @@ __global__ void k_level_matrix(LevelGeom g, const T* __restrict__ phi, const T* 
 }
 
 // CGSolver<3>::BuildRHS (PressureSolver.cpp:682-698)
-template <class T>
-__global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const T* __restrict__ phi,
-                            const T* __restrict__ lwx, const T* __restrict__ lwy, const T* __restrict__ lwz,
-                            const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz,
+// (TI = float, T = double: the FP64 right-hand side of the mixed mode's
+// outer residual, from the same float fields)
+template <class T, class TI = T>
+__global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const TI* __restrict__ phi,
+                            const TI* __restrict__ lwx, const TI* __restrict__ lwy, const TI* __restrict__ lwz,
+                            const TI* __restrict__ vx, const TI* __restrict__ vy, const TI* __restrict__ vz,
                             T* __restrict__ rhs) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)nx * ny * nz;
     if (i >= n) return;
     T b = T(0);
-    if (!(phi[i] > T(0))) {
+    if (!(T(phi[i]) > T(0))) {
         int x, y, z;
         decode(i, ny, nz, x, y, z);
         long long fxi = ((long long)x * ny + y) * nz + z, fxs = (long long)ny * nz;
         long long fyi = ((long long)x * (ny + 1) + y) * nz + z, fys = nz;
         long long fzi = ((long long)x * ny + y) * (nz + 1) + z;
-        b = X<T>::sub(b, X<T>::div(X<T>::mul(lwx[fxi + fxs], vx[fxi + fxs]), h0));
-        b = X<T>::add(b, X<T>::div(X<T>::mul(lwx[fxi], vx[fxi]), h0));
-        b = X<T>::sub(b, X<T>::div(X<T>::mul(lwy[fyi + fys], vy[fyi + fys]), h1));
-        b = X<T>::add(b, X<T>::div(X<T>::mul(lwy[fyi], vy[fyi]), h1));
-        b = X<T>::sub(b, X<T>::div(X<T>::mul(lwz[fzi + 1], vz[fzi + 1]), h2));
-        b = X<T>::add(b, X<T>::div(X<T>::mul(lwz[fzi], vz[fzi]), h2));
+        b = X<T>::sub(b, X<T>::div(X<T>::mul(T(lwx[fxi + fxs]), T(vx[fxi + fxs])), h0));
+        b = X<T>::add(b, X<T>::div(X<T>::mul(T(lwx[fxi]), T(vx[fxi])), h0));
+        b = X<T>::sub(b, X<T>::div(X<T>::mul(T(lwy[fyi + fys]), T(vy[fyi + fys])), h1));
+        b = X<T>::add(b, X<T>::div(X<T>::mul(T(lwy[fyi]), T(vy[fyi])), h1));
+        b = X<T>::sub(b, X<T>::div(X<T>::mul(T(lwz[fzi + 1]), T(vz[fzi + 1])), h2));
+        b = X<T>::add(b, X<T>::div(X<T>::mul(T(lwz[fzi]), T(vz[fzi])), h2));
     }
     rhs[i] = b;
 }
@@ -1415,21 +1425,23 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_update_xr(LevelK<T> L, Tile
     cg_decide(sc, tot[0], cf, false);
 }
 
-// r = b - A x on the update region (stored when `store`), summed squares.
-template <class T, class TX>
+// r = b - A x on the update region (stored when `store`, as TR), summed
+// squares.  The mixed mode passes its FP64 finest-level matrix and
+// right-hand side here (T = double) with the FP32 residual (TR = float).
+template <class T, class TX, class TR>
 __device__ __forceinline__ void true_residual_sweep(const LevelK<T>& L, const TileK& tk, int region, const T* __restrict__ b,
-                                                    const TX* __restrict__ x, T* __restrict__ r, bool store, double& acc) {
+                                                    const TX* __restrict__ x, TR* __restrict__ r, bool store, double& acc) {
     for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zi, long long i) {
         if (L.type[i] == 0 || !in_region(xi, yi, zi, L.nx, L.ny, L.nz, region)) return;
         const double res = double(b[i]) - ax_at<double>(L, x, i, xi, yi, zi);
-        if (store) r[i] = T(res);
+        if (store) r[i] = TR(res);
         acc += res * res;
     });
 }
 
-template <class T, class TX>
+template <class T, class TX, class TR = T>
 __global__ void __launch_bounds__(kTileThreads) k_cg_true_residual(LevelK<T> L, TileK tk, const T* __restrict__ b,
-                                                                   const TX* __restrict__ x, T* __restrict__ r,
+                                                                   const TX* __restrict__ x, TR* __restrict__ r,
                                                                    double* __restrict__ partials,
                                                                    unsigned* __restrict__ counter,
                                                                    SolveScalars* __restrict__ sc, CgConf cf) {
@@ -1451,7 +1463,7 @@ __global__ void __launch_bounds__(kTileThreads) k_true_residual_final(LevelK<T> 
                                                                       unsigned* __restrict__ counter,
                                                                       double* __restrict__ out) {
     double v[1] = {0.0};
-    true_residual_sweep<T, TX>(L, tk, region, b, x, nullptr, false, v[0]);
+    true_residual_sweep<T, TX, T>(L, tk, region, b, x, nullptr, false, v[0]);
     grid_sum_finish<1>(v, partials, counter, out);
 }
 
@@ -1692,6 +1704,11 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_rhs() {
     k_build_rhs<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], liquid_phi_,
                                                               lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_);
     LHI_LAUNCH_CHECK();
+    if constexpr (kHiResidual) {
+        k_build_rhs<double, T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(
+            nx_, ny_, nz_, dxd_[0], dxd_[1], dxd_[2], liquid_phi_, lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_hi_);
+        LHI_LAUNCH_CHECK();
+    }
 }
 
 // CGSolver<3>::BuildLHS (PressureSolver.cpp:544-664) for every level, then
@@ -1711,6 +1728,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
                                                                   L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1],
                                                                   L.cf[2]);
         LHI_LAUNCH_CHECK();
+        if constexpr (kHiResidual) {
+            if (l == 0) {
+                k_level_matrix<double, T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
+                    g, liquid_phi_, lw_[0], lw_[1], lw_[2], dxd_[0], dxd_[1], dxd_[2], dt, rho, diag_hi_, cf_hi_[0],
+                    cf_hi_[1], cf_hi_[2]);
+                LHI_LAUNCH_CHECK();
+            }
+        }
     }
     build_tiles();
     build_masks();
@@ -2055,8 +2080,12 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_body(unsigned long 
                                                             cf);
         LHI_LAUNCH_CHECK();
         if (sp_.true_residual_every > 0) {
-            k_cg_true_residual<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, x_, L0.r, partials_, counter_,
-                                                                    sc_, cf);
+            if constexpr (kHiResidual)
+                k_cg_true_residual<double, TX, T><<<G, kTileThreads, 0, cur_>>>(lk_hi(*this), tk, rhs_hi_, x_, L0.r,
+                                                                                partials_, counter_, sc_, cf);
+            else
+                k_cg_true_residual<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, x_, L0.r, partials_,
+                                                                        counter_, sc_, cf);
             LHI_LAUNCH_CHECK();
         }
     }
@@ -2085,9 +2114,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_final() {
     auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
     k_x_to_pressure<T, TX><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(ncell_, x_, pressure_);
     LHI_LAUNCH_CHECK();
-    k_true_residual_final<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tile_k(L0, &sc_->tile_count[0], tile_grid_),
-                                                               sp_.update_region, rhs_, x_, partials_, counter_,
-                                                               &sc_->true2);
+    if constexpr (kHiResidual)
+        k_true_residual_final<double, TX><<<G, kTileThreads, 0, cur_>>>(
+            lk_hi(*this), tile_k(L0, &sc_->tile_count[0], tile_grid_), sp_.update_region, rhs_hi_, x_, partials_, counter_,
+            &sc_->true2);
+    else
+        k_true_residual_final<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tile_k(L0, &sc_->tile_count[0], tile_grid_),
+                                                                   sp_.update_region, rhs_, x_, partials_, counter_,
+                                                                   &sc_->true2);
     LHI_LAUNCH_CHECK();
 }
 

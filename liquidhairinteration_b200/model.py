@@ -454,13 +454,6 @@ class LiquidModel:
     def GetSolver(self):
         return self.m_solver
 
-    def Render(self):
-        """Headless: positions mapped to the GL clip cube as the reference's
-        vertex shader does (Shader/Scene3D_vertex.glsl)."""
-        pos = self.m_ps.GetPositions().astype(np.float32)
-        mn = np.array(self.grid.min_coord, np.float32)
-        mx = np.array(self.grid.max_coord, np.float32)
-        return (pos - mn) / (mx - mn) * np.float32(2.0) - np.float32(1.0)
 
     # -- extras
     def sort_particles(self):
