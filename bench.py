@@ -49,6 +49,25 @@ REFERENCE_PCG_ITERATIONS = 21
 # reference loop is linear in cells or particles and the small grid is
 # cache-resident, so the extrapolation favours the reference.
 REFERENCE_SAMPLE_N = 32
+PRECISION_TEXT = {
+    "mixed": "FP32 V-cycle and loop SpMV, FP64 x, dots, finest-level matrix and right-hand side for the true "
+             "residual every 10 iterations and the final check",
+    "fp64": "all FP64", "fp32": "all FP32"}
+
+
+def scene_text(spec):
+    parts = []
+    for p in spec.prims:
+        if p["kind"] == 0:
+            parts.append("block [%g,%g]x[%g,%g]x[%g,%g)" % (p["a"][0], p["b"][0], p["a"][1], p["b"][1], p["a"][2],
+                                                             p["b"][2]))
+        else:
+            parts.append("sphere r=%g at (%g,%g,%g)" % (p["b"][0], *p["a"]))
+    if spec.name == "dam256":
+        parts.append("two solid boxes")
+    return ", ".join(parts)
+
+
 # the grid inputs of a pressure solve, shared by the GPU and the oracle check
 GRID_INPUTS = ("vx", "vy", "vz", "liquidPhi", "liquidWx", "liquidWy", "liquidWz")
 
@@ -69,6 +88,8 @@ def parse():
     ap.add_argument("--no-oracle-check", action="store_true", help="skip error_vs_fp64_oracle")
     ap.add_argument("--ref-steps", type=int, default=1,
                     help="reference arm: full-size reference steps timed (each takes minutes)")
+    ap.add_argument("--ref-iterations", type=int, default=REFERENCE_PCG_ITERATIONS,
+                    help="reference arm: PCG iterations per step (our MGPCG's count on the workload)")
     return ap.parse_args()
 
 
@@ -332,11 +353,12 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else
             {"fp32": "f32", "fp64": "f64"}[args.precision], "data": "synthetic",
             "config": {
-                "workload": f"{spec.name}: {spec.n}^3 unit-cube dam break, block [0,0.35]x[0,0.7]x[0,1), two solid "
-                            f"boxes, {n_particles} particles (8 per cell, seed {spec.seed}), dt 1/960, one replica per GPU",
-                "solver": "MGPCG: 5 levels, 2+2 red-black damped Gauss-Seidel (w=1), 20 coarsest sweeps, flexible "
-                          "CG on every fluid cell, FP32 V-cycle, FP64 x/dots/true residual every 10, "
-                          "||r||/||b|| <= 1e-6 on the true residual",
+                "workload": f"{spec.name}: {spec.n}^3 unit-cube dam break ({scene_text(spec)}), {n_particles} "
+                            f"particles (8 per cell, seed {spec.seed}), dt {spec.dt:.6g}, one replica per GPU",
+                "solver": f"MGPCG: {solver.num_level} levels, {solver.num_pre_smooth}+{solver.num_post_smooth} "
+                          f"red-black damped Gauss-Seidel (w=1), {solver.num_final_smooth} coarsest sweeps, flexible "
+                          "CG on every fluid cell, " + PRECISION_TEXT[args.precision] +
+                          ", ||r||/||b|| <= 1e-6 on the true residual",
                 "precision": args.precision,
                 "l2": "inputs larger than L2 (grid fields ~1.2 GB, particles ~1.9 GB)",
                 "parallelism": f"replicas x{world}",
@@ -447,8 +469,8 @@ def oracle_check(model, spec):
 def reference_model(po, spec, iterations):
     """The reference's LiquidModel<3> on the scene (Scene<3> built from the
     reference JSON schema), PCG capped at ``iterations``."""
-    solver = spec.solver_params(robust=False, max_iterations=iterations, tolerance=1e-30,
-                                num_level=5, num_pre_smooth=2, num_post_smooth=2, num_final_smooth=20)
+    # the scene's own MG settings (levels, sweeps) with the reference's solver semantics
+    solver = spec.solver_params(robust=False, max_iterations=iterations, tolerance=1e-30)
     ref = po.Reference(spec.config_json(solver))
     ref.set_boundary(spec.boundary)
     return ref
@@ -463,14 +485,14 @@ def scaled_scene(n):
     return small
 
 
-def reference_stepper(po, spec):
+def reference_stepper(po, spec, iterations=REFERENCE_PCG_ITERATIONS):
     """A function that times one reference PreStep + Step on the scene and
     returns seconds, and the particle count.  Each timed step restarts from
     the seeded state so the reference's own (non-converging) PCG cannot
     accumulate NaN from step to step."""
     import numpy as np
     pos, vel = po.seed_scene(spec, "fp32")
-    ref = reference_model(po, spec, REFERENCE_PCG_ITERATIONS)
+    ref = reference_model(po, spec, iterations)
     dt = np.float32(spec.dt)
 
     def step():
@@ -533,14 +555,14 @@ def run_reference(args):
     t0 = time.perf_counter()
     threads, calib = fastest_reference_threads(po, spec)
     po.set_reference_threads(threads)
-    step, npart = reference_stepper(po, spec)
+    step, npart = reference_stepper(po, spec, args.ref_iterations)
     setup_s = time.perf_counter() - t0
     k = max(1, args.ref_steps)
     secs = [step() for _ in range(k)]
     ms = sum(secs) / len(secs) * 1e3
     sample = (f"reference LiquidModel<3>::PreStep+Step (its own sources, OpenMP, {threads} threads: the fastest of a "
               f"32^3 calibration) on the full {spec.n}^3 scene, {npart} particles, PCG capped at "
-              f"{REFERENCE_PCG_ITERATIONS} iterations (the GPU's count; the reference's own PCG does not converge on "
+              f"{args.ref_iterations} iterations (the GPU's count; the reference's own PCG does not converge on "
               f"this scene), {k} step(s) timed, no warm-up step (each takes minutes)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(ms, 1), "unit": UNIT, "n_gpus": world,

@@ -59,7 +59,7 @@ struct SolveScalars {
     int true_now;     // this iteration recomputes r = b - A x
     int tile_count[kMaxLevels];
     int timeout;      // a bounded wait on a shared-memory staging copy gave up
-    int pad_i[1];
+    int p2g_overflow;  // P2G: particles outside the cell they were sorted into (listed for a second kernel)
 };
 
 // Active-tile set of one level: 8 x 8 x 32-cell tiles (x, y, z) holding a

@@ -319,14 +319,17 @@ __host__ __device__ constexpr int p2g_region(int a) {
 }
 
 // Staged particle record of the P2G warp loop (values of T):
-//   [0, 12)   face weights wf[axis][4], window slots -1..2 (node = cell + slot)
-//   [12, 21)  centre weights wc[axis][3], slots -1..1 (node centre = cell + slot + 0.5)
-//   [21, 33)  tf[a][4] = C_aa * (x_a - face node a)          (component a, its own axis)
-//   [33, 51)  tc[a][j][3] = C_ab * (x_b - centre node b), b the j-th other axis of a
-//   [51, 54)  v
-//   [54]      z offset of the particle's cell in its row (bits of an int), -1: skip
+//   [0, 12)   wf[a][4]: face weights of component a along its own axis,
+//             window slots -1..2 (node = cell + slot)
+//   [12, 24)  tf[a][4] = C_aa * (x_a - face node a)
+//   [24, 51)  W[l], column l = 9a + 3s + t of the warp loop: the product of
+//             the two cell-centre weights across component a (slot s on its
+//             first other axis, t on the second; node centre = cell + slot + 0.5)
+//   [51, 78)  B[l] = v_a + C_ab (x_b - centre b) + C_ac (x_c - centre c)
+//   [78]      z offset of the particle's cell in its row (bits of an int)
 // A weight outside the reference's window (+-d) or with |e| >= 1.5 is 0.
-constexpr int kP2GRec = 55;
+// The stride is odd, so the staging lanes' stores fall in distinct banks.
+constexpr int kP2GRec = 79;
 constexpr int kP2GWarps = 8;
 
 __device__ __forceinline__ void p2g_other_axes(int a, int& b, int& c) {
@@ -334,20 +337,16 @@ __device__ __forceinline__ void p2g_other_axes(int a, int& b, int& c) {
     c = (a == 2) ? 1 : 2;
 }
 
-// Computes the record of one particle (one lane per particle).  Returns the
-// z offset of its cell in the row, or -1 when its own truncated index
+// Computes the record of one particle (one lane per particle) and returns
+// the z offset of its cell in the row, or -1 when its own truncated index
 // (cast<Integer>, LiquidModel.cpp:629) is not the cell it was sorted into
-// (outside the grid, where the sort key is clamped): then its window goes
-// straight to global memory here, component by component.
+// (outside the grid, where the sort key is clamped): such a particle is
+// listed for k_p2g_overflow instead.
 template <class T>
-__device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __restrict__ pd, long long cap, long long p,
-                         int rx, int ry, int z0, int zend, T* rec, T* __restrict__ gw0, T* __restrict__ gv0,
-                         T* __restrict__ gw1, T* __restrict__ gv1, T* __restrict__ gw2, T* __restrict__ gv2) {
+__device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __restrict__ pd, long long cap,
+                         long long p, int rx, int ry, int z0, int zend, T* rec, int* __restrict__ ov_count,
+                         int32_t* __restrict__ ov_list) {
     const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
-    const T v[3] = {pd[3 * cap + p], pd[4 * cap + p], pd[5 * cap + p]};
-    T C[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) C[k] = pd[(6 + k) * cap + p];  // column-major: C[3a + i] = C(i, a)
     T g3[3];
     int ci[3];
 #pragma unroll
@@ -356,44 +355,58 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __r
         ci[i] = int(g3[i]);                                     // cast<Integer>
     }
     if (ci[0] != rx || ci[1] != ry || ci[2] < z0 || ci[2] >= zend) {
-        const int d[3] = {d0, d1, d2};
-        p2g_particle_global<T, 0>(g, d, q, g3, v[0], C[0], C[1], C[2], gw0, gv0);
-        p2g_particle_global<T, 1>(g, d, q, g3, v[1], C[3], C[4], C[5], gw1, gv1);
-        p2g_particle_global<T, 2>(g, d, q, g3, v[2], C[6], C[7], C[8], gw2, gv2);
+        ov_list[atomicAdd(ov_count, 1)] = int32_t(p);
         return -1;
     }
+    T C[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) C[k] = pd[(6 + k) * cap + p];  // column-major: C[3a + i] = C(i, a)
+    T wc[3][3], tc[3][2][3];  // centre weights per axis; C_ab (x_b - centre) per component and other axis
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const int di = (i == 0) ? d0 : (i == 1) ? d1 : d2;
+        const T cb = T(ci[i]);  // integer grid coordinates are exact in T
 #pragma unroll
         for (int s2 = 0; s2 < 4; ++s2) {  // face nodes: component i's own axis
             const int o = s2 - 1;
-            const T c = T(ci[i] + o);
+            const T c = X<T>::add(cb, T(o));
             const T e = X<T>::sub(g3[i], c);
             const bool ok = o >= -di && o <= di && !(fabs(e) >= T(1.5f));
             rec[i * 4 + s2] = ok ? qweight(e) : T(0);
             const T df = X<T>::sub(q[i], X<T>::add(X<T>::mul(c, g.dx[i]), g.mn[i]));
-            rec[21 + i * 4 + s2] = X<T>::mul(C[4 * i], df);  // C(i, i)
+            rec[12 + i * 4 + s2] = X<T>::mul(C[4 * i], df);  // C(i, i)
         }
 #pragma unroll
         for (int s2 = 0; s2 < 3; ++s2) {  // cell-centre nodes: the other two components
             const int o = s2 - 1;
-            const T c = X<T>::add(T(ci[i] + o), T(0.5));
+            const T c = X<T>::add(X<T>::add(cb, T(o)), T(0.5));
             const T e = X<T>::sub(g3[i], c);
             const bool ok = o >= -di && o <= di && !(fabs(e) >= T(1.5f));
-            rec[12 + i * 3 + s2] = ok ? qweight(e) : T(0);
+            wc[i][s2] = ok ? qweight(e) : T(0);
             const T dc = X<T>::sub(q[i], X<T>::add(X<T>::mul(c, g.dx[i]), g.mn[i]));
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 if (a == i) continue;
                 int b, c2;
                 p2g_other_axes(a, b, c2);
-                rec[33 + a * 6 + (b == i ? 0 : 3) + s2] = X<T>::mul(C[3 * a + i], dc);
+                tc[a][b == i ? 0 : 1][s2] = X<T>::mul(C[3 * a + i], dc);
             }
         }
     }
 #pragma unroll
-    for (int a = 0; a < 3; ++a) rec[51 + a] = v[a];
+    for (int a = 0; a < 3; ++a) {
+        int b, c;
+        p2g_other_axes(a, b, c);
+        const T va = pd[(3 + a) * cap + p];
+#pragma unroll
+        for (int s2 = 0; s2 < 3; ++s2)
+#pragma unroll
+            for (int t2 = 0; t2 < 3; ++t2) {
+                const int l = 9 * a + 3 * s2 + t2;
+                rec[24 + l] = wc[b][s2] * wc[c][t2];
+                rec[51 + l] = va + tc[a][0][s2] + tc[a][1][t2];
+            }
+    }
     return ci[2] - z0;
 }
 
@@ -403,7 +416,8 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __r
 // the tile: the particles of a row are contiguous in the sorted order.  The
 // row's particles are staged 32 at a time (one lane per particle computes
 // its per-axis weights and C.(x_p - x_node) terms once, for all three
-// components), then the warp walks them in order: lane l < 27 owns one
+// components, and the per-column products below), then the warp walks them
+// in order, two at a time while they share a cell: lane l < 27 owns one
 // column of 4 window nodes of one component (component l / 9, along that
 // component's own axis; the 3 x 3 columns across it) and sums the weights
 // and APIC values of the current cell's particles in registers.  When the
@@ -416,7 +430,8 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __r
 template <class T>
 __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_t* __restrict__ cs,
                                                         const T* __restrict__ pd, long long cap, int d0, int d1,
-                                                        int d2, P2GOut<T> out) {
+                                                        int d2, P2GOut<T> out, int* __restrict__ ov_count,
+                                                        int32_t* __restrict__ ov_list) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
     __shared__ int any;
@@ -444,16 +459,18 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
     int b = 0, c = 0;
     p2g_other_axes(a < 3 ? a : 0, b, c);
     const bool col = lane < 27;
-    const int ey = kTile + 2 + (a == 1), ez = kTile + 2 + (a == 2);
-    const int astride = (a == 0) ? ey * ez : (a == 1) ? ez : 1;
+    const int ac = col ? a : 0;
+    const int ey = kTile + 2 + (ac == 1), ez = kTile + 2 + (ac == 2);
+    const int astride = (ac == 0) ? ey * ez : (ac == 1) ? ez : 1;
     // the column's first node relative to its cell, per axis (slot - 1, plus 1 for the halo): face slot 0
     // along a, centre slot s along b, t along c (b < c)
-    const int ox = (a == 0) ? 0 : s;
-    const int oy = (a == 1) ? 0 : (b == 1 ? s : t);
-    const int oz = (a == 2) ? 0 : t;
+    const int ox = (ac == 0) ? 0 : s;
+    const int oy = (ac == 1) ? 0 : (b == 1 ? s : t);
+    const int oz = (ac == 2) ? 0 : t;
     // component a's weight and value accumulators: [w_0 | v_0 | w_1 | v_1 | w_2 | v_2]
-    T* aw_s = acc + ((a == 1) ? 2 * R0 : (a == 2) ? 2 * (R0 + R1) : 0);
-    T* av_s = aw_s + ((a == 1) ? R1 : (a == 2) ? R2 : R0);
+    T* aw_s = acc + ((ac == 1) ? 2 * R0 : (ac == 2) ? 2 * (R0 + R1) : 0);
+    T* av_s = aw_s + ((ac == 1) ? R1 : (ac == 2) ? R2 : R0);
+    const int lw = col ? lane : 0;  // record offsets of this lane's column
     for (int row = warp; row < kTile * kTile; row += kP2GWarps) {
         const int rx = x0 + (row >> 3), ry = y0 + (row & 7);
         if (rx >= g.nx || ry >= g.ny) continue;
@@ -474,33 +491,50 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
                 av[k] = T(0);
             }
         };
+        auto add = [&](const T* r) {
+            const T W = r[24 + lw], B = r[51 + lw];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const T w = W * r[ac * 4 + k];
+                aw[k] += w;
+                av[k] = fma(w, B + r[12 + ac * 4 + k], av[k]);
+            }
+        };
         for (int chunk = pbeg; chunk < pend; chunk += 32) {
             const int n = min(32, pend - chunk);
             __syncwarp();
             if (lane < n) {
-                const int zo = p2g_stage<T>(g, d0, d1, d2, pd, cap, chunk + lane, rx, ry, z0, zend, stage + lane * kP2GRec,
-                                            out.w[0], out.v[0], out.w[1], out.v[1], out.w[2], out.v[2]);
-                stage[lane * kP2GRec + 54] = T(0);
-                reinterpret_cast<int*>(stage + lane * kP2GRec + 54)[0] = zo;
+                T* rec = stage + lane * kP2GRec;
+                const int zo = p2g_stage<T>(g, d0, d1, d2, pd, cap, chunk + lane, rx, ry, z0, zend, rec, ov_count,
+                                            ov_list);
+                rec[78] = T(0);
+                reinterpret_cast<int*>(rec + 78)[0] = zo;
             }
             __syncwarp();
-            for (int j = 0; j < n; ++j) {
-                const T* r = stage + j * kP2GRec;
-                const int zo = reinterpret_cast<const int*>(r + 54)[0];
-                if (zo < 0) continue;
-                if (zo != cur) {
-                    flush();
-                    cur = zo;
+            int j = 0;
+            while (j < n) {
+                const T* r0 = stage + j * kP2GRec;
+                const int zo0 = reinterpret_cast<const int*>(r0 + 78)[0];
+                if (j + 1 < n) {
+                    const T* r1 = r0 + kP2GRec;
+                    const int zo1 = reinterpret_cast<const int*>(r1 + 78)[0];
+                    if (zo0 == cur && zo1 == cur) {  // both in the current cell
+                        if (col) {
+                            add(r0);
+                            add(r1);
+                        }
+                        j += 2;
+                        continue;
+                    }
                 }
-                if (!col) continue;
-                const T wbc = r[12 + b * 3 + s] * r[12 + c * 3 + t];
-                const T base = r[51 + a] + r[33 + a * 6 + s] + r[33 + a * 6 + 3 + t];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const T w = wbc * r[a * 4 + k];
-                    aw[k] += w;
-                    av[k] = fma(w, base + r[21 + a * 4 + k], av[k]);
+                if (zo0 >= 0) {
+                    if (zo0 != cur) {
+                        flush();
+                        cur = zo0;
+                    }
+                    if (col) add(r0);
                 }
+                ++j;
             }
         }
         flush();
@@ -525,6 +559,28 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
             atomicAdd(&out.w[a2][gi], wv);
             atomicAdd(&out.v[a2][gi], vv);
         }
+    }
+}
+
+// The particles k_p2g listed (outside the cell they were sorted into: off
+// the grid) add their windows straight to global memory.
+template <class T>
+__global__ void k_p2g_overflow(GridP<T> g, const T* __restrict__ pd, long long cap, int d0, int d1, int d2,
+                               P2GOut<T> out, const int* __restrict__ ov_count, const int32_t* __restrict__ ov_list) {
+    const int n = *ov_count;
+    const int d[3] = {d0, d1, d2};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const long long p = ov_list[i];
+        const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
+        T g3[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) g3[k] = X<T>::div(X<T>::sub(q[k], g.mn[k]), g.dx[k]);
+        T C[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) C[k] = pd[(6 + k) * cap + p];
+        p2g_particle_global<T, 0>(g, d, q, g3, pd[3 * cap + p], C[0], C[1], C[2], out.w[0], out.v[0]);
+        p2g_particle_global<T, 1>(g, d, q, g3, pd[4 * cap + p], C[3], C[4], C[5], out.w[1], out.v[1]);
+        p2g_particle_global<T, 2>(g, d, q, g3, pd[5 * cap + p], C[6], C[7], C[8], out.w[2], out.v[2]);
     }
 }
 
@@ -1059,8 +1115,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
     LHI_CUDA(cudaFuncSetAttribute(k_p2g<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid(unsigned((nz_ + kTile - 1) / kTile), unsigned((ny_ + kTile - 1) / kTile),
               unsigned((nx_ + kTile - 1) / kTile));
+    // particles off the grid are listed (in vals_[1], free after the sort) for k_p2g_overflow
+    int* ov_count = &sc_->p2g_overflow;
+    LHI_CUDA(cudaMemsetAsync(ov_count, 0, sizeof(int), stream_));
     k_p2g<T><<<grid, kP2GWarps * 32, smem, stream_>>>(gridp(*this), cell_start_, pdata_[pcur_], pcap_, d0, d1, d2,
-                                                       out);
+                                                       out, ov_count, vals_[1]);
+    LHI_LAUNCH_CHECK();
+    k_p2g_overflow<T><<<kSMs, 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, d0, d1, d2, out, ov_count,
+                                                 vals_[1]);
     LHI_LAUNCH_CHECK();
 }
 
