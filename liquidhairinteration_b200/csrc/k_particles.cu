@@ -705,11 +705,19 @@ template <class T> __device__ void solid_grad_at(const GridP<T>& g, const T* sp,
 // v = sum wX A, C = (sum gX A, sum wX B, sum wX D) -- with fused
 // multiply-adds: about a third of the arithmetic, the same value up to
 // rounding.
+// Where a gather reads the face velocities of one component: the global
+// array (origin 0, the face grid's extents) or a tile's staged copy in
+// shared memory (origin one node before the tile, the region's extents).
+template <class T> struct VSrc {
+    const T* v;
+    int ox, oy, oz;
+    long long fy, fz;
+};
+
 template <class T, int A, bool FACTORED>
 __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3], const T g3[3], const int ci[3],
-                                              const T* __restrict__ vf, T& velA, T col[3]) {
+                                              const VSrc<T> vs, T& velA, T col[3]) {
     const int hmax[3] = {g.nx - 1 + (A == 0), g.ny - 1 + (A == 1), g.nz - 1 + (A == 2)};
-    const long long fy = g.ny + (A == 1), fz = g.nz + (A == 2);
     T ew[3][3], eg[3][3];
     int first[3], cnt[3];
 #pragma unroll
@@ -746,7 +754,8 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
 #pragma unroll
             for (int jy = 0; jy < 3; ++jy) {
                 if (jy >= cnt[1]) break;
-                const T* row = vf + ((long long)(first[0] + jx) * fy + (first[1] + jy)) * fz + first[2];
+                const T* row = vs.v + ((long long)(first[0] + jx - vs.ox) * vs.fy + (first[1] + jy - vs.oy)) * vs.fz +
+                               (first[2] - vs.oz);
                 T s = T(0), t = T(0);
 #pragma unroll
                 for (int jz = 0; jz < 3; ++jz) {
@@ -774,7 +783,8 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
             if (jy >= cnt[1]) break;
             const T wY = ew[1][jy], gY = eg[1][jy];
             const T wXY = X<T>::mul(wX, wY), gXwY = X<T>::mul(gX, wY), wXgY = X<T>::mul(wX, gY);
-            const T* row = vf + ((long long)(first[0] + jx) * fy + (first[1] + jy)) * fz + first[2];
+            const T* row = vs.v + ((long long)(first[0] + jx - vs.ox) * vs.fy + (first[1] + jy - vs.oy)) * vs.fz +
+                               (first[2] - vs.oz);
 #pragma unroll
             for (int jz = 0; jz < 3; ++jz) {
                 if (jz >= cnt[2]) break;
@@ -794,20 +804,19 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
     }
 }
 
-// LiquidModel<3>::Grid2Particle (LiquidModel.cpp:724-823) fused with
-// AdvectParticle (LiquidModel.cpp:913-935) and the next step's cell key.
-template <class T, bool FACTORED>
-__global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, long long cap, long long n, int d0,
-                                             int d1, int d2, const T* __restrict__ vx, const T* __restrict__ vy,
-                                             const T* __restrict__ vz, int do_g2p, int do_advect, T dt,
+// One particle of LiquidModel<3>::Grid2Particle (LiquidModel.cpp:724-823)
+// fused with AdvectParticle (LiquidModel.cpp:913-935) and the next step's
+// cell key.  The face velocities come from the sources the caller picks
+// for the particle's truncated cell ci (staged in shared memory when ci lies
+// in the tile, global memory otherwise).
+template <class T, bool FACTORED, class PickSrc>
+__device__ __forceinline__ void g2p_particle(const GridP<T>& g, T* __restrict__ pd, long long cap, long long i,
+                                             const int d[3], int do_g2p, int do_advect, T dt,
                                              const T* __restrict__ sp, uint32_t* __restrict__ keys,
-                                             int32_t* __restrict__ vals) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+                                             int32_t* __restrict__ vals, PickSrc pick) {
     T q[3] = {pd[i], pd[cap + i], pd[2 * cap + i]};
     T vel[3];
     if (do_g2p) {
-        const int d[3] = {d0, d1, d2};
         T g3[3];
         int ci[3];
 #pragma unroll
@@ -819,9 +828,11 @@ __global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, lon
         vel[0] = vel[1] = vel[2] = T(0);
 #pragma unroll
         for (int k = 0; k < 9; ++k) C[k] = T(0);
-        g2p_component<T, 0, FACTORED>(g, d, g3, ci, vx, vel[0], &C[0]);
-        g2p_component<T, 1, FACTORED>(g, d, g3, ci, vy, vel[1], &C[3]);
-        g2p_component<T, 2, FACTORED>(g, d, g3, ci, vz, vel[2], &C[6]);
+        VSrc<T> src[3];
+        pick(ci, src);
+        g2p_component<T, 0, FACTORED>(g, d, g3, ci, src[0], vel[0], &C[0]);
+        g2p_component<T, 1, FACTORED>(g, d, g3, ci, src[1], vel[1], &C[3]);
+        g2p_component<T, 2, FACTORED>(g, d, g3, ci, src[2], vel[2], &C[6]);
 #pragma unroll
         for (int k = 0; k < 3; ++k) pd[(3 + k) * cap + i] = vel[k];
 #pragma unroll
@@ -845,6 +856,105 @@ __global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, lon
         for (int k = 0; k < 3; ++k) pd[k * cap + i] = q[k];
         keys[i] = cell_key(g, q[0], q[1], q[2]);
         vals[i] = int32_t(i);
+    }
+}
+
+template <class T> __device__ __forceinline__ void global_sources(const GridP<T>& g, const T* vx, const T* vy,
+                                                                  const T* vz, VSrc<T> src[3]) {
+    src[0] = VSrc<T>{vx, 0, 0, 0, g.ny, g.nz};
+    src[1] = VSrc<T>{vy, 0, 0, 0, g.ny + 1, g.nz};
+    src[2] = VSrc<T>{vz, 0, 0, 0, g.ny, g.nz + 1};
+}
+
+// One thread per particle, face velocities from global memory (the
+// advection alone, and any particle order).
+template <class T, bool FACTORED>
+__global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, long long cap, long long n, int d0,
+                                             int d1, int d2, const T* __restrict__ vx, const T* __restrict__ vy,
+                                             const T* __restrict__ vz, int do_g2p, int do_advect, T dt,
+                                             const T* __restrict__ sp, uint32_t* __restrict__ keys,
+                                             int32_t* __restrict__ vals) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int d[3] = {d0, d1, d2};
+    g2p_particle<T, FACTORED>(g, pd, cap, i, d, do_g2p, do_advect, dt, sp, keys, vals,
+                              [&](const int*, VSrc<T> src[3]) { global_sources(g, vx, vy, vz, src); });
+}
+
+// G2P + advection over the cell-sorted particles, one CTA per 8^3-cell tile:
+// the tile's window region of each face component (the P2G region) is
+// staged once in shared memory with coalesced loads, then every particle of
+// the tile's 64 rows gathers from it.  The gather arithmetic is that of
+// k_g2p (bit-identical in FP32 / FP64, the factored sums in mixed precision).
+template <class T, bool FACTORED>
+__global__ void __launch_bounds__(256, 3) k_g2p_tile(GridP<T> g, T* __restrict__ pd, long long cap,
+                                                  const int32_t* __restrict__ cs, int d0, int d1, int d2,
+                                                  const T* __restrict__ vx, const T* __restrict__ vy,
+                                                  const T* __restrict__ vz, T dt, const T* __restrict__ sp,
+                                                  uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sv = reinterpret_cast<T*>(smem_raw);
+    __shared__ int roff[kTile * kTile + 1];
+    __shared__ int rbeg[kTile * kTile];
+    const int x0 = blockIdx.z * kTile, y0 = blockIdx.y * kTile, z0 = blockIdx.x * kTile;
+    const int zend = min(z0 + kTile, g.nz);
+    if (threadIdx.x < kTile * kTile) {
+        const int rx = x0 + (threadIdx.x >> 3), ry = y0 + (threadIdx.x & 7);
+        int cnt = 0, beg = 0;
+        if (rx < g.nx && ry < g.ny) {
+            const long long c = ((long long)rx * g.ny + ry) * g.nz + z0;
+            beg = cs[c];
+            cnt = cs[c + (zend - z0)] - beg;
+        }
+        rbeg[threadIdx.x] = beg;
+        roff[threadIdx.x + 1] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        roff[0] = 0;
+        for (int r = 0; r < kTile * kTile; ++r) roff[r + 1] += roff[r];
+    }
+    __syncthreads();
+    const int total = roff[kTile * kTile];
+    if (total == 0) return;
+    const int R0 = p2g_region(0), R1 = p2g_region(1);
+    const T* vsrc[3] = {vx, vy, vz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int ey = kTile + 2 + (a == 1), ez = kTile + 2 + (a == 2);
+        const int R = p2g_region(a);
+        T* dst = sv + ((a == 1) ? R0 : (a == 2) ? R0 + R1 : 0);
+        const int fy = g.ny + (a == 1), fz = g.nz + (a == 2), fx = g.nx + (a == 0);
+        for (int e = threadIdx.x; e < R; e += blockDim.x) {
+            const int lz = e % ez, ly = (e / ez) % ey, lx = e / (ey * ez);
+            const int xi = x0 - 1 + lx, yi = y0 - 1 + ly, zi = z0 - 1 + lz;
+            T v = T(0);
+            if (xi >= 0 && xi < fx && yi >= 0 && yi < fy && zi >= 0 && zi < fz)
+                v = vsrc[a][((long long)xi * fy + yi) * fz + zi];
+            dst[e] = v;
+        }
+    }
+    __syncthreads();
+    const int d[3] = {d0, d1, d2};
+    for (int f = threadIdx.x; f < total; f += blockDim.x) {
+        int lo = 0, hi = kTile * kTile;  // the row r with roff[r] <= f < roff[r + 1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (roff[mid] <= f) lo = mid;
+            else hi = mid;
+        }
+        const long long i = rbeg[lo] + (f - roff[lo]);
+        g2p_particle<T, FACTORED>(g, pd, cap, i, d, 1, 1, dt, sp, keys, vals, [&](const int* ci, VSrc<T> src[3]) {
+            const bool in = ci[0] >= x0 && ci[0] < x0 + kTile && ci[1] >= y0 && ci[1] < y0 + kTile && ci[2] >= z0 &&
+                            ci[2] < zend;
+            if (!in) {  // off the grid: sorted into a clamped cell
+                global_sources(g, vx, vy, vz, src);
+                return;
+            }
+            src[0] = VSrc<T>{sv, x0 - 1, y0 - 1, z0 - 1, kTile + 2, kTile + 2};
+            src[1] = VSrc<T>{sv + R0, x0 - 1, y0 - 1, z0 - 1, kTile + 3, kTile + 2};
+            src[2] = VSrc<T>{sv + R0 + R1, x0 - 1, y0 - 1, z0 - 1, kTile + 2, kTile + 3};
+        });
     }
 }
 
@@ -1168,9 +1278,21 @@ template <class T, class TX> void LiquidImpl<T, TX>::g2p(bool do_advect, T dt) {
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
     auto ps_ = scope(LHI_KERNEL_G2P);
     // mixed precision takes the factored sums; FP32 and FP64 keep the reference's order bit for bit
-    auto kern = precision_ == LHI_PRECISION_MIXED ? k_g2p<T, true> : k_g2p<T, false>;
-    kern<<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0], v_[1],
-                                                    v_[2], 1, do_advect ? 1 : 0, dt, solid_phi_, keys_[0], vals_[0]);
+    const bool fact = precision_ == LHI_PRECISION_MIXED;
+    if (do_advect) {
+        // over the cell-sorted particles, tile by tile, with the face velocities staged in shared memory
+        ensure_sorted();
+        const size_t smem = sizeof(T) * size_t(p2g_region(0) + p2g_region(1) + p2g_region(2));
+        dim3 grid(unsigned((nz_ + kTile - 1) / kTile), unsigned((ny_ + kTile - 1) / kTile),
+                  unsigned((nx_ + kTile - 1) / kTile));
+        auto kern = fact ? k_g2p_tile<T, true> : k_g2p_tile<T, false>;
+        kern<<<grid, 256, smem, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, cell_start_, d0, d1, d2, v_[0], v_[1],
+                                           v_[2], dt, solid_phi_, keys_[0], vals_[0]);
+    } else {
+        auto kern = fact ? k_g2p<T, true> : k_g2p<T, false>;
+        kern<<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
+                                                        v_[1], v_[2], 1, 0, dt, solid_phi_, keys_[0], vals_[0]);
+    }
     LHI_LAUNCH_CHECK();
     if (do_advect) {
         sorted_ = false;
