@@ -174,6 +174,20 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
                                                     const uint8_t* __restrict__ occ, int ox, int oy, int oz,
                                                     const T* __restrict__ pd, long long cap, T radius, int d0, int d1,
                                                     int d2, T* __restrict__ phi) {
+    // lower bound of |x_c - x_p| - r over the particles of a window cell at
+    // offset (ax, ay, az) from c, with a safety margin: every point of that
+    // cell's box is at least the box distance from the centre
+    __shared__ double s_lb[9 * 9 * 9];
+    const int nb = (d0 + 1) * (d1 + 1) * (d2 + 1);
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+        const int az = e % (d2 + 1), ay = (e / (d2 + 1)) % (d1 + 1), ax = e / ((d1 + 1) * (d2 + 1));
+        T lx = T(fmax(double(ax) - 0.5, 0.0)) * g.dx[0];
+        T ly = T(fmax(double(ay) - 0.5, 0.0)) * g.dx[1];
+        T lz = T(fmax(double(az) - 0.5, 0.0)) * g.dx[2];
+        s_lb[e] = sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
+                  double(radius) * (1.0 + 1e-6);
+    }
+    __syncthreads();
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long nc = (long long)g.nx * g.ny * g.nz;
     if (c >= nc) return;
@@ -204,18 +218,13 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
     // bound holds for particles clamped into an outer-layer cell too: they
     // lie beyond it).
     auto visit = [&](int wx, int wy, int wz, bool prune) {
+        if (prune) {  // the bound needs no memory access but the table: test it first
+            const int ax = abs(wx - cx), ay = abs(wy - cy), az = abs(wz - cz);
+            if (double(cur) < s_lb[(ax * (d1 + 1) + ay) * (d2 + 1) + az]) return;
+        }
         const long long w = ((long long)wx * g.ny + wy) * g.nz + wz;
         const int s = cs[w], e = cs[w + 1];
         if (s == e) return;
-        if (prune) {
-            const int ax = abs(wx - cx), ay = abs(wy - cy), az = abs(wz - cz);
-            T lx = T(fmax(double(ax) - 0.5, 0.0)) * g.dx[0];
-            T ly = T(fmax(double(ay) - 0.5, 0.0)) * g.dx[1];
-            T lz = T(fmax(double(az) - 0.5, 0.0)) * g.dx[2];
-            double lb = sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
-                        double(radius) * (1.0 + 1e-6);
-            if (double(cur) < lb) return;
-        }
         // the particles of a cell off the grid's outer layer were sorted
         // into it by their own unclamped Point2Index: all inside the window
         const bool own = wx > 0 && wx < g.nx - 1 && wy > 0 && wy < g.ny - 1 && wz > 0 && wz < g.nz - 1;
