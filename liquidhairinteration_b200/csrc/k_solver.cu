@@ -196,6 +196,10 @@ __global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)g.nx * g.ny * g.nz;
     if (i >= n) return;
+    // the FP64 copy is read only on rows with phi <= 0 (and their fluid
+    // neighbours): air cells need no entries
+    if constexpr (!std::is_same<T, TI>::value)
+        if (T(phi[i]) > T(0)) return;
     int x, y, z;
     decode(i, g.ny, g.nz, x, y, z);
     const long long sy = g.nz, sx = (long long)g.ny * g.nz;
@@ -255,6 +259,8 @@ __global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const TI* 
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)nx * ny * nz;
     if (i >= n) return;
+    if constexpr (!std::is_same<T, TI>::value)  // the FP64 copy is read only where phi <= 0
+        if (T(phi[i]) > T(0)) return;
     T b = T(0);
     if (!(T(phi[i]) > T(0))) {
         int x, y, z;
