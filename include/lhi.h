@@ -89,6 +89,17 @@ extern "C" {
    the same values. */
 #define LHI_SWEEP_FUSED 0
 #define LHI_SWEEP_SPLIT 1
+/* Coarse multigrid operators: the reference's re-discretisation from the
+   level's approximated liquid SDF and face fractions (BuildLHS,
+   PressureSolver.cpp:544-664), or the Galerkin operator of the finer level
+   under the V-cycle's own transfers: A_c = P^T A P / 8 with P the constant
+   injection (Prolong, :774-794), so the coarse correction of the averaging
+   restriction (Restrict, :796-819) is the A-orthogonal projection.  The
+   Galerkin levels stay consistent with the finest level where thin solids
+   make the re-discretised ones disagree with it (the V-cycle then stops
+   being a usable preconditioner); no counterpart in the reference. */
+#define LHI_COARSE_REFERENCE 0
+#define LHI_COARSE_GALERKIN 1
 
 typedef struct lhi_grid_desc {
     int32_t dim[3];        /* gridDimension (SceneParameter.h:137)          */
@@ -121,6 +132,7 @@ typedef struct lhi_solver_params {   /* SolverParameter<3> (SceneParameter.h:10-
                                         with a conditional while node          */
     int32_t sweep_kernel;            /* LHI_SWEEP_* (0 = fused where the level
                                         allows it)                             */
+    int32_t coarse_operator;         /* LHI_COARSE_* (0 = reference)           */
 } lhi_solver_params;
 
 typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> */

@@ -248,6 +248,67 @@ __global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI
     diag[i] = d;
 }
 
+// Galerkin coarse level (LHI_COARSE_GALERKIN): A_c = P^T A P / 8 of the
+// finer level f under the V-cycle's transfers (constant injection P, the
+// 1/8 averaging restriction), with A_ij = [type_i >= 1][type_j == 2] c_ij as
+// every kernel of the solver applies it.  Coarse cell I takes its 8
+// children's diagonals and the couplings between them; the coupling of I
+// with its +x / +y / +z neighbour is the sum over the 4 child pairs across
+// that face.  type_I = 2 if a child is fluid, else 1 if a child has phi = 0.
+template <class T>
+__global__ void k_level_galerkin(LevelK<T> F, int cnx, int cny, int cnz, T* __restrict__ diag, T* __restrict__ cx,
+                                 T* __restrict__ cy, T* __restrict__ cz, uint8_t* __restrict__ type,
+                                 uint8_t* __restrict__ tile_flag, int tdy, int tdz) {
+    long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long n = (long long)cnx * cny * cnz;
+    if (I >= n) return;
+    int X, Y, Z;
+    decode(I, cny, cnz, X, Y, Z);
+    const long long fsy = F.nz, fsx = (long long)F.ny * F.nz;
+    auto fi = [&](int x, int y, int z) -> long long { return ((long long)x * F.ny + y) * F.nz + z; };
+    // A_ij of fine cells i and its +axis neighbour j = i + step: rows couple to fluid columns only
+    auto a_ij = [&](long long i, long long j, T c) -> T {
+        return (F.type[i] >= 1 && F.type[j] == 2) ? c : T(0);
+    };
+    T d = T(0);
+    uint8_t t = 0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) {
+                const long long i = fi(2 * X + a, 2 * Y + b, 2 * Z + c);
+                const uint8_t ti = F.type[i];
+                t = (ti == 2 || t == 2) ? 2 : (ti == 1 ? uint8_t(1) : t);
+                if (ti >= 1) d += F.diag[i];
+                // couplings inside the coarse cell, both directions
+                if (a == 0) d += a_ij(i, i + fsx, F.cx[i]) + a_ij(i + fsx, i, F.cx[i]);
+                if (b == 0) d += a_ij(i, i + fsy, F.cy[i]) + a_ij(i + fsy, i, F.cy[i]);
+                if (c == 0) d += a_ij(i, i + 1, F.cz[i]) + a_ij(i + 1, i, F.cz[i]);
+            }
+    T ccx = T(0), ccy = T(0), ccz = T(0);
+    for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 2; ++v) {
+            if (X + 1 < cnx) {
+                const long long i = fi(2 * X + 1, 2 * Y + u, 2 * Z + v);
+                ccx += a_ij(i, i + fsx, F.cx[i]);
+            }
+            if (Y + 1 < cny) {
+                const long long i = fi(2 * X + u, 2 * Y + 1, 2 * Z + v);
+                ccy += a_ij(i, i + fsy, F.cy[i]);
+            }
+            if (Z + 1 < cnz) {
+                const long long i = fi(2 * X + u, 2 * Y + v, 2 * Z + 1);
+                ccz += a_ij(i, i + 1, F.cz[i]);
+            }
+        }
+    const T s = T(0.125);
+    diag[I] = d * s;
+    cx[I] = ccx * s;
+    cy[I] = ccy * s;
+    cz[I] = ccz * s;
+    type[I] = t;
+    if (t != 0) tile_flag[((long long)(X / kTileX) * tdy + Y / kTileY) * tdz + Z / kTileZ] = 1;
+}
+
 // CGSolver<3>::BuildRHS (PressureSolver.cpp:682-698)
 // (TI = float, T = double: the FP64 right-hand side of the mixed mode's
 // outer residual, from the same float fields)
@@ -1726,6 +1787,13 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
         if (L.n == 0) continue;
         LevelGeom g{L.nx, L.ny, L.nz, nx_, ny_, nz_, l};
         LHI_CUDA(cudaMemsetAsync(L.tile_flag, 0, size_t(L.ntiles), cur_));
+        if (l > 0 && sp_.coarse_operator == LHI_COARSE_GALERKIN) {
+            k_level_galerkin<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(lk(lv_[l - 1]), L.nx, L.ny, L.nz, L.diag,
+                                                                        L.cf[0], L.cf[1], L.cf[2], L.type,
+                                                                        L.tile_flag, L.tdim[1], L.tdim[2]);
+            LHI_LAUNCH_CHECK();
+            continue;
+        }
         k_level_phi<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(g, liquid_phi_, L.phi, L.type, L.tile_flag, L.tdim[1],
                                                               L.tdim[2]);
         LHI_LAUNCH_CHECK();

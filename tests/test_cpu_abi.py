@@ -37,11 +37,12 @@ def test_library_exports_every_declared_symbol(lhi):
 def test_abi_struct_layouts():
     # sizes of the POD structs in include/lhi.h (x86-64 System V)
     assert C.sizeof(abi.GridDesc) == 64
-    assert C.sizeof(abi.SolverParams) == 72
+    assert C.sizeof(abi.SolverParams) == 80
     assert C.sizeof(abi.LiquidParams) == 56
     assert C.sizeof(abi.SolveStats) == 40
     assert C.sizeof(abi.BoundaryNode) == 64
     assert C.sizeof(abi.FluidPrim) == 80
+    assert C.sizeof(abi.RenderParams) == 20
 
 
 def test_spawn_lattice_matches_liquiddata_frame0(lhi):
