@@ -27,8 +27,9 @@ from ._lib import call
 CANDIDATES = [(1, 512), (2, 512), (2, 4096), (3, 4096)]
 
 
-def build_scene(spec, precision, pre, coarse):
-    solver = spec.solver_params(num_pre_smooth=pre, num_post_smooth=pre, coarse_cells=coarse)
+def build_scene(spec, precision, pre, coarse, coarse_operator=abi.COARSE_GALERKIN):
+    solver = spec.solver_params(num_pre_smooth=pre, num_post_smooth=pre, coarse_cells=coarse,
+                                coarse_operator=coarse_operator)
     return scenes.build(spec, precision, solver)
 
 
@@ -38,12 +39,12 @@ def stats_of(m):
     return st.as_dict()
 
 
-def autotune(spec, precision, steps=3):
+def autotune(spec, precision, steps=3, coarse_operator=abi.COARSE_GALERKIN):
     """(pre/post sweeps, coarse cells) with the smallest mean solve time on
     ``spec`` after one warm-up step."""
     best, table = None, {}
     for pre, coarse in CANDIDATES:
-        m = build_scene(spec, precision, pre, coarse)
+        m = build_scene(spec, precision, pre, coarse, coarse_operator)
         m.PreStep(spec.dt)
         m.Step(spec.dt)
         t = []
@@ -60,20 +61,22 @@ def autotune(spec, precision, steps=3):
 
 
 class BatchRunner:
-    def __init__(self, specs, precision="mixed", tune=True, log_dir=None):
+    def __init__(self, specs, precision="mixed", tune=True, log_dir=None, coarse_operator=abi.COARSE_GALERKIN):
         self.specs = specs
         self.precision = precision
+        self.coarse_operator = coarse_operator
         self.tuned, self.tune_tables = {}, {}
         for spec in specs:
             if spec.n not in self.tuned:
                 if tune:
-                    self.tuned[spec.n], self.tune_tables[spec.n] = autotune(spec, precision)
+                    self.tuned[spec.n], self.tune_tables[spec.n] = autotune(spec, precision,
+                                                                             coarse_operator=coarse_operator)
                 else:
                     self.tuned[spec.n] = (2, 4096)
         self.models = []
         for spec in specs:
             pre, coarse = self.tuned[spec.n]
-            m = build_scene(spec, precision, pre, coarse)
+            m = build_scene(spec, precision, pre, coarse, coarse_operator)
             if log_dir is None:
                 call("lhi_liquid_set_async", m._h, 1)
             else:
@@ -148,11 +151,14 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--log-dir", default=None)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--coarse", default="galerkin", choices=["galerkin", "reference"],
+                    help="coarse multigrid operators: Galerkin (default) or the reference's re-discretisation")
     a = ap.parse_args(argv)
+    cop = abi.COARSE_GALERKIN if a.coarse == "galerkin" else abi.COARSE_REFERENCE
     rng = np.random.default_rng(a.seed)
     specs = [scenes.random_scene(rng) for _ in range(a.scenes)]
     t0 = time.time()
-    runner = BatchRunner(specs, a.precision, tune=not a.no_tune, log_dir=a.log_dir)
+    runner = BatchRunner(specs, a.precision, tune=not a.no_tune, log_dir=a.log_dir, coarse_operator=cop)
     setup_s = time.time() - t0
     import torch
     torch.cuda.synchronize()
@@ -169,6 +175,7 @@ def main(argv=None):
            "cells": cells, "wall_s": round(wall, 3), "scene_steps_per_s": round(scene_steps / wall, 2),
            "ms_per_batch_step": round(1000 * wall / a.steps, 3), "mean_cg_iterations": round(float(np.mean(iters)), 2),
            "failed_solves": bad, "diverged_scenes": {str(k): v for k, v in runner.diverged.items()},
+           "coarse_operator": a.coarse,
            "setup_s": round(setup_s, 1),
            "autotuned": {str(k): {"sweeps": v[0], "coarse_cells": v[1]} for k, v in runner.tuned.items()},
            "autotune_solve_ms": {str(k): v for k, v in runner.tune_tables.items()},
