@@ -19,7 +19,8 @@ def test_async_batch_matches_sequential(lhi):
     from liquidhairinteration_b200.batch import BatchRunner
     specs = _specs(4)
     runner = BatchRunner(specs, "mixed", tune=False)
-    seq = [scenes.build(s, "mixed", s.solver_params(num_pre_smooth=2, num_post_smooth=2, coarse_cells=4096))
+    seq = [scenes.build(s, "mixed", s.solver_params(num_pre_smooth=2, num_post_smooth=2, coarse_cells=4096,
+                                                    coarse_operator=abi.COARSE_GALERKIN))
            for s in specs]
     for _ in range(3):
         st_b = runner.step()

@@ -73,7 +73,10 @@ def test_galerkin_levels(lhi, prec):
 
 
 def test_galerkin_solve_matches_reference_levels(lhi):
-    """Same system on the finest level: the pressures agree to the solver tolerance."""
+    """Same system on the finest level: the pressures agree to the solver
+    tolerance on every row the matrix couples (a cell closed on all six
+    faces has an empty row, and its pressure is whatever the preconditioner
+    left there)."""
     spec = scenes.dam(32)
     out = []
     for op in (abi.COARSE_REFERENCE, abi.COARSE_GALERKIN):
@@ -86,7 +89,8 @@ def test_galerkin_solve_matches_reference_levels(lhi):
         st = g.GetSolver().Solve(spec.density, spec.dt)
         assert st["status"] == abi.LHI_OK, (op, st)
         out.append(g.field("pressure"))
-    assert rel_l2(out[1], out[0]) < 1e-8
+        rows = g.field("Adiag", 0) > 0
+    assert rel_l2(out[1][rows], out[0][rows]) < 1e-8
 
 
 def test_galerkin_converges_where_reference_levels_stall(lhi):
