@@ -45,6 +45,7 @@ SIGNATURES = {
     "lhi_solver_spmv": [_h, C.POINTER(C.c_double), C.POINTER(C.c_int32)],
     "lhi_liquid_render": [_h, C.POINTER(abi.RenderParams), _vp, _vp],
     "lhi_liquid_correct_volume": [_h, C.c_double],
+    "lhi_debug_set_stage_wait_limit": [C.c_double],
     "lhi_liquid_get_cfl": [_h, C.POINTER(C.c_double)],
     "lhi_net_create": [C.c_uint64, C.POINTER(C.c_void_p)],
     "lhi_net_destroy": [C.c_void_p],

@@ -440,6 +440,9 @@ public:
     T* p_ptr(int k) const { return pdata_[pcur_] + size_t(k) * size_t(pcap_); }
 };
 
+// limit of the solver kernels' waits on their TMA staging copies, on the current device (k_solver.cu)
+void set_stage_wait_limit_ns(unsigned long long ns);
+
 // device-wide exclusive scan (k_sort.cu)
 void device_exclusive_scan_i32(const int32_t* in, int32_t* out, long long n, void* tmp, long long tmp_bytes,
                                cudaStream_t s);

@@ -36,6 +36,12 @@ namespace {
 
 constexpr int kGraphIterationCap = 100000;  // hard stop of the device-side loop
 
+// Limit of the solver kernels' waits on their TMA staging copies (200 ms;
+// lhi_debug_set_stage_wait_limit lowers it to test the timeout path).  On
+// a timeout a CTA records it, waits (200 ms at most) for every copy of its
+// own still in flight, and leaves.
+__device__ unsigned long long g_stage_wait_ns = kWaitLimitNs;
+
 template <class T> struct LevelK {
     int nx, ny, nz;
     const T* diag;
@@ -624,12 +630,14 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
             rb_issue(sm + rb::kBase + (s ^ 1) * rb::kStage, &bar[s ^ 1], &mz, &mr, &md, &mcx, &mcy, &mcz, &mm, a, b,
                      c);
         }
-        if (__syncthreads_or(!bar_wait(&bar[s], (it >> 1) & 1))) {  // every thread leaves together
+        if (__syncthreads_or(!bar_wait(&bar[s], (it >> 1) & 1, g_stage_wait_ns))) {  // every thread leaves together
             if (threadIdx.x == 0) {
                 sc->timeout = 1;
                 sc->status = LHI_E_TIMEOUT;
                 sc->stop = 1;
-                if (un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);  // the prefetch, bounded too
+                // no copy of this CTA may still be landing when it exits: the one given up on and the prefetch
+                bar_wait(&bar[s], (it >> 1) & 1);
+                if (un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);
             }
             break;  // a CTA that gave up still takes part in the grid-wide sum below
         }
@@ -1250,8 +1258,11 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             tile_origin(ids, un, tdy, tdz, a, b, c);
             sp_issue(sm + sp::kBase + (s ^ 1) * sp::kStage, &bar[s ^ 1], &mp, &md, &mcx, &mcy, &mcz, &mm, a, b, c);
         }
-        if (__syncthreads_or(!bar_wait(&bar[s], (it >> 1) & 1))) {  // every thread leaves together
-            if (threadIdx.x == 0 && un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);  // the prefetch, bounded
+        if (__syncthreads_or(!bar_wait(&bar[s], (it >> 1) & 1, g_stage_wait_ns))) {  // every thread leaves together
+            if (threadIdx.x == 0) {  // drain this CTA's copies in flight (the one given up on, the prefetch)
+                bar_wait(&bar[s], (it >> 1) & 1);
+                if (un < units) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1);
+            }
             failed = true;
             break;
         }
@@ -1350,12 +1361,14 @@ __global__ void __launch_bounds__(kTileThreads, 3)
             tma_load_box(sm + rs::oCZ, &mcz, z0 - 4, y0, x0, bar);
             tma_load_box(sm + rs::oM, &mm, z0, y0, x0, bar);
         }
-        if (__syncthreads_or(!bar_wait(bar, parity))) {  // every thread leaves together
+        if (__syncthreads_or(!bar_wait(bar, parity, g_stage_wait_ns))) {  // every thread leaves together
             if (threadIdx.x == 0) {
                 sc->timeout = 1;
                 sc->status = LHI_E_TIMEOUT;
                 sc->stop = 1;
+                bar_wait(bar, parity);  // the copy given up on lands before the CTA exits
             }
+            __syncthreads();
             return;
         }
         parity ^= 1u;
@@ -2526,6 +2539,10 @@ template <class T, class TX> void LiquidImpl<T, TX>::get_acoef(int level, T* hos
     LHI_CUDA(cudaMemcpyAsync(host_out, d, sizeof(T) * 6 * L.n, cudaMemcpyDeviceToHost, stream_));
     LHI_CUDA(cudaStreamSynchronize(stream_));
     cudaFree(d);
+}
+
+void set_stage_wait_limit_ns(unsigned long long ns) {
+    LHI_CUDA(cudaMemcpyToSymbol(g_stage_wait_ns, &ns, sizeof(ns)));
 }
 
 template class LiquidImpl<float, float>;

@@ -75,8 +75,11 @@ __device__ __forceinline__ uint64_t timer_ns() {
     return t;
 }
 
-// Waits for the barrier phase of this parity; gives up after 200 ms.
-__device__ __forceinline__ bool bar_wait(uint64_t* bar, unsigned parity) {
+constexpr uint64_t kWaitLimitNs = 200000000ull;  // 200 ms
+
+// Waits for the barrier phase of this parity; gives up after limit_ns
+// (200 ms unless the caller passes another limit).
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, unsigned parity, uint64_t limit_ns = kWaitLimitNs) {
     const uint32_t addr = smem_addr(bar);
     uint64_t deadline = 0;
     for (;;) {
@@ -90,7 +93,7 @@ __device__ __forceinline__ bool bar_wait(uint64_t* bar, unsigned parity) {
             : "memory");
         if (done) return true;
         const uint64_t now = timer_ns();
-        if (deadline == 0) deadline = now + 200000000ull;
+        if (deadline == 0) deadline = now + limit_ns;
         else if (now > deadline) return false;
     }
 }
