@@ -60,7 +60,7 @@ __global__ void k_cell_count(const uint32_t* __restrict__ keys, long long n, int
 // the particles of its cell.  Lanes of a warp with the same key take
 // consecutive ranks in lane order from one atomic add; warps take their
 // blocks of ranks in whatever order the atomics land, so k_cell_order then
-// sorts every cell's indices, which makes the whole order the stable one.
+// orders every cell by particle ID.
 __global__ void k_rank_scatter(const uint32_t* __restrict__ keys, long long n, const int32_t* __restrict__ cs,
                                int32_t* __restrict__ cursor, uint32_t* __restrict__ skeys,
                                int32_t* __restrict__ order) {
@@ -79,10 +79,15 @@ __global__ void k_rank_scatter(const uint32_t* __restrict__ keys, long long n, c
     order[pos] = int32_t(i);
 }
 
-// Sorts the indices of every cell ascending (insertion sort for the usual
-// handful, heap sort for a crowded cell), so equal keys keep their input
-// order: the result is the stable sort by cell key.
-__global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, int32_t* __restrict__ order) {
+// Orders every cell's particles by particle ID (insertion sort for the usual
+// handful, nearly in order already since most particles stay in their cell;
+// heap sort for a crowded cell).  The sorted order is then the stable sort
+// of the caller's order by cell key whatever order the device held before,
+// so every sum taken in sorted order (P2G, CorrectVolume) depends only on
+// the particles' state, and a run resumed from a checkpoint repeats the
+// uninterrupted one bit for bit.
+__global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, const int32_t* __restrict__ pid,
+                             int32_t* __restrict__ order) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     const int s = cs[c], e = cs[c + 1];
@@ -92,8 +97,9 @@ __global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, in
     if (len <= 64) {
         for (int i = 1; i < len; ++i) {
             const int32_t v = a[i];
+            const int32_t kv = pid[v];
             int j = i - 1;
-            while (j >= 0 && a[j] > v) {
+            while (j >= 0 && pid[a[j]] > kv) {
                 a[j + 1] = a[j];
                 --j;
             }
@@ -101,12 +107,12 @@ __global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, in
         }
         return;
     }
-    auto sift = [&](int root, int end) {  // max-heap on a[0, end)
+    auto sift = [&](int root, int end) {  // max-heap on pid[a[0, end)]
         while (true) {
             int ch = 2 * root + 1;
             if (ch >= end) return;
-            if (ch + 1 < end && a[ch + 1] > a[ch]) ++ch;
-            if (a[root] >= a[ch]) return;
+            if (ch + 1 < end && pid[a[ch + 1]] > pid[a[ch]]) ++ch;
+            if (pid[a[root]] >= pid[a[ch]]) return;
             const int32_t t = a[root];
             a[root] = a[ch];
             a[ch] = t;
@@ -1187,7 +1193,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
         k_rank_scatter<<<blocks_for(np_, 256), 256, 0, stream_>>>(keys_[0], np_, cell_start_, cell_count_, keys_[1],
                                                                  vals_[1]);
         LHI_LAUNCH_CHECK();
-        k_cell_order<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, ncell_, vals_[1]);
+        k_cell_order<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, ncell_, pid_[pcur_], vals_[1]);
         LHI_LAUNCH_CHECK();
         k_permute<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_,
                                                                 pid_[pcur_], pid_[pcur_ ^ 1], vals_[1], np_);

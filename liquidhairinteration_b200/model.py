@@ -222,17 +222,27 @@ class ParticleSystem:
         from . import snapshots
         snapshots.write_frame(filename, self.GetPositions(), append=isAppend)
 
+    def _meta(self):
+        g = self._m.grid
+        return {"precision": self._m.precision, "grid_dim": list(g.dim),
+                "min_coord": list(g.min_coord), "max_coord": list(g.max_coord)}
+
     def SaveCheckpoint(self, filename, **counters):
-        """Binary checkpoint of the whole particle state (exact bits) plus
-        the caller's counters, e.g. step and time."""
+        """Binary checkpoint of the whole particle state (exact bits), the
+        model's precision and grid, and the caller's counters (e.g. step and
+        time).  The device's cell order breaks ties by particle id, so
+        stepping a model loaded from it repeats the uninterrupted run bit
+        for bit under the same solver and liquid parameters."""
         from . import snapshots
         pos, vel, aff = self.GetParticles()
-        snapshots.save_checkpoint(filename, pos, vel, aff, **counters)
+        snapshots.save_checkpoint(filename, pos, vel, aff, meta=self._meta(), **counters)
 
     def LoadCheckpoint(self, filename):
-        """Restores a SaveCheckpoint file; returns its counters."""
+        """Restores a SaveCheckpoint file; returns its counters.  A file
+        saved with another precision or grid raises ValueError and leaves
+        the particles as they were."""
         from . import snapshots
-        c = snapshots.load_checkpoint(filename)
+        c = snapshots.load_checkpoint(filename, meta=self._meta())
         self.SetParticles(c.pop("pos"), c.pop("vel"), c.pop("affine"))
         return c
 

@@ -40,19 +40,28 @@ def read_frames(path):
     return frames
 
 
-def save_checkpoint(path, pos, vel, affine, **counters):
+def save_checkpoint(path, pos, vel, affine, meta=None, **counters):
     """Positions (n x 3), velocities (n x 3) and affine matrices (n x 9,
-    column-major) plus named scalar counters (step, time, ...)."""
+    column-major), the model description ``meta`` (precision, grid dims and
+    bounds) and named scalar counters (step, time, ...)."""
     pos, vel, affine = (np.ascontiguousarray(a) for a in (pos, vel, affine))
     if not (pos.shape[0] == vel.shape[0] == affine.shape[0]) or pos.dtype != vel.dtype or pos.dtype != affine.dtype:
         raise ValueError("positions, velocities and affine matrices must have one count and one dtype")
-    np.savez(path, pos=pos.reshape(-1, 3), vel=vel.reshape(-1, 3), affine=affine.reshape(-1, 9),
+    extra = {"meta_" + k: np.asarray(v) for k, v in (meta or {}).items()}
+    np.savez(path, pos=pos.reshape(-1, 3), vel=vel.reshape(-1, 3), affine=affine.reshape(-1, 9), **extra,
              **{"counter_" + k: np.asarray(v) for k, v in counters.items()})
 
 
-def load_checkpoint(path):
-    """dict with pos, vel, affine and the saved counters."""
+def load_checkpoint(path, meta=None):
+    """dict with pos, vel, affine and the saved counters.  With ``meta``,
+    every entry it names must equal the one saved (ValueError otherwise)."""
     with np.load(path) as z:
+        for k, want in (meta or {}).items():
+            if "meta_" + k not in z.files:
+                raise ValueError(f"checkpoint {path} does not record {k}")
+            got = z["meta_" + k]
+            if got.shape != np.shape(want) or not np.array_equal(got, np.asarray(want)):
+                raise ValueError(f"checkpoint {path} was saved with {k} = {got.tolist()}, this model has {want}")
         out = {"pos": z["pos"], "vel": z["vel"], "affine": z["affine"]}
         for k in z.files:
             if k.startswith("counter_"):

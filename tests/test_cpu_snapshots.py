@@ -54,6 +54,22 @@ def test_checkpoint_restores_exact_bits(tmp_path, dtype):
     assert c["step"] == 17 and c["time"] == 0.0354
 
 
+def test_checkpoint_meta_mismatch_rejected(tmp_path):
+    pos = np.zeros((4, 3), np.float32)
+    aff = np.zeros((4, 9), np.float32)
+    meta = {"precision": "fp32", "grid_dim": [16, 16, 16], "min_coord": [0.0] * 3, "max_coord": [1.0] * 3}
+    path = tmp_path / "ck.npz"
+    snapshots.save_checkpoint(path, pos, pos, aff, meta=meta, step=3)
+    assert snapshots.load_checkpoint(path, meta=meta)["step"] == 3
+    for k, v in (("precision", "fp64"), ("grid_dim", [16, 16, 32]), ("max_coord", [2.0, 1.0, 1.0])):
+        with pytest.raises(ValueError, match=k):
+            snapshots.load_checkpoint(path, meta=dict(meta, **{k: v}))
+    old = tmp_path / "old.npz"
+    snapshots.save_checkpoint(old, pos, pos, aff)
+    with pytest.raises(ValueError, match="does not record"):
+        snapshots.load_checkpoint(old, meta=meta)
+
+
 def test_render_oracle_pixel_rule(oracle_mod):
     """The oracle's point rasterisation on a 16 x 16 image with 5-pixel
     points: a point at the domain centre covers pixels 5..9 on both axes, a

@@ -1,7 +1,8 @@
 """Around the step: LiquidModel<3>::GetCFL (LiquidModel.h:49-55), the
 reference's clamp of dx / max|v| over the particles' velocities, the same
 after a step and after the same particles are set again; and the particle
-checkpoint, which restores the exact particle state in a fresh model."""
+checkpoint, which restores the exact particle state in a fresh model whose
+next steps then repeat the uninterrupted run bit for bit."""
 import numpy as np
 import pytest
 
@@ -39,9 +40,12 @@ def test_cfl_after_step_and_after_set_particles(lhi, prec):
 def test_checkpoint_restores_particles(lhi, prec, tmp_path):
     """ParticleSystem SaveCheckpoint / LoadCheckpoint through the C-ABI: a
     fresh model loaded from a checkpoint holds the same particle bits, in
-    the caller's order, and gets the counters back."""
+    the caller's order, gets the counters back, and its next steps repeat
+    the uninterrupted run bit for bit.  A model of another precision or
+    grid refuses the file."""
     spec = scenes.dam(16)
-    m = gpu_model(spec, prec, spec.solver_params(coarse_cells=64, true_residual_every=0 if prec == "fp32" else 10))
+    solver = spec.solver_params(coarse_cells=64, true_residual_every=0 if prec == "fp32" else 10)
+    m = gpu_model(spec, prec, solver)
     pos, vel = scenes.seed(spec, "fp64" if prec == "fp64" else "fp32")
     m.GetParticleSystem().SetParticles(pos, vel)
     for _ in range(2):
@@ -50,10 +54,24 @@ def test_checkpoint_restores_particles(lhi, prec, tmp_path):
     path = tmp_path / "ck.npz"
     m.GetParticleSystem().SaveCheckpoint(path, step=2, time=2 * spec.dt)
     saved = m.GetParticleSystem().GetParticles()
-    m2 = gpu_model(spec, prec)
+    m2 = gpu_model(spec, prec, solver)
     counters = m2.GetParticleSystem().LoadCheckpoint(path)
     assert counters == {"step": 2, "time": 2 * spec.dt}
     for a, b in zip(m2.GetParticleSystem().GetParticles(), saved):
         assert np.array_equal(a, b)
-    m.close()
-    m2.close()
+    for step in range(2):
+        for x in (m, m2):
+            x.PreStep(spec.dt)
+            x.Step(spec.dt)
+        for a, b in zip(m2.GetParticleSystem().GetParticles(), m.GetParticleSystem().GetParticles()):
+            assert np.array_equal(a, b), f"resumed step {step + 3}"
+    other = gpu_model(spec, "fp64" if prec != "fp64" else "fp32")
+    with pytest.raises(ValueError, match="precision"):
+        other.GetParticleSystem().LoadCheckpoint(path)
+    spec24 = scenes.dam(24)
+    other24 = gpu_model(spec24, prec)
+    with pytest.raises(ValueError, match="grid_dim"):
+        other24.GetParticleSystem().LoadCheckpoint(path)
+    assert other24.GetParticleSystem().NumParticles() == 0
+    for x in (m, m2, other, other24):
+        x.close()

@@ -3,10 +3,11 @@
 
 The oracle walks a particle's neighbours cell by cell in caller order; the
 GPU walks the cell-sorted particles, whose order within a cell is the
-caller order right after the particles are set (the radix sort is stable),
-so the sums match bit for bit there; after steps the order within a cell
-differs and the comparison has a tolerance.  Coincident particles take the
-seeded counter-based random numbers on both sides."""
+caller order (the sort breaks ties by particle id), so the sums match bit
+for bit on fresh particles and after steps.  Whole steps with the
+correction on track the oracle within a tolerance (their P2G sums in
+another order).  Coincident particles take the seeded counter-based random
+numbers on both sides."""
 import numpy as np
 import pytest
 
@@ -57,8 +58,25 @@ def test_correct_volume_bitwise_on_fresh_particles(oracle_mod, lhi, prec):
         moved = np.flatnonzero((after != before).any(axis=1))
         assert moved.size > 0
         assert (moved % 8 == call_no).all(), "only the particles of this step of the cycle move"
-        # the next call walks the moved positions: re-seed the device order from the caller order
-        g.GetParticleSystem().SetParticles(after, vel)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_correct_volume_bitwise_after_steps(oracle_mod, lhi, prec):
+    """After 3 steps the device holds the particles in the previous sort's
+    order; the oracle gets the GPU's particles (caller order) and both
+    correct them: bit for bit."""
+    spec = scenes.dam(16)
+    g, o = _pair(oracle_mod, spec, prec)
+    pos, vel = scenes.seed(spec, "fp64" if prec == "fp64" else "fp32")
+    g.GetParticleSystem().SetParticles(pos, vel)
+    for _ in range(3):
+        g.PreStep(spec.dt)
+        g.Step(spec.dt)
+    o.set_particles(*g.GetParticleSystem().GetParticles())
+    for call_no in range(2):
+        g.CorrectVolume(spec.dt)
+        o.correct_volume(spec.dt)
+        assert_bitwise(g.GetParticleSystem().GetPositions(), o.get_particles()[0], f"call {call_no}")
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])

@@ -74,7 +74,8 @@ def test_cell_sort_bitwise(oracle_mod, lhi, prec):
 @pytest.mark.parametrize("prec", PRECS)
 def test_cell_sort_after_advection(oracle_mod, lhi, prec):
     """After a step the device order is the previous sort; the new sort must
-    give the same keys per particle and the same per-cell particle sets."""
+    still be the stable sort of the caller's order: the oracle's ids, keys
+    and cell ranges on the GPU's own positions."""
     spec = scenes.dam(16)
     g, o = pair(oracle_mod, spec, prec)
     for m in (g,):
@@ -89,8 +90,9 @@ def test_cell_sort_after_advection(oracle_mod, lhi, prec):
     ids = g.field("particle_id")
     assert_bitwise(g.field("cell_key"), keys[ids], "keys")
     cs = g.field("cell_start")
-    _, cs_o = o.sort_by_cell()
+    ids_o, cs_o = o.sort_by_cell()
     assert_bitwise(cs, cs_o, "cell_start")
+    assert_bitwise(ids, ids_o, "stable order")
 
 
 @pytest.mark.parametrize("prec", PRECS)
