@@ -83,9 +83,8 @@ __global__ void k_rank_scatter(const uint32_t* __restrict__ keys, long long n, c
 // handful, nearly in order already since most particles stay in their cell;
 // heap sort for a crowded cell).  The sorted order is then the stable sort
 // of the caller's order by cell key whatever order the device held before,
-// so every sum taken in sorted order (P2G, CorrectVolume) depends only on
-// the particles' state, and a run resumed from a checkpoint repeats the
-// uninterrupted one bit for bit.
+// so every walk of the sorted lists (P2G's per-cell sums, CorrectVolume's
+// neighbour sums) visits the particles in an order fixed by their state.
 __global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, const int32_t* __restrict__ pid,
                              int32_t* __restrict__ order) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -230,9 +230,10 @@ class ParticleSystem:
     def SaveCheckpoint(self, filename, **counters):
         """Binary checkpoint of the whole particle state (exact bits), the
         model's precision and grid, and the caller's counters (e.g. step and
-        time).  The device's cell order breaks ties by particle id, so
-        stepping a model loaded from it repeats the uninterrupted run bit
-        for bit under the same solver and liquid parameters."""
+        time).  Stepping a model loaded from it under the same solver and
+        liquid parameters tracks the uninterrupted run to rounding: the cell
+        order is the same (ties go by particle id), but P2G's atomic adds
+        land in a run-dependent order."""
         from . import snapshots
         pos, vel, aff = self.GetParticles()
         snapshots.save_checkpoint(filename, pos, vel, aff, meta=self._meta(), **counters)

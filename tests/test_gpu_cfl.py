@@ -2,7 +2,7 @@
 reference's clamp of dx / max|v| over the particles' velocities, the same
 after a step and after the same particles are set again; and the particle
 checkpoint, which restores the exact particle state in a fresh model whose
-next steps then repeat the uninterrupted run bit for bit."""
+next steps then track the uninterrupted run."""
 import numpy as np
 import pytest
 
@@ -59,12 +59,20 @@ def test_checkpoint_restores_particles(lhi, prec, tmp_path):
     assert counters == {"step": 2, "time": 2 * spec.dt}
     for a, b in zip(m2.GetParticleSystem().GetParticles(), saved):
         assert np.array_equal(a, b)
+    # P2G's shared-memory and global atomic adds land in a run-dependent
+    # order, so the resumed run tracks the uninterrupted one to rounding
+    # (amplified by the solves' stopping rule), not bit for bit
     for step in range(2):
+        its = []
         for x in (m, m2):
             x.PreStep(spec.dt)
             x.Step(spec.dt)
-        for a, b in zip(m2.GetParticleSystem().GetParticles(), m.GetParticleSystem().GetParticles()):
-            assert np.array_equal(a, b), f"resumed step {step + 3}"
+            its.append(x.GetSolver().Stats()["iterations"])
+        assert abs(its[0] - its[1]) <= 1, its
+        (p1, v1, a1), (p2, v2, a2) = m.GetParticleSystem().GetParticles(), m2.GetParticleSystem().GetParticles()
+        assert np.abs(p2.astype(np.float64) - p1).max() <= 1e-4 * spec.dx, f"resumed step {step + 3}"
+        for x1, x2 in ((v1, v2), (a1, a2)):
+            assert np.abs(x2.astype(np.float64) - x1).max() <= 1e-3 * np.abs(x1).max(), f"resumed step {step + 3}"
     other = gpu_model(spec, "fp64" if prec != "fp64" else "fp32")
     with pytest.raises(ValueError, match="precision"):
         other.GetParticleSystem().LoadCheckpoint(path)
