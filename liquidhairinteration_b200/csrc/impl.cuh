@@ -18,6 +18,16 @@
 #include "net.cuh"
 #include "tma.cuh"
 
+// One window offset of the liquid SDF's gather: a lower bound (with a safety
+// margin) of |x_c - x_p| - r over every particle of the window cell at this
+// offset from cell c, and the offset packed as (ox + 16) | (oy + 16) << 8 |
+// (oz + 16) << 16.
+struct LphiOffset {
+    double lb;
+    int32_t off;
+    int32_t pad;
+};
+
 namespace lhi {
 
 constexpr int kMaxBoundaryNodes = 32;
@@ -307,6 +317,7 @@ public:
     // ---- internals shared by the .cu files
     void alloc_particles(int64_t cap);
     void ensure_sorted();
+    void build_liquid_phi_table();
     void p2g_accumulate();
     void p2g_normalize(bool with_gravity, T gdt);
     void g2p(bool advect, T dt);
@@ -358,6 +369,8 @@ public:
     uint8_t* valid_ = nullptr;  // isValid: 255 invalid, else the sweep it became valid
     uint8_t* occ_ = nullptr;    // 4^3-cell block occupancy for the liquid SDF
     int occ_dim_[3];
+    LphiOffset* lphi_tab_ = nullptr;  // the liquid SDF's window offsets by ascending distance bound
+    int lphi_n_ = 0;
 
     // particles (SoA, sorted by cell): 15 scalars + caller id, double-buffered
     int64_t np_ = 0, pcap_ = 0;

@@ -380,6 +380,7 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
     LHI_CUDA(cudaMemsetAsync(valid_, 255, nnode_, stream_));  // std::vector<bool>: all false
     for (int i = 0; i < 3; ++i) occ_dim_[i] = (dims[i] + 3) / 4;
     LHI_CUDA(cudaMalloc(&occ_, size_t(occ_dim_[0]) * occ_dim_[1] * occ_dim_[2]));
+    build_liquid_phi_table();
     LHI_CUDA(cudaMalloc(&cell_count_, sizeof(int32_t) * (ncell_ + 1)));
     LHI_CUDA(cudaMalloc(&cell_start_, sizeof(int32_t) * (ncell_ + 1)));
     LHI_CUDA(cudaMemsetAsync(cell_start_, 0, sizeof(int32_t) * (ncell_ + 1), stream_));
@@ -469,6 +470,7 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
     F(solid_phi_);
     F(valid_);
     F(occ_);
+    F(lphi_tab_);
     F(cell_count_);
     F(cell_start_);
     F(scan_tmp_);

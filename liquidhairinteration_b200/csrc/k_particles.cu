@@ -1,10 +1,16 @@
 // k_particles.cu -- particle side of the liquid step.
 //
-//   keys -> radix sort -> permute  : particles stay physically sorted by cell
-//   liquid SDF (ComputeLiquidPhi)  : per-cell gather over the sorted cells
-//   P2G (Particle2Grid)            : 8^3-cell tiles accumulated in shared
-//                                    memory, flushed once per node
-//   G2P + advection                : one thread per particle, exact rounding
+//   keys -> counting sort -> permute : particles stay physically sorted by
+//                                      cell (ties by particle id)
+//   liquid SDF (ComputeLiquidPhi)    : per-cell gather over the sorted cells,
+//                                      nearest window cells first
+//   P2G (Particle2Grid)              : 8^3-cell tiles accumulated in shared
+//                                      memory, flushed once per node
+//   G2P + advection                  : 8^3-cell tiles of face velocities
+//                                      staged in shared memory, one thread
+//                                      per particle
+#include <algorithm>
+
 #include "impl.cuh"
 
 namespace lhi {
@@ -171,36 +177,25 @@ __global__ void k_soa_to_aos(const T* __restrict__ pd, long long cap, const int3
 // LiquidModel<3>::ComputeLiquidPhi (LiquidModel.cpp:540-560) as a gather:
 // cell c takes min(|x_c - x_p| - r) over particles p whose Point2Index cell
 // lies within +-d of c.  The minimum does not depend on visiting order, so
-// the result is bit-identical to the reference.  Window cells that provably
-// cannot lower the current minimum are skipped (bound with safety margin),
-// and the cell's own particles are visited first so the bound bites early.
+// the result is bit-identical to the reference.  The window's cells are
+// visited in ascending order of a lower bound of what their particles can
+// give (the table, own cell first); the walk ends at the first bound above
+// the current minimum, since no later cell can lower it.  Inside the liquid
+// the cell's own particles already end it.
 template <class T>
 __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* __restrict__ cs,
                                                     const uint8_t* __restrict__ occ, int ox, int oy, int oz,
                                                     const T* __restrict__ pd, long long cap, T radius, int d0, int d1,
-                                                    int d2, T* __restrict__ phi) {
-    // lower bound of |x_c - x_p| - r over the particles of a window cell at
-    // offset (ax, ay, az) from c, with a safety margin: every point of that
-    // cell's box is at least the box distance from the centre
-    __shared__ double s_lb[9 * 9 * 9];
-    const int nb = (d0 + 1) * (d1 + 1) * (d2 + 1);
-    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
-        const int az = e % (d2 + 1), ay = (e / (d2 + 1)) % (d1 + 1), ax = e / ((d1 + 1) * (d2 + 1));
-        T lx = T(fmax(double(ax) - 0.5, 0.0)) * g.dx[0];
-        T ly = T(fmax(double(ay) - 0.5, 0.0)) * g.dx[1];
-        T lz = T(fmax(double(az) - 0.5, 0.0)) * g.dx[2];
-        s_lb[e] = sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
-                  double(radius) * (1.0 + 1e-6);
-    }
-    __syncthreads();
+                                                    int d2, const LphiOffset* __restrict__ tab, int ntab,
+                                                    T* __restrict__ phi) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long nc = (long long)g.nx * g.ny * g.nz;
     if (c >= nc) return;
     int cx, cy, cz;
     idx3(c, g.ny, g.nz, cx, cy, cz);
-    int x0 = max(0, cx - d0), x1 = min(g.nx - 1, cx + d0);
-    int y0 = max(0, cy - d1), y1 = min(g.ny - 1, cy + d1);
-    int z0 = max(0, cz - d2), z1 = min(g.nz - 1, cz + d2);
+    const int x0 = max(0, cx - d0), x1 = min(g.nx - 1, cx + d0);
+    const int y0 = max(0, cy - d1), y1 = min(g.ny - 1, cy + d1);
+    const int z0 = max(0, cz - d2), z1 = min(g.nz - 1, cz + d2);
     bool any = false;
     for (int bx = x0 >> 2; bx <= (x1 >> 2) && !any; ++bx)
         for (int by = y0 >> 2; by <= (y1 >> 2) && !any; ++by)
@@ -218,22 +213,21 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
     const T* px = pd;
     const T* py = pd + cap;
     const T* pz = pd + 2 * cap;
-    // Visits window cell (wx, wy, wz).  With prune, a cell is skipped when
-    // every point of its box is farther than cur + r from the centre (the
-    // bound holds for particles clamped into an outer-layer cell too: they
-    // lie beyond it).
-    auto visit = [&](int wx, int wy, int wz, bool prune) {
-        if (prune) {  // the bound needs no memory access but the table: test it first
-            const int ax = abs(wx - cx), ay = abs(wy - cy), az = abs(wz - cz);
-            if (double(cur) < s_lb[(ax * (d1 + 1) + ay) * (d2 + 1) + az]) return;
-        }
+    for (int k = 0; k < ntab; ++k) {
+        const LphiOffset e = tab[k];
+        if (double(cur) < e.lb) break;
+        const int wx = cx + (e.off & 255) - 16, wy = cy + ((e.off >> 8) & 255) - 16,
+                  wz = cz + ((e.off >> 16) & 255) - 16;
+        if (wx < x0 || wx > x1 || wy < y0 || wy > y1 || wz < z0 || wz > z1) continue;
         const long long w = ((long long)wx * g.ny + wy) * g.nz + wz;
-        const int s = cs[w], e = cs[w + 1];
-        if (s == e) return;
+        const int s = cs[w], en = cs[w + 1];
+        if (s == en) continue;
         // the particles of a cell off the grid's outer layer were sorted
         // into it by their own unclamped Point2Index: all inside the window
+        // (and the bound holds for particles clamped into an outer-layer
+        // cell: they lie beyond it)
         const bool own = wx > 0 && wx < g.nx - 1 && wy > 0 && wy < g.ny - 1 && wz > 0 && wz < g.nz - 1;
-        for (int p = s; p < e; ++p) {
+        for (int p = s; p < en; ++p) {
             T qx = px[p], qy = py[p], qz = pz[p];
             if (!own) {
                 int tx = cell_trunc(qx, g.mn[0], g.dx[0]);
@@ -245,22 +239,7 @@ __global__ void __launch_bounds__(256) k_liquid_phi(GridP<T> g, const int32_t* _
             T ph = X<T>::sub(dist, radius);
             cur = (cur < ph) ? cur : ph;
         }
-    };
-    // The minimum does not depend on the visiting order, so the cell's own
-    // particles go first: inside the liquid they already bring cur below the
-    // bound of every neighbouring cell.  Then the 26 neighbours, then the
-    // rest of the window, both pruned.
-    visit(cx, cy, cz, false);
-    for (int pass = 1; pass < 3; ++pass)
-        for (int wx = x0; wx <= x1; ++wx)
-            for (int wy = y0; wy <= y1; ++wy)
-                for (int wz = z0; wz <= z1; ++wz) {
-                    const int ax = abs(wx - cx), ay = abs(wy - cy), az = abs(wz - cz);
-                    if ((ax | ay | az) == 0) continue;
-                    const bool inner = ax <= 1 && ay <= 1 && az <= 1;
-                    if (inner != (pass == 1)) continue;
-                    visit(wx, wy, wz, true);
-                }
+    }
     phi[c] = cur;
 }
 
@@ -818,11 +797,100 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
     }
 }
 
+// Quadratic B-spline weights (qweight) and the reference's gradient weights
+// (gqweight) of the three nodes around a middle node at signed distance
+// t = x - node in [-1/2, 1/2] (grid units): the nodes at -1, 0, +1 sit at
+// distances t + 1, t, t - 1, which fall on the outer branch, the inner
+// branch and the outer branch of both functions.
+template <class T> __device__ __forceinline__ void axis_weights(T t, T w[3], T gw[3]) {
+    const T l = T(0.5f) - t, r = T(0.5f) + t;
+    w[0] = T(0.5f) * l * l;
+    w[1] = T(0.75f) - t * t;
+    w[2] = T(0.5f) * r * r;
+    gw[0] = -l;
+    gw[1] = T(-2.f) * fabs(t);
+    gw[2] = -r;
+}
+
+// Factored gather (mixed precision) of a particle whose truncated cell ci
+// lies in the staged tile.  Per axis the particle has one window for face
+// nodes (middle node = the nearest integer coordinate) and one for cell
+// centres (middle node = the centre of ci), each three nodes wide; the
+// weights of both are formed once and shared by the three components (the
+// face window on a component's own axis, the centre window across it).
+// Nodes outside the reference's clipped window (+-d around ci) or the face
+// grid get zero weights; the staged region holds every window node of a
+// particle of the tile (zero outside the grid), so the loads need no test.
+// The same sums as the factored path of g2p_component, up to rounding.
+template <class T, int A>
+__device__ __forceinline__ void g2p_staged_component(const T wf[3][3], const T gf[3][3], const T wc[3][3],
+                                                     const T gc[3][3], const int mf[3], const int ci[3],
+                                                     const VSrc<T>& vs, T& velA, T col[3]) {
+    const int bx = ((A == 0) ? mf[0] : ci[0]) - 1, by = ((A == 1) ? mf[1] : ci[1]) - 1,
+              bz = ((A == 2) ? mf[2] : ci[2]) - 1;
+    const T* wx = (A == 0) ? wf[0] : wc[0];
+    const T* gx = (A == 0) ? gf[0] : gc[0];
+    const T* wy = (A == 1) ? wf[1] : wc[1];
+    const T* gy = (A == 1) ? gf[1] : gc[1];
+    const T* wz = (A == 2) ? wf[2] : wc[2];
+    const T* gz = (A == 2) ? gf[2] : gc[2];
+    const T* base = vs.v + ((long long)(bx - vs.ox) * vs.fy + (by - vs.oy)) * vs.fz + (bz - vs.oz);
+#pragma unroll
+    for (int jx = 0; jx < 3; ++jx) {
+        T a = T(0), b = T(0), dd = T(0);
+#pragma unroll
+        for (int jy = 0; jy < 3; ++jy) {
+            const T* row = base + ((long long)jx * vs.fy + jy) * vs.fz;
+            T s = T(0), t = T(0);
+#pragma unroll
+            for (int jz = 0; jz < 3; ++jz) {
+                const T val = row[jz];
+                s = fma(wz[jz], val, s);
+                t = fma(gz[jz], val, t);
+            }
+            a = fma(wy[jy], s, a);
+            b = fma(gy[jy], s, b);
+            dd = fma(wy[jy], t, dd);
+        }
+        velA = fma(wx[jx], a, velA);
+        col[0] = fma(gx[jx], a, col[0]);
+        col[1] = fma(wx[jx], b, col[1]);
+        col[2] = fma(wx[jx], dd, col[2]);
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void g2p_staged_factored(const GridP<T>& g, const int d[3], const T g3[3], const int ci[3],
+                                                    const VSrc<T> src[3], T vel[3], T C[9]) {
+    T wf[3][3], gf[3][3], wc[3][3], gc[3][3];
+    int mf[3];
+    const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const T f = g3[i] - T(ci[i]);  // exact: g3 and ci are within one unit
+        const int up = f >= T(0.5f);
+        mf[i] = ci[i] + up;
+        axis_weights(g3[i] - T(mf[i]), wf[i], gf[i]);
+        axis_weights(f - T(0.5f), wc[i], gc[i]);
+        const int lo = off_lo(d[i]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int of = up + j - 1, nf = mf[i] + j - 1;  // face node: offset from ci, index
+            if (of < lo || of > min(2, d[i]) || nf < 0 || nf > n[i]) wf[i][j] = gf[i][j] = T(0);
+            const int nc = ci[i] + j - 1;  // centre node (offset j - 1)
+            if (j - 1 < lo || j - 1 > min(1, d[i]) || nc < 0 || nc > n[i] - 1) wc[i][j] = gc[i][j] = T(0);
+        }
+    }
+    g2p_staged_component<T, 0>(wf, gf, wc, gc, mf, ci, src[0], vel[0], &C[0]);
+    g2p_staged_component<T, 1>(wf, gf, wc, gc, mf, ci, src[1], vel[1], &C[3]);
+    g2p_staged_component<T, 2>(wf, gf, wc, gc, mf, ci, src[2], vel[2], &C[6]);
+}
+
 // One particle of LiquidModel<3>::Grid2Particle (LiquidModel.cpp:724-823)
 // fused with AdvectParticle (LiquidModel.cpp:913-935) and the next step's
 // cell key.  The face velocities come from the sources the caller picks
 // for the particle's truncated cell ci (staged in shared memory when ci lies
-// in the tile, global memory otherwise).
+// in the tile -- pick returns true -- global memory otherwise).
 template <class T, bool FACTORED, class PickSrc>
 __device__ __forceinline__ void g2p_particle(const GridP<T>& g, T* __restrict__ pd, long long cap, long long i,
                                              const int d[3], int do_g2p, int do_advect, T dt,
@@ -843,10 +911,15 @@ __device__ __forceinline__ void g2p_particle(const GridP<T>& g, T* __restrict__ 
 #pragma unroll
         for (int k = 0; k < 9; ++k) C[k] = T(0);
         VSrc<T> src[3];
-        pick(ci, src);
-        g2p_component<T, 0, FACTORED>(g, d, g3, ci, src[0], vel[0], &C[0]);
-        g2p_component<T, 1, FACTORED>(g, d, g3, ci, src[1], vel[1], &C[3]);
-        g2p_component<T, 2, FACTORED>(g, d, g3, ci, src[2], vel[2], &C[6]);
+        const bool staged = pick(ci, src);
+        // (g3 >= 0: ci is then the floor, as the staged windows assume)
+        if (FACTORED && staged && g3[0] >= T(0) && g3[1] >= T(0) && g3[2] >= T(0)) {
+            g2p_staged_factored<T>(g, d, g3, ci, src, vel, C);
+        } else {
+            g2p_component<T, 0, FACTORED>(g, d, g3, ci, src[0], vel[0], &C[0]);
+            g2p_component<T, 1, FACTORED>(g, d, g3, ci, src[1], vel[1], &C[3]);
+            g2p_component<T, 2, FACTORED>(g, d, g3, ci, src[2], vel[2], &C[6]);
+        }
 #pragma unroll
         for (int k = 0; k < 3; ++k) pd[(3 + k) * cap + i] = vel[k];
 #pragma unroll
@@ -892,7 +965,10 @@ __global__ void __launch_bounds__(256) k_g2p(GridP<T> g, T* __restrict__ pd, lon
     if (i >= n) return;
     const int d[3] = {d0, d1, d2};
     g2p_particle<T, FACTORED>(g, pd, cap, i, d, do_g2p, do_advect, dt, sp, keys, vals,
-                              [&](const int*, VSrc<T> src[3]) { global_sources(g, vx, vy, vz, src); });
+                              [&](const int*, VSrc<T> src[3]) {
+                                  global_sources(g, vx, vy, vz, src);
+                                  return false;
+                              });
 }
 
 // G2P + advection over the cell-sorted particles, one CTA per 8^3-cell tile:
@@ -963,11 +1039,12 @@ __global__ void __launch_bounds__(256, 3) k_g2p_tile(GridP<T> g, T* __restrict__
                             ci[2] < zend;
             if (!in) {  // off the grid: sorted into a clamped cell
                 global_sources(g, vx, vy, vz, src);
-                return;
+                return false;
             }
             src[0] = VSrc<T>{sv, x0 - 1, y0 - 1, z0 - 1, kTile + 2, kTile + 2};
             src[1] = VSrc<T>{sv + R0, x0 - 1, y0 - 1, z0 - 1, kTile + 3, kTile + 2};
             src[2] = VSrc<T>{sv + R0 + R1, x0 - 1, y0 - 1, z0 - 1, kTile + 2, kTile + 3};
+            return true;
         });
     }
 }
@@ -1213,6 +1290,36 @@ template <class T, class TX> void LiquidImpl<T, TX>::ensure_sorted() {
     if (!sorted_) sort_particles();
 }
 
+// The window offsets of k_liquid_phi with their distance bounds: a window
+// cell at offset (ax, ay, az) holds points no nearer to the cell centre than
+// the box distance max(|a| - 1/2, 0) dx per axis; the bound takes 1e-5 off
+// that distance and adds 1e-6 to r, far more than the rounding of the
+// kernel's |x_c - x_p| - r.  Sorted ascending (stable, own cell first).
+template <class T, class TX> void LiquidImpl<T, TX>::build_liquid_phi_table() {
+    const int d[3] = {window(radius_, dx_[0]), window(radius_, dx_[1]), window(radius_, dx_[2])};
+    if (d[0] > 8 || d[1] > 8 || d[2] > 8) return;  // compute_liquid_phi refuses such a radius
+    std::vector<LphiOffset> tab;
+    for (int ax = -d[0]; ax <= d[0]; ++ax)
+        for (int ay = -d[1]; ay <= d[1]; ++ay)
+            for (int az = -d[2]; az <= d[2]; ++az) {
+                const T lx = T(std::fmax(double(std::abs(ax)) - 0.5, 0.0)) * dx_[0];
+                const T ly = T(std::fmax(double(std::abs(ay)) - 0.5, 0.0)) * dx_[1];
+                const T lz = T(std::fmax(double(std::abs(az)) - 0.5, 0.0)) * dx_[2];
+                LphiOffset e;
+                e.lb = std::sqrt(double(lx) * lx + double(ly) * ly + double(lz) * lz) * (1.0 - 1e-5) -
+                       double(radius_) * (1.0 + 1e-6);
+                e.off = (ax + 16) | ((ay + 16) << 8) | ((az + 16) << 16);
+                e.pad = (ax == 0 && ay == 0 && az == 0) ? 0 : 1;
+                tab.push_back(e);
+            }
+    std::stable_sort(tab.begin(), tab.end(), [](const LphiOffset& a, const LphiOffset& b) {
+        return a.pad != b.pad ? a.pad < b.pad : a.lb < b.lb;
+    });
+    lphi_n_ = int(tab.size());
+    LHI_CUDA(cudaMalloc(&lphi_tab_, sizeof(LphiOffset) * tab.size()));
+    LHI_CUDA(cudaMemcpy(lphi_tab_, tab.data(), sizeof(LphiOffset) * tab.size(), cudaMemcpyHostToDevice));
+}
+
 template <class T, class TX> void LiquidImpl<T, TX>::compute_liquid_phi() {
     if (np_ == 0) return;
     ensure_sorted();
@@ -1221,7 +1328,8 @@ template <class T, class TX> void LiquidImpl<T, TX>::compute_liquid_phi() {
     auto ps_ = scope(LHI_KERNEL_LIQUID_PHI);
     k_liquid_phi<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(gridp(*this), cell_start_, occ_, occ_dim_[0],
                                                                   occ_dim_[1], occ_dim_[2], pdata_[pcur_], pcap_,
-                                                                  radius_, d0, d1, d2, liquid_phi_);
+                                                                  radius_, d0, d1, d2, lphi_tab_, lphi_n_,
+                                                                  liquid_phi_);
     LHI_LAUNCH_CHECK();
 }
 

@@ -1147,6 +1147,13 @@ __device__ void cg_decide(SolveScalars* sc, double res2, const CgConf& cf, bool 
     if (cf.use_cond) cudaGraphSetConditional(cf.cond, stop ? 0u : 1u);
 }
 
+// A loop-body kernel that finds the solve stopped by another kernel (a
+// bounded wait that ran out) ends the graph's while loop: the iteration that
+// set the conditional to continue did so before the stop.
+__device__ __forceinline__ void cg_end_loop(const CgConf& cf) {
+    if (cf.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cf.cond, 0u);
+}
+
 // r0 = rhs on fluid cells (PressureSolver.cpp:847-856)
 template <class T>
 __global__ void __launch_bounds__(kTileThreads) k_cg_init_r(LevelK<T> L, TileK tk, const T* __restrict__ rhs, T* __restrict__ r) {
@@ -1471,7 +1478,10 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_update_xr(LevelK<T> L, Tile
                                                                T* __restrict__ r, double* __restrict__ partials,
                                                                unsigned* __restrict__ counter,
                                                                SolveScalars* __restrict__ sc, CgConf cf) {
-    if (sc->stop) return;
+    if (sc->stop) {
+        cg_end_loop(cf);
+        return;
+    }
     const double alpha = sc->alpha;
     double v[1] = {0.0};
     for_tile_cols(tk, L.nx, L.ny, L.nz, [&](int xi, int zi, long long i0, int yb, int rows, int ys) {
@@ -1525,7 +1535,11 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_true_residual(LevelK<T> L, 
                                                                    double* __restrict__ partials,
                                                                    unsigned* __restrict__ counter,
                                                                    SolveScalars* __restrict__ sc, CgConf cf) {
-    if (sc->stop || !sc->true_now) return;
+    if (sc->stop) {
+        cg_end_loop(cf);
+        return;
+    }
+    if (!sc->true_now) return;
     double v[1] = {0.0};
     true_residual_sweep(L, tk, cf.region, b, x, r, true, v[0]);
     double tot[1];

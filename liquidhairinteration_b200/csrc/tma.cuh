@@ -78,8 +78,10 @@ __device__ __forceinline__ uint64_t timer_ns() {
 constexpr uint64_t kWaitLimitNs = 200000000ull;  // 200 ms
 
 // Waits for the barrier phase of this parity; gives up after limit_ns
-// (200 ms unless the caller passes another limit).
+// (200 ms unless the caller passes another limit).  A limit of 0 gives up
+// at once, without looking at the barrier: the timeout path on demand.
 __device__ __forceinline__ bool bar_wait(uint64_t* bar, unsigned parity, uint64_t limit_ns = kWaitLimitNs) {
+    if (limit_ns == 0) return false;
     const uint32_t addr = smem_addr(bar);
     uint64_t deadline = 0;
     for (;;) {
