@@ -356,7 +356,7 @@ def run_ours(args):
                 "workload": f"{spec.name}: {spec.n}^3 unit-cube dam break ({scene_text(spec)}), {n_particles} "
                             f"particles (8 per cell, seed {spec.seed}), dt {spec.dt:.6g}, one replica per GPU",
                 "solver": f"MGPCG: {solver.num_level} levels, {solver.num_pre_smooth}+{solver.num_post_smooth} "
-                          f"red-black damped Gauss-Seidel (w=1), {solver.num_final_smooth} coarsest sweeps, flexible "
+                          f"red-black damped Gauss-Seidel (w={solver.smoothing_factor:g}), {solver.num_final_smooth} coarsest sweeps, flexible "
                           "CG on every fluid cell, " + PRECISION_TEXT[args.precision] +
                           ", ||r||/||b|| <= 1e-6 on the true residual",
                 "precision": args.precision,

@@ -158,7 +158,8 @@ typedef struct lhi_render_params {
 
 typedef struct lhi_solve_stats {
     int32_t iterations;        /* PCG iterations taken                        */
-    int32_t status;            /* LHI_OK or LHI_E_NOT_CONVERGED / LHI_E_NAN   */
+    int32_t status;            /* LHI_OK or LHI_E_NOT_CONVERGED / LHI_E_NAN /
+                                  LHI_E_TIMEOUT                               */
     double initial_residual;   /* ||r0|| over all cells (PressureSolver.cpp:868) */
     double final_residual;     /* recursive ||r|| over interior fluid cells   */
     double true_residual;      /* ||b - A x|| over interior fluid cells, or -1 */

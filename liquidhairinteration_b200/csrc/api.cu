@@ -237,6 +237,7 @@ LHI_API int lhi_liquid_projection(lhi_liquid* h, double dt) {
     return guarded([&]() -> int {
         int st = h->impl->projection(dt);
         if (st == LHI_E_NAN) return fail(LHI_E_NAN, "pressure solve produced NaN/Inf");
+        if (st == LHI_E_TIMEOUT) return fail(LHI_E_TIMEOUT, "a bounded wait of the solver kernels ran out");
         return LHI_OK;
     });
 }
@@ -251,6 +252,7 @@ LHI_API int lhi_liquid_step(lhi_liquid* h, double dt) {
     return guarded([&]() -> int {
         int st = h->impl->step(dt);
         if (st == LHI_E_NAN) return fail(LHI_E_NAN, "pressure solve produced NaN/Inf");
+        if (st == LHI_E_TIMEOUT) return fail(LHI_E_TIMEOUT, "a bounded wait of the solver kernels ran out");
         return LHI_OK;
     });
 }
@@ -509,6 +511,7 @@ LHI_API int lhi_solver_solve(lhi_liquid* h, double density, double dt, lhi_solve
         if (stats) *stats = h->impl->stats();
         if (st == LHI_E_NAN) return fail(LHI_E_NAN, "pressure solve produced NaN/Inf");
         if (st == LHI_E_NOT_CONVERGED) return fail(LHI_E_NOT_CONVERGED, "pressure solve hit the iteration cap");
+        if (st == LHI_E_TIMEOUT) return fail(LHI_E_TIMEOUT, "a bounded wait of the solver kernels ran out");
         return LHI_OK;
     });
 }

@@ -317,6 +317,7 @@ public:
     // ---- internals shared by the .cu files
     void alloc_particles(int64_t cap);
     void ensure_sorted();
+    void apply_order();
     void build_liquid_phi_table();
     void p2g_accumulate();
     void p2g_normalize(bool with_gravity, T gdt);
@@ -379,6 +380,12 @@ public:
     int pcur_ = 0;
     bool sorted_ = false;
     bool keys_fresh_ = false;  // keys_[0]/vals_[0] hold (cell key, identity) of the current order
+    // The sort's permutation not applied yet: pdata_[pcur_] is in the order
+    // before the sort, vals_[0] maps a sorted index to its place there, and
+    // rows 0-2 of pdata_[pcur_ ^ 1] hold the positions in sorted order.  The
+    // liquid SDF, P2G and G2P + advection read through it (G2P writes the
+    // sorted state, which applies it); anything else applies it first.
+    bool perm_pending_ = false;
     uint32_t* keys_[2] = {nullptr, nullptr};
     int32_t* vals_[2] = {nullptr, nullptr};
     int32_t* cell_count_ = nullptr;  // ncell + 1

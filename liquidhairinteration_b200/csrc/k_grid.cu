@@ -749,6 +749,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::get_field(int f, int level,
         return;
     }
     if (f == LHI_FIELD_PARTICLE_ID) {
+        apply_order();  // the ids in the current (cell-sorted, once sorted) order
         LHI_CUDA(cudaMemcpyAsync(out, pid_[pcur_], count * 4, cudaMemcpyDeviceToHost, stream_));
         LHI_CUDA(cudaStreamSynchronize(stream_));
         return;

@@ -18,6 +18,7 @@ namespace lhi {
 template <class T> struct GridP {
     int nx, ny, nz;
     T mn[3], mx[3], dx[3];
+    T idx[3];  // 1 / dx, for the gathers that need not be bit-exact
 };
 
 template <class T> __device__ __forceinline__ int cell_trunc(T p, T mn, T dx) {
@@ -51,6 +52,18 @@ __global__ void k_permute(const T* __restrict__ src, T* __restrict__ dst, long l
 #pragma unroll
     for (int c = 0; c < 15; ++c) dst[c * cap + k] = src[c * cap + s];
     did[k] = sid[s];
+}
+
+// The sorted positions alone (rows 0-2 of dst): the permutation of the rest
+// waits for G2P, which reads through it and writes the sorted state.
+template <class T>
+__global__ void k_gather_pos(const T* __restrict__ src, T* __restrict__ dst, long long cap,
+                             const int32_t* __restrict__ order, long long n) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    long long s = order[k];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dst[c * cap + k] = src[c * cap + s];
 }
 
 __global__ void k_cell_count(const uint32_t* __restrict__ keys, long long n, int32_t* __restrict__ count) {
@@ -252,6 +265,21 @@ constexpr int kTile = 8;
 __device__ __forceinline__ int off_lo(int d) { return max(-1, -d); }
 __device__ __forceinline__ int off_hi(int i, int a, int d) { return min(i == a ? 2 : 1, d); }
 
+// Quadratic B-spline weights (qweight) and the reference's gradient weights
+// (gqweight) of the three nodes around a middle node at signed distance
+// t = x - node in [-1/2, 1/2] (grid units): the nodes at -1, 0, +1 sit at
+// distances t + 1, t, t - 1, which fall on the outer branch, the inner
+// branch and the outer branch of both functions.
+template <class T> __device__ __forceinline__ void axis_weights(T t, T w[3], T gw[3]) {
+    const T l = T(0.5f) - t, r = T(0.5f) + t;
+    w[0] = T(0.5f) * l * l;
+    w[1] = T(0.75f) - t * t;
+    w[2] = T(0.5f) * r * r;
+    gw[0] = -l;
+    gw[1] = T(-2.f) * fabs(t);
+    gw[2] = -r;
+}
+
 // LiquidModel<3>::Particle2Grid accumulation (LiquidModel.cpp:614-701).
 // One CTA per 8^3-cell tile.  Thread t owns cells t and t + 256 of the tile;
 // for each face component it walks its cell's sorted particles and sums
@@ -302,6 +330,17 @@ __device__ void p2g_particle_global(const GridP<T>& g, const int d[3], const T q
     }
 }
 
+// The cell-sorted particle state as P2G reads it: the positions of sorted
+// index k in pos (rows 0-2, stride cap), the other 12 scalars at row r of
+// rest, index order ? order[k] : k (order: the sort's permutation while it
+// is deferred).
+template <class T> struct PView {
+    const T* pos;
+    const T* rest;
+    const int32_t* order;
+    long long cap;
+};
+
 template <class T> struct P2GOut {
     T* v[3];
     T* w[3];
@@ -311,78 +350,115 @@ __host__ __device__ constexpr int p2g_region(int a) {
     return (kTile + 2 + (a == 0)) * (kTile + 2 + (a == 1)) * (kTile + 2 + (a == 2));
 }
 
-// Staged particle record of the P2G warp loop (values of T):
-//   [0, 12)   wf[a][4]: face weights of component a along its own axis,
-//             window slots -1..2 (node = cell + slot)
-//   [12, 24)  tf[a][4] = C_aa * (x_a - face node a)
-//   [24, 51)  W[l], column l = 9a + 3s + t of the warp loop: the product of
-//             the two cell-centre weights across component a (slot s on its
-//             first other axis, t on the second; node centre = cell + slot + 0.5)
-//   [51, 78)  B[l] = v_a + C_ab (x_b - centre b) + C_ac (x_c - centre c)
-//   [78]      z offset of the particle's cell in its row (bits of an int)
-// A weight outside the reference's window (+-d) or with |e| >= 1.5 is 0.
-// The stride is odd, so the staging lanes' stores fall in distinct banks.
-constexpr int kP2GRec = 79;
+// Staged particle records of the P2G warp loop (values of T), two per
+// particle:
+//   A (kP2GRecA values, 16-byte aligned: the lanes read wf and tf as vectors)
+//     [0, 12)   wf[a][4]: face weights of component a along its own axis,
+//               window slots -1..2 (node = cell + slot)
+//     [12, 24)  tf[a][4] = C_aa * (x_a - face node a)
+//     [24]      z offset of the particle's cell in its row (bits of an int)
+//   B (kP2GRecB values, odd stride: the staging lanes' stores fall in
+//     distinct banks)
+//     [0, 27)   W[l], column l = 9a + 3s + t of the warp loop: the product of
+//               the two cell-centre weights across component a (slot s on its
+//               first other axis, t on the second; node centre = cell + slot + 0.5)
+//     [27, 54)  B[l] = v_a + C_ab (x_b - centre b) + C_ac (x_c - centre c)
+// The weights are the quadratic B-spline's in closed form around the
+// particle's middle node (axis_weights); a node outside the reference's
+// window (+-d) gets 0, as does a node at |e| >= 1.5 by the formula itself.
+constexpr int kP2GRecA = 28;
+constexpr int kP2GRecB = 55;
 constexpr int kP2GWarps = 8;
+constexpr int kP2GChunk = 16;  // particles staged at a time per warp
+constexpr int kP2GStage = kP2GChunk * (kP2GRecA + kP2GRecB);  // values per warp
 
 __device__ __forceinline__ void p2g_other_axes(int a, int& b, int& c) {
     b = (a == 0) ? 1 : 0;
     c = (a == 2) ? 1 : 2;
 }
 
-// Computes the record of one particle (one lane per particle) and returns
+__device__ __forceinline__ void load4(const float* p, float v[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+}
+__device__ __forceinline__ void load4(const double* p, double v[4]) {
+    const double2 t0 = reinterpret_cast<const double2*>(p)[0], t1 = reinterpret_cast<const double2*>(p)[1];
+    v[0] = t0.x;
+    v[1] = t0.y;
+    v[2] = t1.x;
+    v[3] = t1.y;
+}
+__device__ __forceinline__ void store4(float* p, const float v[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double v[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// Computes the records of one particle (one lane per particle) and returns
 // the z offset of its cell in the row, or -1 when its own truncated index
-// (cast<Integer>, LiquidModel.cpp:629) is not the cell it was sorted into
-// (outside the grid, where the sort key is clamped): such a particle is
-// listed for k_p2g_overflow instead.
+// (cast<Integer>, LiquidModel.cpp:629) is not the cell it was sorted into,
+// or its grid coordinate is negative (both only outside the grid, where the
+// sort key is clamped): such a particle is listed for k_p2g_overflow.
 template <class T>
-__device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __restrict__ pd, long long cap,
-                         long long p, int rx, int ry, int z0, int zend, T* rec, int* __restrict__ ov_count,
-                         int32_t* __restrict__ ov_list) {
-    const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
+__device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const PView<T>& pv, long long p, int rx, int ry,
+                         int z0, int zend, T* ra, T* rb, int* __restrict__ ov_count, int32_t* __restrict__ ov_list) {
+    const long long cap = pv.cap;
+    const T q[3] = {pv.pos[p], pv.pos[cap + p], pv.pos[2 * cap + p]};
     T g3[3];
     int ci[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        g3[i] = X<T>::div(X<T>::sub(q[i], g.mn[i]), g.dx[i]);  // cwiseQuotient
-        ci[i] = int(g3[i]);                                     // cast<Integer>
+        // cwiseQuotient as a multiply (P2G equals the reference up to rounding; a particle whose cell then
+        // differs from its sort key's takes the overflow path, which divides)
+        g3[i] = (q[i] - g.mn[i]) * g.idx[i];
+        ci[i] = int(g3[i]);  // cast<Integer>
     }
-    if (ci[0] != rx || ci[1] != ry || ci[2] < z0 || ci[2] >= zend) {
+    if (ci[0] != rx || ci[1] != ry || ci[2] < z0 || ci[2] >= zend ||
+        !(g3[0] >= T(0) && g3[1] >= T(0) && g3[2] >= T(0))) {
         ov_list[atomicAdd(ov_count, 1)] = int32_t(p);
         return -1;
     }
+    const long long ps = pv.order ? (long long)pv.order[p] : p;
     T C[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) C[k] = pd[(6 + k) * cap + p];  // column-major: C[3a + i] = C(i, a)
+    for (int k = 0; k < 9; ++k) C[k] = pv.rest[(6 + k) * cap + ps];  // column-major: C[3a + i] = C(i, a)
+    const int dd[3] = {d0, d1, d2};
     T wc[3][3], tc[3][2][3];  // centre weights per axis; C_ab (x_b - centre) per component and other axis
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        const int di = (i == 0) ? d0 : (i == 1) ? d1 : d2;
         const T cb = T(ci[i]);  // integer grid coordinates are exact in T
+        const T f = g3[i] - cb;  // exact, in [0, 1)
+        const bool up = f >= T(0.5f);
+        T w3[3], gu[3];
+        axis_weights(g3[i] - (up ? cb + T(1) : cb), w3, gu);  // face nodes: middle node = nearest integer
+        T wf[4], tf[4];
 #pragma unroll
-        for (int s2 = 0; s2 < 4; ++s2) {  // face nodes: component i's own axis
+        for (int s2 = 0; s2 < 4; ++s2) {  // slot s2 = offset + 1 from the cell
             const int o = s2 - 1;
-            const T c = X<T>::add(cb, T(o));
-            const T e = X<T>::sub(g3[i], c);
-            const bool ok = o >= -di && o <= di && !(fabs(e) >= T(1.5f));
-            rec[i * 4 + s2] = ok ? qweight(e) : T(0);
-            const T df = X<T>::sub(q[i], X<T>::add(X<T>::mul(c, g.dx[i]), g.mn[i]));
-            rec[12 + i * 4 + s2] = X<T>::mul(C[4 * i], df);  // C(i, i)
+            T wv = up ? (s2 >= 1 ? w3[s2 - 1] : T(0)) : (s2 <= 2 ? w3[s2] : T(0));
+            if (o < -dd[i] || o > dd[i]) wv = T(0);
+            wf[s2] = wv;
+            tf[s2] = C[4 * i] * (q[i] - fma(cb + T(o), g.dx[i], g.mn[i]));  // C(i, i)
         }
+        store4(ra + 4 * i, wf);
+        store4(ra + 12 + 4 * i, tf);
+        axis_weights(f - T(0.5f), wc[i], gu);  // cell-centre nodes: middle node = this cell's centre
 #pragma unroll
-        for (int s2 = 0; s2 < 3; ++s2) {  // cell-centre nodes: the other two components
+        for (int s2 = 0; s2 < 3; ++s2) {
             const int o = s2 - 1;
-            const T c = X<T>::add(X<T>::add(cb, T(o)), T(0.5));
-            const T e = X<T>::sub(g3[i], c);
-            const bool ok = o >= -di && o <= di && !(fabs(e) >= T(1.5f));
-            wc[i][s2] = ok ? qweight(e) : T(0);
-            const T dc = X<T>::sub(q[i], X<T>::add(X<T>::mul(c, g.dx[i]), g.mn[i]));
+            if (o < -dd[i] || o > dd[i]) wc[i][s2] = T(0);
+            const T dc = q[i] - fma(cb + T(o) + T(0.5f), g.dx[i], g.mn[i]);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 if (a == i) continue;
-                int b, c2;
-                p2g_other_axes(a, b, c2);
-                tc[a][b == i ? 0 : 1][s2] = X<T>::mul(C[3 * a + i], dc);
+                int b, c;
+                p2g_other_axes(a, b, c);
+                tc[a][b == i ? 0 : 1][s2] = C[3 * a + i] * dc;
             }
         }
     }
@@ -390,14 +466,14 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __r
     for (int a = 0; a < 3; ++a) {
         int b, c;
         p2g_other_axes(a, b, c);
-        const T va = pd[(3 + a) * cap + p];
+        const T va = pv.rest[(3 + a) * cap + ps];
 #pragma unroll
         for (int s2 = 0; s2 < 3; ++s2)
 #pragma unroll
             for (int t2 = 0; t2 < 3; ++t2) {
                 const int l = 9 * a + 3 * s2 + t2;
-                rec[24 + l] = wc[b][s2] * wc[c][t2];
-                rec[51 + l] = va + tc[a][0][s2] + tc[a][1][t2];
+                rb[l] = wc[b][s2] * wc[c][t2];
+                rb[27 + l] = va + tc[a][0][s2] + tc[a][1][t2];
             }
     }
     return ci[2] - z0;
@@ -407,7 +483,7 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __r
 // One CTA per 8^3-cell tile, shared-memory accumulators for the tile's
 // window nodes of the three face components.  A warp takes whole z rows of
 // the tile: the particles of a row are contiguous in the sorted order.  The
-// row's particles are staged 32 at a time (one lane per particle computes
+// row's particles are staged 16 at a time (one lane per particle computes
 // its per-axis weights and C.(x_p - x_node) terms once, for all three
 // components, and the per-column products below), then the warp walks them
 // in order, two at a time while they share a cell: lane l < 27 owns one
@@ -416,15 +492,14 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const T* __r
 // and APIC values of the current cell's particles in registers.  When the
 // walk reaches the next cell each lane adds its 4 nodes once into the
 // tile's accumulators; at the end every touched node goes to global memory
-// with one add.  The per-axis weights are the reference's, rounded the same
-// way; the per-node products are regrouped and fused and particles are
+// with one add.  The per-axis weights are the reference's B-spline in closed
+// form; the per-node products are regrouped and fused and particles are
 // summed in another order, so P2G matches the reference to rounding, not
 // bit for bit.  No per-particle global atomics.
 template <class T>
-__global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_t* __restrict__ cs,
-                                                        const T* __restrict__ pd, long long cap, int d0, int d1,
-                                                        int d2, P2GOut<T> out, int* __restrict__ ov_count,
-                                                        int32_t* __restrict__ ov_list) {
+__global__ void __launch_bounds__(kP2GWarps * 32, sizeof(T) == 4 ? 3 : 1) k_p2g(GridP<T> g, const int32_t* __restrict__ cs, PView<T> pv,
+                                                        int d0, int d1, int d2, P2GOut<T> out,
+                                                        int* __restrict__ ov_count, int32_t* __restrict__ ov_list) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
     __shared__ int any;
@@ -432,7 +507,9 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
     const int zend = min(z0 + kTile, g.nz);
     const int R0 = p2g_region(0), R1 = p2g_region(1), R2 = p2g_region(2);
     const int ntot = 2 * (R0 + R1 + R2);
-    T* stage = acc + ntot + (threadIdx.x >> 5) * 32 * kP2GRec;
+    static_assert(kP2GStage % 4 == 0 && kP2GRecA % 4 == 0, "records stay 16-byte aligned");
+    T* stA = acc + ntot + (threadIdx.x >> 5) * kP2GStage;  // ntot is a multiple of 4
+    T* stB = stA + kP2GChunk * kP2GRecA;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     if (threadIdx.x < kTile * kTile) {  // row (x0 + t / 8, y0 + t % 8)
@@ -484,37 +561,39 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
                 av[k] = T(0);
             }
         };
-        auto add = [&](const T* r) {
-            const T W = r[24 + lw], B = r[51 + lw];
+        auto add = [&](int j) {
+            T wf[4], tf[4];
+            load4(stA + j * kP2GRecA + 4 * ac, wf);
+            load4(stA + j * kP2GRecA + 12 + 4 * ac, tf);
+            const T W = stB[j * kP2GRecB + lw], B = stB[j * kP2GRecB + 27 + lw];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const T w = W * r[ac * 4 + k];
+                const T w = W * wf[k];
                 aw[k] += w;
-                av[k] = fma(w, B + r[12 + ac * 4 + k], av[k]);
+                av[k] = fma(w, B + tf[k], av[k]);
             }
         };
-        for (int chunk = pbeg; chunk < pend; chunk += 32) {
-            const int n = min(32, pend - chunk);
+        auto zoff = [&](int j) { return reinterpret_cast<const int*>(stA + j * kP2GRecA + 24)[0]; };
+        for (int chunk = pbeg; chunk < pend; chunk += kP2GChunk) {
+            const int n = min(kP2GChunk, pend - chunk);
             __syncwarp();
             if (lane < n) {
-                T* rec = stage + lane * kP2GRec;
-                const int zo = p2g_stage<T>(g, d0, d1, d2, pd, cap, chunk + lane, rx, ry, z0, zend, rec, ov_count,
-                                            ov_list);
-                rec[78] = T(0);
-                reinterpret_cast<int*>(rec + 78)[0] = zo;
+                T* ra = stA + lane * kP2GRecA;
+                const int zo = p2g_stage<T>(g, d0, d1, d2, pv, chunk + lane, rx, ry, z0, zend, ra,
+                                            stB + lane * kP2GRecB, ov_count, ov_list);
+                ra[24] = T(0);
+                reinterpret_cast<int*>(ra + 24)[0] = zo;
             }
             __syncwarp();
             int j = 0;
             while (j < n) {
-                const T* r0 = stage + j * kP2GRec;
-                const int zo0 = reinterpret_cast<const int*>(r0 + 78)[0];
+                const int zo0 = zoff(j);
                 if (j + 1 < n) {
-                    const T* r1 = r0 + kP2GRec;
-                    const int zo1 = reinterpret_cast<const int*>(r1 + 78)[0];
+                    const int zo1 = zoff(j + 1);
                     if (zo0 == cur && zo1 == cur) {  // both in the current cell
                         if (col) {
-                            add(r0);
-                            add(r1);
+                            add(j);
+                            add(j + 1);
                         }
                         j += 2;
                         continue;
@@ -525,7 +604,7 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
                         flush();
                         cur = zo0;
                     }
-                    if (col) add(r0);
+                    if (col) add(j);
                 }
                 ++j;
             }
@@ -558,22 +637,24 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g(GridP<T> g, const int32_
 // The particles k_p2g listed (outside the cell they were sorted into: off
 // the grid) add their windows straight to global memory.
 template <class T>
-__global__ void k_p2g_overflow(GridP<T> g, const T* __restrict__ pd, long long cap, int d0, int d1, int d2,
-                               P2GOut<T> out, const int* __restrict__ ov_count, const int32_t* __restrict__ ov_list) {
+__global__ void k_p2g_overflow(GridP<T> g, PView<T> pv, int d0, int d1, int d2, P2GOut<T> out,
+                               const int* __restrict__ ov_count, const int32_t* __restrict__ ov_list) {
     const int n = *ov_count;
     const int d[3] = {d0, d1, d2};
+    const long long cap = pv.cap;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const long long p = ov_list[i];
-        const T q[3] = {pd[p], pd[cap + p], pd[2 * cap + p]};
+        const long long ps = pv.order ? (long long)pv.order[p] : p;
+        const T q[3] = {pv.pos[p], pv.pos[cap + p], pv.pos[2 * cap + p]};
         T g3[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) g3[k] = X<T>::div(X<T>::sub(q[k], g.mn[k]), g.dx[k]);
         T C[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) C[k] = pd[(6 + k) * cap + p];
-        p2g_particle_global<T, 0>(g, d, q, g3, pd[3 * cap + p], C[0], C[1], C[2], out.w[0], out.v[0]);
-        p2g_particle_global<T, 1>(g, d, q, g3, pd[4 * cap + p], C[3], C[4], C[5], out.w[1], out.v[1]);
-        p2g_particle_global<T, 2>(g, d, q, g3, pd[5 * cap + p], C[6], C[7], C[8], out.w[2], out.v[2]);
+        for (int k = 0; k < 9; ++k) C[k] = pv.rest[(6 + k) * cap + ps];
+        p2g_particle_global<T, 0>(g, d, q, g3, pv.rest[3 * cap + ps], C[0], C[1], C[2], out.w[0], out.v[0]);
+        p2g_particle_global<T, 1>(g, d, q, g3, pv.rest[4 * cap + ps], C[3], C[4], C[5], out.w[1], out.v[1]);
+        p2g_particle_global<T, 2>(g, d, q, g3, pv.rest[5 * cap + ps], C[6], C[7], C[8], out.w[2], out.v[2]);
     }
 }
 
@@ -797,31 +878,17 @@ __device__ __forceinline__ void g2p_component(const GridP<T>& g, const int d[3],
     }
 }
 
-// Quadratic B-spline weights (qweight) and the reference's gradient weights
-// (gqweight) of the three nodes around a middle node at signed distance
-// t = x - node in [-1/2, 1/2] (grid units): the nodes at -1, 0, +1 sit at
-// distances t + 1, t, t - 1, which fall on the outer branch, the inner
-// branch and the outer branch of both functions.
-template <class T> __device__ __forceinline__ void axis_weights(T t, T w[3], T gw[3]) {
-    const T l = T(0.5f) - t, r = T(0.5f) + t;
-    w[0] = T(0.5f) * l * l;
-    w[1] = T(0.75f) - t * t;
-    w[2] = T(0.5f) * r * r;
-    gw[0] = -l;
-    gw[1] = T(-2.f) * fabs(t);
-    gw[2] = -r;
-}
-
 // Factored gather (mixed precision) of a particle whose truncated cell ci
-// lies in the staged tile.  Per axis the particle has one window for face
+// lies in the staged tile, at least one cell away from the grid's faces,
+// with a window of +-2 or more (every window node then exists and lies in
+// the reference's window).  Per axis the particle has one window for face
 // nodes (middle node = the nearest integer coordinate) and one for cell
 // centres (middle node = the centre of ci), each three nodes wide; the
 // weights of both are formed once and shared by the three components (the
-// face window on a component's own axis, the centre window across it).
-// Nodes outside the reference's clipped window (+-d around ci) or the face
-// grid get zero weights; the staged region holds every window node of a
-// particle of the tile (zero outside the grid), so the loads need no test.
-// The same sums as the factored path of g2p_component, up to rounding.
+// face window on a component's own axis, the centre window across it).  The
+// staged region holds every window node of a particle of the tile, so the
+// loads need no test.  The same sums as the factored path of
+// g2p_component, up to rounding.
 template <class T, int A>
 __device__ __forceinline__ void g2p_staged_component(const T wf[3][3], const T gf[3][3], const T wc[3][3],
                                                      const T gc[3][3], const int mf[3], const int ci[3],
@@ -864,7 +931,6 @@ __device__ __forceinline__ void g2p_staged_factored(const GridP<T>& g, const int
                                                     const VSrc<T> src[3], T vel[3], T C[9]) {
     T wf[3][3], gf[3][3], wc[3][3], gc[3][3];
     int mf[3];
-    const int n[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const T f = g3[i] - T(ci[i]);  // exact: g3 and ci are within one unit
@@ -872,18 +938,21 @@ __device__ __forceinline__ void g2p_staged_factored(const GridP<T>& g, const int
         mf[i] = ci[i] + up;
         axis_weights(g3[i] - T(mf[i]), wf[i], gf[i]);
         axis_weights(f - T(0.5f), wc[i], gc[i]);
-        const int lo = off_lo(d[i]);
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const int of = up + j - 1, nf = mf[i] + j - 1;  // face node: offset from ci, index
-            if (of < lo || of > min(2, d[i]) || nf < 0 || nf > n[i]) wf[i][j] = gf[i][j] = T(0);
-            const int nc = ci[i] + j - 1;  // centre node (offset j - 1)
-            if (j - 1 < lo || j - 1 > min(1, d[i]) || nc < 0 || nc > n[i] - 1) wc[i][j] = gc[i][j] = T(0);
-        }
     }
     g2p_staged_component<T, 0>(wf, gf, wc, gc, mf, ci, src[0], vel[0], &C[0]);
     g2p_staged_component<T, 1>(wf, gf, wc, gc, mf, ci, src[1], vel[1], &C[3]);
     g2p_staged_component<T, 2>(wf, gf, wc, gc, mf, ci, src[2], vel[2], &C[6]);
+}
+
+// The factored gather of the particles the staged closed-form path does not
+// take (near the grid's faces, off the tile, or a window below +-2), kept
+// out of line so that its registers do not weigh on the common path.
+template <class T>
+__device__ __noinline__ void g2p_general_factored(const GridP<T>& g, const int d[3], const T g3[3], const int ci[3],
+                                                  const VSrc<T> src[3], T vel[3], T C[9]) {
+    g2p_component<T, 0, true>(g, d, g3, ci, src[0], vel[0], &C[0]);
+    g2p_component<T, 1, true>(g, d, g3, ci, src[1], vel[1], &C[3]);
+    g2p_component<T, 2, true>(g, d, g3, ci, src[2], vel[2], &C[6]);
 }
 
 // One particle of LiquidModel<3>::Grid2Particle (LiquidModel.cpp:724-823)
@@ -896,14 +965,16 @@ __device__ __forceinline__ void g2p_particle(const GridP<T>& g, T* __restrict__ 
                                              const int d[3], int do_g2p, int do_advect, T dt,
                                              const T* __restrict__ sp, uint32_t* __restrict__ keys,
                                              int32_t* __restrict__ vals, PickSrc pick) {
-    T q[3] = {pd[i], pd[cap + i], pd[2 * cap + i]};
+    T q[3] = {pd[i], pd[cap + i], pd[2 * cap + i]};  // (the positions are rows 0-2 of pd also while the sort's
+                                                     // permutation waits: pd is then the sorted buffer)
     T vel[3];
     if (do_g2p) {
         T g3[3];
         int ci[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            g3[k] = X<T>::div(X<T>::sub(q[k], g.mn[k]), g.dx[k]);
+            // the factored sums equal the reference's up to rounding anyway: a multiply for the divide
+            g3[k] = FACTORED ? (q[k] - g.mn[k]) * g.idx[k] : X<T>::div(X<T>::sub(q[k], g.mn[k]), g.dx[k]);
             ci[k] = int(g3[k]);
         }
         T C[9];
@@ -912,9 +983,14 @@ __device__ __forceinline__ void g2p_particle(const GridP<T>& g, T* __restrict__ 
         for (int k = 0; k < 9; ++k) C[k] = T(0);
         VSrc<T> src[3];
         const bool staged = pick(ci, src);
-        // (g3 >= 0: ci is then the floor, as the staged windows assume)
-        if (FACTORED && staged && g3[0] >= T(0) && g3[1] >= T(0) && g3[2] >= T(0)) {
+        // the staged closed-form path: ci >= 1 (so g3 >= 0 and ci is the floor) and ci <= n - 2 on every
+        // axis with a window of +-2 or more; anything else takes the general path
+        const bool full = d[0] >= 2 && d[1] >= 2 && d[2] >= 2 && ci[0] >= 1 && ci[0] <= g.nx - 2 && ci[1] >= 1 &&
+                          ci[1] <= g.ny - 2 && ci[2] >= 1 && ci[2] <= g.nz - 2;
+        if (FACTORED && staged && full) {
             g2p_staged_factored<T>(g, d, g3, ci, src, vel, C);
+        } else if constexpr (FACTORED) {
+            g2p_general_factored<T>(g, d, g3, ci, src, vel, C);  // out of line: the rare particles
         } else {
             g2p_component<T, 0, FACTORED>(g, d, g3, ci, src[0], vel[0], &C[0]);
             g2p_component<T, 1, FACTORED>(g, d, g3, ci, src[1], vel[1], &C[3]);
@@ -981,7 +1057,8 @@ __global__ void __launch_bounds__(256, 3) k_g2p_tile(GridP<T> g, T* __restrict__
                                                   const int32_t* __restrict__ cs, int d0, int d1, int d2,
                                                   const T* __restrict__ vx, const T* __restrict__ vy,
                                                   const T* __restrict__ vz, T dt, const T* __restrict__ sp,
-                                                  uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+                                                  uint32_t* __restrict__ keys, int32_t* __restrict__ vals,
+                                                  const int32_t* __restrict__ pid_src, int32_t* __restrict__ pid_dst) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sv = reinterpret_cast<T*>(smem_raw);
     __shared__ int roff[kTile * kTile + 1];
@@ -1034,6 +1111,8 @@ __global__ void __launch_bounds__(256, 3) k_g2p_tile(GridP<T> g, T* __restrict__
             else hi = mid;
         }
         const long long i = rbeg[lo] + (f - roff[lo]);
+        // the deferred permutation: vals holds it and gets the identity below
+        if (pid_src) pid_dst[i] = pid_src[vals[i]];
         g2p_particle<T, FACTORED>(g, pd, cap, i, d, 1, 1, dt, sp, keys, vals, [&](const int* ci, VSrc<T> src[3]) {
             const bool in = ci[0] >= x0 && ci[0] < x0 + kTile && ci[1] >= y0 && ci[1] < y0 + kTile && ci[2] >= z0 &&
                             ci[2] < zend;
@@ -1192,6 +1271,7 @@ template <class T, class TX> static GridP<T> gridp(const LiquidImpl<T, TX>& s) {
         g.mn[i] = s.min_[i];
         g.mx[i] = s.max_[i];
         g.dx[i] = s.dx_[i];
+        g.idx[i] = T(1) / s.dx_[i];
     }
     return g;
 }
@@ -1212,6 +1292,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::alloc_particles(int64_t cap
     }
     pcap_ = cap;
     pcur_ = 0;
+    perm_pending_ = false;
 }
 
 template <class T, class TX>
@@ -1221,6 +1302,7 @@ void LiquidImpl<T, TX>::set_particles(int64_t n, const void* pos, const void* ve
     alloc_particles(std::max<int64_t>(n, 1));
     np_ = n;
     sorted_ = false;
+    perm_pending_ = false;
     if (n == 0) return;
     T* stage = pdata_[pcur_ ^ 1];  // AoS staging: pos[3n] vel[3n] aff[9n]
     LHI_CUDA(cudaMemcpyAsync(stage, pos, sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
@@ -1234,6 +1316,7 @@ void LiquidImpl<T, TX>::set_particles(int64_t n, const void* pos, const void* ve
 
 template <class T, class TX> void LiquidImpl<T, TX>::get_particles(void* pos, void* vel, void* aff) {
     if (np_ == 0) return;
+    apply_order();  // its staging buffer is the other one
     T* stage = pdata_[pcur_ ^ 1];
     k_soa_to_aos<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pcap_, pid_[pcur_], stage, np_);
     LHI_LAUNCH_CHECK();
@@ -1247,6 +1330,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::get_particles(void* pos, vo
 // keys of the current positions are already in keys_[0]/vals_[0] (written by
 // set_particles or by the advection kernel).
 template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
+    apply_order();  // the keys below are those of the physical order
     auto ps_ = scope(LHI_KERNEL_SORT);
     if (np_ > 0) {
         if (!keys_fresh_) {
@@ -1271,12 +1355,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
         LHI_LAUNCH_CHECK();
         k_cell_order<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, ncell_, pid_[pcur_], vals_[1]);
         LHI_LAUNCH_CHECK();
-        k_permute<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_,
-                                                                pid_[pcur_], pid_[pcur_ ^ 1], vals_[1], np_);
+        // only the positions move now (the liquid SDF walks them); P2G reads
+        // the rest through the permutation and G2P writes the sorted state
+        k_gather_pos<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_,
+                                                                   vals_[1], np_);
         LHI_LAUNCH_CHECK();
-        pcur_ ^= 1;
         std::swap(keys_[0], keys_[1]);  // the sorted keys in keys_[0]
-        std::swap(vals_[0], vals_[1]);
+        std::swap(vals_[0], vals_[1]);  // the permutation in vals_[0]
+        perm_pending_ = true;
     }
     LHI_CUDA(cudaMemsetAsync(occ_, 0, size_t(occ_dim_[0]) * occ_dim_[1] * occ_dim_[2], stream_));
     k_occupancy<<<blocks_for(ncell_, 256), 256, 0, stream_>>>(cell_start_, nx_, ny_, nz_, occ_, occ_dim_[0],
@@ -1288,6 +1374,18 @@ template <class T, class TX> void LiquidImpl<T, TX>::sort_particles() {
 
 template <class T, class TX> void LiquidImpl<T, TX>::ensure_sorted() {
     if (!sorted_) sort_particles();
+}
+
+// Applies a deferred permutation: the whole state (and the ids) in sorted order.
+template <class T, class TX> void LiquidImpl<T, TX>::apply_order() {
+    if (!perm_pending_) return;
+    perm_pending_ = false;
+    if (np_ == 0) return;
+    auto ps_ = scope(LHI_KERNEL_SORT);
+    k_permute<T><<<blocks_for(np_, 256), 256, 0, stream_>>>(pdata_[pcur_], pdata_[pcur_ ^ 1], pcap_, pid_[pcur_],
+                                                            pid_[pcur_ ^ 1], vals_[0], np_);
+    LHI_LAUNCH_CHECK();
+    pcur_ ^= 1;
 }
 
 // The window offsets of k_liquid_phi with their distance bounds: a window
@@ -1327,7 +1425,8 @@ template <class T, class TX> void LiquidImpl<T, TX>::compute_liquid_phi() {
     if (d0 > 8 || d1 > 8 || d2 > 8) throw std::invalid_argument("particle radius above 8 cells is not supported");
     auto ps_ = scope(LHI_KERNEL_LIQUID_PHI);
     k_liquid_phi<T><<<blocks_for(ncell_, 256), 256, 0, stream_>>>(gridp(*this), cell_start_, occ_, occ_dim_[0],
-                                                                  occ_dim_[1], occ_dim_[2], pdata_[pcur_], pcap_,
+                                                                  occ_dim_[1], occ_dim_[2],
+                                                                  pdata_[perm_pending_ ? pcur_ ^ 1 : pcur_], pcap_,
                                                                   radius_, d0, d1, d2, lphi_tab_, lphi_n_,
                                                                   liquid_phi_);
     LHI_LAUNCH_CHECK();
@@ -1342,19 +1441,23 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_accumulate() {
         out.v[a] = v_[a];
         out.w[a] = w_[a];
     }
-    // tile accumulators, then one 32-particle staging buffer per warp
-    size_t smem = sizeof(T) * (2 * (p2g_region(0) + p2g_region(1) + p2g_region(2)) + kP2GWarps * 32 * kP2GRec);
+    // tile accumulators, then one staging buffer per warp (small enough for three CTAs per SM)
+    size_t smem = sizeof(T) * (2 * (p2g_region(0) + p2g_region(1) + p2g_region(2)) + kP2GWarps * kP2GStage);
     LHI_CUDA(cudaFuncSetAttribute(k_p2g<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid(unsigned((nz_ + kTile - 1) / kTile), unsigned((ny_ + kTile - 1) / kTile),
               unsigned((nx_ + kTile - 1) / kTile));
     // particles off the grid are listed (in vals_[1], free after the sort) for k_p2g_overflow
     int* ov_count = &sc_->p2g_overflow;
     LHI_CUDA(cudaMemsetAsync(ov_count, 0, sizeof(int), stream_));
-    k_p2g<T><<<grid, kP2GWarps * 32, smem, stream_>>>(gridp(*this), cell_start_, pdata_[pcur_], pcap_, d0, d1, d2,
-                                                       out, ov_count, vals_[1]);
+    PView<T> pv;
+    pv.pos = pdata_[perm_pending_ ? pcur_ ^ 1 : pcur_];
+    pv.rest = pdata_[pcur_];
+    pv.order = perm_pending_ ? vals_[0] : nullptr;
+    pv.cap = pcap_;
+    k_p2g<T><<<grid, kP2GWarps * 32, smem, stream_>>>(gridp(*this), cell_start_, pv, d0, d1, d2, out, ov_count,
+                                                       vals_[1]);
     LHI_LAUNCH_CHECK();
-    k_p2g_overflow<T><<<kSMs, 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, d0, d1, d2, out, ov_count,
-                                                 vals_[1]);
+    k_p2g_overflow<T><<<kSMs, 256, 0, stream_>>>(gridp(*this), pv, d0, d1, d2, out, ov_count, vals_[1]);
     LHI_LAUNCH_CHECK();
 }
 
@@ -1371,6 +1474,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::p2g_normalize(bool with_gra
 template <class T, class TX> void LiquidImpl<T, TX>::correct_volume(double dt) {
     if (np_ == 0) return;
     ensure_sorted();  // cell lists of the current positions
+    apply_order();
     auto ps_ = scope(LHI_KERNEL_G2P);
     // weightFactor = sqrt(dx.x * dx.y * dx.z) (LiquidModel.cpp:1089)
     const T wfac = std::sqrt(dx_[0] * dx_[1] * dx_[2]);
@@ -1408,9 +1512,18 @@ template <class T, class TX> void LiquidImpl<T, TX>::g2p(bool do_advect, T dt) {
         dim3 grid(unsigned((nz_ + kTile - 1) / kTile), unsigned((ny_ + kTile - 1) / kTile),
                   unsigned((nx_ + kTile - 1) / kTile));
         auto kern = fact ? k_g2p_tile<T, true> : k_g2p_tile<T, false>;
-        kern<<<grid, 256, smem, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, cell_start_, d0, d1, d2, v_[0], v_[1],
-                                           v_[2], dt, solid_phi_, keys_[0], vals_[0]);
+        // with the sort's permutation deferred the kernel writes the sorted state into the other buffer
+        // (whose positions are already sorted) and carries the ids over
+        const bool defer = perm_pending_;
+        kern<<<grid, 256, smem, stream_>>>(gridp(*this), pdata_[defer ? pcur_ ^ 1 : pcur_], pcap_, cell_start_, d0,
+                                           d1, d2, v_[0], v_[1], v_[2], dt, solid_phi_, keys_[0], vals_[0],
+                                           defer ? pid_[pcur_] : nullptr, defer ? pid_[pcur_ ^ 1] : nullptr);
+        if (defer) {
+            pcur_ ^= 1;
+            perm_pending_ = false;
+        }
     } else {
+        apply_order();
         auto kern = fact ? k_g2p<T, true> : k_g2p<T, false>;
         kern<<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2, v_[0],
                                                         v_[1], v_[2], 1, 0, dt, solid_phi_, keys_[0], vals_[0]);
@@ -1426,6 +1539,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::grid_to_particle() { g2p(fa
 
 template <class T, class TX> void LiquidImpl<T, TX>::advect(double dt) {
     if (np_ == 0) return;
+    apply_order();
     int d0 = window(radius_, dx_[0]), d1 = window(radius_, dx_[1]), d2 = window(radius_, dx_[2]);
     auto ps_ = scope(LHI_KERNEL_G2P);
     k_g2p<T, false><<<blocks_for(np_, 256), 256, 0, stream_>>>(gridp(*this), pdata_[pcur_], pcap_, np_, d0, d1, d2,
