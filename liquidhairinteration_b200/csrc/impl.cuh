@@ -265,6 +265,7 @@ public:
     int projection(double dt) override;
     void velocity_update(double dt) override;
     void extrapolate() override;
+    void build_extrapolation_lists();
     void grid_to_particle() override;
     void advect(double dt) override;
     int pre_step(double dt) override;
@@ -368,6 +369,15 @@ public:
     T* liquid_phi_ = nullptr;
     T* solid_phi_ = nullptr;
     uint8_t* valid_ = nullptr;  // isValid: 255 invalid, else the sweep it became valid
+    // Extrapolation work lists per component (isValid node indices), rebuilt
+    // after the solid fractions or isValid change: ext_u_ the nodes of the
+    // component's range that some component's init can make invalid (the
+    // only ones whose flag can differ from 0 there), ext_s_ those the
+    // component's own init makes invalid (the only ones its sweeps change).
+    int32_t* ext_u_[3] = {};
+    int32_t* ext_s_[3] = {};
+    long long ext_nu_[3] = {}, ext_ns_[3] = {};
+    bool ext_dirty_ = true;
     uint8_t* occ_ = nullptr;    // 4^3-cell block occupancy for the liquid SDF
     int occ_dim_[3];
     LphiOffset* lphi_tab_ = nullptr;  // the liquid SDF's window offsets by ascending distance bound

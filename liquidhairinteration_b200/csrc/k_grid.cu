@@ -230,6 +230,103 @@ __global__ void k_extrap_finish(ExtRange r, uint8_t* __restrict__ valid) {
     }
 }
 
+// The same three stages over a list of isValid nodes of the range (the
+// nodes whose flag can be other than 0 there; every other node of the
+// range holds 0 before and after, so skipping it changes nothing).
+__device__ __forceinline__ void ext_node(const ExtRange& r, int32_t vi, int& x, int& y, int& z) {
+    const int yz = r.ny1 * r.nz1;
+    x = vi / yz;
+    const int rem = vi - x * yz;
+    y = rem / r.nz1;
+    z = rem - y * r.nz1;
+}
+
+template <class T>
+__global__ void k_extrap_init_l(ExtRange r, const int32_t* __restrict__ list, long long n, const T* __restrict__ lw,
+                                uint8_t* __restrict__ valid) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    ext_node(r, list[i], x, y, z);
+    valid[list[i]] = (lw[((long long)x * r.fy + y) * r.fz + z] > T(0)) ? 0 : 255;
+}
+
+// In place (sweeps before the ones through tempV), as k_extrap_sweep with t == v.
+template <class T>
+__global__ void k_extrap_sweep_l(ExtRange r, const int32_t* __restrict__ list, long long n, int k, T* v,
+                                 uint8_t* __restrict__ valid) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t vi = list[i];
+    if (valid[vi] <= k) return;
+    int x, y, z;
+    ext_node(r, vi, x, y, z);
+    T sum = T(0);
+    int count = 0;
+    for (int a = -1; a <= 1; ++a)
+        for (int b = -1; b <= 1; ++b)
+            for (int c = -1; c <= 1; ++c) {
+                long long nv = ((long long)(x + a) * r.ny1 + (y + b)) * r.nz1 + (z + c);
+                if (valid[nv] <= k) {
+                    sum = X<T>::add(sum, v[((long long)(x + a) * r.fy + (y + b)) * r.fz + (z + c)]);
+                    ++count;
+                }
+            }
+    if (count > 0) {
+        v[((long long)x * r.fy + y) * r.fz + z] = X<T>::div(sum, T(count));
+        valid[vi] = uint8_t(k + 1);
+    }
+}
+
+__global__ void k_extrap_finish_l(const int32_t* __restrict__ list, long long n, uint8_t* __restrict__ valid) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t v = valid[list[i]];
+    valid[list[i]] = (v == 255) ? 255 : 0;
+}
+
+// Builds the lists: node (x, y, z) of component a's range goes to U_a when
+// some component b has it in its range with liquidW_b = 0 there, and to S_a
+// when component a does.  count_only: counts alone.
+struct ExtRanges {
+    ExtRange r[3];
+};
+__device__ __forceinline__ bool ext_in(const ExtRange& r, int x, int y, int z) {
+    return x >= r.x0 && x <= r.x1 && y >= r.y0 && y <= r.y1 && z >= r.z0 && z <= r.z1;
+}
+template <class T>
+__global__ void k_extrap_lists(ExtRanges rs, long long nnode, const T* __restrict__ lw0, const T* __restrict__ lw1,
+                               const T* __restrict__ lw2, unsigned long long* __restrict__ counts,
+                               int32_t* __restrict__ u0, int32_t* __restrict__ u1, int32_t* __restrict__ u2,
+                               int32_t* __restrict__ s0, int32_t* __restrict__ s1, int32_t* __restrict__ s2) {
+    const long long vi = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (vi >= nnode) return;
+    int x, y, z;
+    ext_node(rs.r[0], int32_t(vi), x, y, z);
+    const T* lw[3] = {lw0, lw1, lw2};
+    int32_t* u[3] = {u0, u1, u2};
+    int32_t* sl[3] = {s0, s1, s2};
+    bool in[3], solid[3], any = false;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const ExtRange& r = rs.r[b];
+        in[b] = ext_in(r, x, y, z);
+        solid[b] = in[b] && !(lw[b][((long long)x * r.fy + y) * r.fz + z] > T(0));
+        any |= solid[b];
+    }
+    if (!any) return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (!in[a]) continue;
+        const unsigned long long iu = atomicAdd(&counts[a], 1ull);
+        if (u[a]) u[a][iu] = int32_t(vi);
+        if (solid[a]) {
+            const unsigned long long is = atomicAdd(&counts[3 + a], 1ull);
+            if (sl[a]) sl[a][is] = int32_t(vi);
+        }
+    }
+}
+
 // LiquidModel<3>::ComputeDivergence (LiquidModel.cpp:1066-1083): per fluid
 // cell divergence in Scalar, summed in double together with the cell count.
 template <class T>
@@ -469,6 +566,10 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
     F(liquid_phi_);
     F(solid_phi_);
     F(valid_);
+    for (int a = 0; a < 3; ++a) {
+        F(ext_u_[a]);
+        F(ext_s_[a]);
+    }
     F(occ_);
     F(lphi_tab_);
     F(cell_count_);
@@ -535,6 +636,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::clear() {
 
 template <class T, class TX> void LiquidImpl<T, TX>::set_boundary(const BoundaryProgram& prog) {
     solid_cell_fresh_ = false;
+    ext_dirty_ = true;
     G3<T> g{nx_, ny_, nz_, {min_[0], min_[1], min_[2]}, {dx_[0], dx_[1], dx_[2]}};
     k_boundary<T><<<blocks_for(nnode_, 256), 256, 0, stream_>>>(prog, g, solid_phi_);
     LHI_LAUNCH_CHECK();
@@ -546,6 +648,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::set_boundary(const Boundary
 
 template <class T, class TX> void LiquidImpl<T, TX>::set_solid_phi(const void* host) {
     solid_cell_fresh_ = false;
+    ext_dirty_ = true;
     LHI_CUDA(cudaMemcpyAsync(solid_phi_, host, sizeof(T) * nnode_, cudaMemcpyHostToDevice, stream_));
     for (int a = 0; a < 3; ++a) {
         k_face_fractions<T><<<blocks_for(nface_[a], 256), 256, 0, stream_>>>(solid_phi_, nx_, ny_, nz_, a, lw_[a]);
@@ -579,24 +682,68 @@ template <class T, class TX> int LiquidImpl<T, TX>::projection(double dt) {
     return st;
 }
 
+// The extrapolation range of face component a (LiquidModel.cpp:949-953).
+static ExtRange ext_range(int a, int nx, int ny, int nz) {
+    ExtRange r;
+    r.x0 = 1;
+    r.x1 = (a == 0) ? nx - 1 : nx - 2;
+    r.y0 = 1;
+    r.y1 = (a == 1) ? ny - 1 : ny - 2;
+    r.z0 = 1;
+    r.z1 = (a == 2) ? nz - 1 : nz - 2;
+    r.fy = ny + (a == 1);
+    r.fz = nz + (a == 2);
+    r.ny1 = ny + 1;
+    r.nz1 = nz + 1;
+    return r;
+}
+
+template <class T, class TX> void LiquidImpl<T, TX>::build_extrapolation_lists() {
+    ExtRanges rs;
+    for (int a = 0; a < 3; ++a) {
+        rs.r[a] = ext_range(a, nx_, ny_, nz_);
+        if (ext_u_[a]) cudaFree(ext_u_[a]);
+        if (ext_s_[a]) cudaFree(ext_s_[a]);
+        ext_u_[a] = ext_s_[a] = nullptr;
+    }
+    unsigned long long* counts = reinterpret_cast<unsigned long long*>(partials_);  // 6 counters, scratch
+    unsigned long long hc[6];
+    for (int pass = 0; pass < 2; ++pass) {
+        LHI_CUDA(cudaMemsetAsync(counts, 0, sizeof(hc), stream_));
+        k_extrap_lists<T><<<blocks_for(nnode_, 256), 256, 0, stream_>>>(rs, nnode_, lw_[0], lw_[1], lw_[2], counts,
+                                                                       ext_u_[0], ext_u_[1], ext_u_[2], ext_s_[0],
+                                                                       ext_s_[1], ext_s_[2]);
+        LHI_LAUNCH_CHECK();
+        LHI_CUDA(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, stream_));
+        LHI_CUDA(cudaStreamSynchronize(stream_));
+        if (pass == 1) break;
+        for (int a = 0; a < 3; ++a) {  // first pass counted: allocate, then fill
+            ext_nu_[a] = (long long)hc[a];
+            ext_ns_[a] = (long long)hc[3 + a];
+            LHI_CUDA(cudaMalloc(&ext_u_[a], sizeof(int32_t) * size_t(std::max(ext_nu_[a], 1LL))));
+            LHI_CUDA(cudaMalloc(&ext_s_[a], sizeof(int32_t) * size_t(std::max(ext_ns_[a], 1LL))));
+        }
+    }
+    ext_dirty_ = false;
+}
+
+// LiquidModel<3>::Extrapolate.  After the first call (or a change of the
+// solid fractions or of isValid, which run the full passes again) the init,
+// the in-place sweeps and the finish walk the node lists; the sweeps through
+// tempV keep their full pass, which also copies every face of the range.
 template <class T, class TX> void LiquidImpl<T, TX>::extrapolate() {
     if (np_ == 0) return;
     auto ps_ = scope(LHI_KERNEL_EXTRAPOLATE);
+    const bool full = ext_dirty_;
     for (int a = 0; a < 3; ++a) {
-        ExtRange r;
-        r.x0 = 1;
-        r.x1 = (a == 0) ? nx_ - 1 : nx_ - 2;
-        r.y0 = 1;
-        r.y1 = (a == 1) ? ny_ - 1 : ny_ - 2;
-        r.z0 = 1;
-        r.z1 = (a == 2) ? nz_ - 1 : nz_ - 2;
-        r.fy = ny_ + (a == 1);
-        r.fz = nz_ + (a == 2);
-        r.ny1 = ny_ + 1;
-        r.nz1 = nz_ + 1;
+        const ExtRange r = ext_range(a, nx_, ny_, nz_);
         const long long n = ext_threads(r);  // 4 faces along z per thread
-        if (n > 0) {
+        if (full && n > 0) {
             k_extrap_init<T><<<blocks_for(n, 256), 256, 0, stream_>>>(r, lw_[a], valid_);
+            LHI_LAUNCH_CHECK();
+        } else if (ext_nu_[a] > 0) {
+            k_extrap_init_l<T><<<blocks_for(ext_nu_[a], 256), 256, 0, stream_>>>(r, ext_u_[a], ext_nu_[a], lw_[a],
+                                                                                 valid_);
             LHI_LAUNCH_CHECK();
         }
         // The reference sweeps into tempV and swaps (std::swap(m_grid.tempVx,
@@ -608,6 +755,14 @@ template <class T, class TX> void LiquidImpl<T, TX>::extrapolate() {
         const int jacobi_from = extrap_iters_ - ((extrap_iters_ % 2) ? 1 : 2);
         for (int k = 0; k < extrap_iters_; ++k) {
             const bool swap = k >= jacobi_from;
+            if (!full && !swap) {
+                if (ext_ns_[a] > 0) {
+                    k_extrap_sweep_l<T><<<blocks_for(ext_ns_[a], 256), 256, 0, stream_>>>(r, ext_s_[a], ext_ns_[a], k,
+                                                                                         v_[a], valid_);
+                    LHI_LAUNCH_CHECK();
+                }
+                continue;
+            }
             if (n > 0) {
                 k_extrap_sweep<T><<<blocks_for(n, 256), 256, 0, stream_>>>(r, k, v_[a], swap ? tv_[a] : v_[a],
                                                                          valid_);
@@ -615,11 +770,15 @@ template <class T, class TX> void LiquidImpl<T, TX>::extrapolate() {
             }
             if (swap) std::swap(v_[a], tv_[a]);
         }
-        if (n > 0) {
+        if (full && n > 0) {
             k_extrap_finish<<<blocks_for(n, 256), 256, 0, stream_>>>(r, valid_);
+            LHI_LAUNCH_CHECK();
+        } else if (ext_ns_[a] > 0) {
+            k_extrap_finish_l<<<blocks_for(ext_ns_[a], 256), 256, 0, stream_>>>(ext_s_[a], ext_ns_[a], valid_);
             LHI_LAUNCH_CHECK();
         }
     }
+    if (full) build_extrapolation_lists();
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::divergence(double* mean, double* max_abs) {
@@ -779,6 +938,9 @@ template <class T, class TX> void LiquidImpl<T, TX>::set_field(int f, int level,
     if (f == LHI_FIELD_CELL_KEY || f == LHI_FIELD_PARTICLE_ID || f == LHI_FIELD_CELL_START ||
         f == LHI_FIELD_ACOEF)
         throw std::invalid_argument("field is read-only");
+    if (f == LHI_FIELD_IS_VALID || f == LHI_FIELD_LIQUID_WX || f == LHI_FIELD_LIQUID_WY ||
+        f == LHI_FIELD_LIQUID_WZ)
+        ext_dirty_ = true;  // the extrapolation's node lists follow these
     if (f == LHI_FIELD_IS_VALID) {
         std::vector<uint8_t> tmp(count);
         const uint8_t* p = static_cast<const uint8_t*>(in);

@@ -318,8 +318,12 @@ def test_velocity_update_bitwise(oracle_mod, lhi, prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
-def test_extrapolate_bitwise(oracle_mod, lhi, prec):
-    spec = scenes.dam(16)
+@pytest.mark.parametrize("scene", ["dam", "obstacle"])
+def test_extrapolate_bitwise(oracle_mod, lhi, prec, scene):
+    """Three passes: the first runs the full passes and builds the node
+    lists, the later ones walk the lists and see the earlier passes'
+    persistent flags."""
+    spec = scenes.dam(16) if scene == "dam" else obstacle_scene(16)
     o = _oracle_after_p2g(oracle_mod, spec, prec)
     g, _ = pair(oracle_mod, spec, prec)
     g.clear()
@@ -328,7 +332,7 @@ def test_extrapolate_bitwise(oracle_mod, lhi, prec):
         v = rng.standard_normal(o.field(f).size).astype(g.dtype)
         o.set_field(f, v)
         g.set_field(f, v)
-    for _ in range(2):  # the second pass sees the first's persistent flags
+    for _ in range(3):
         o.extrapolate(oracle_mod.EXTRAP_JACOBI)
         g.Extrapolate()
         for f in ("vx", "vy", "vz", "tempVx", "tempVy", "tempVz"):
