@@ -13,6 +13,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "lhi.h"
 #include "net.cuh"
@@ -162,15 +164,29 @@ struct Profiler {
     }
 };
 
+// Names of the LHI_KERNEL_* categories, as the NVTX ranges of the stages
+// carry them (a profiler that records NVTX, such as Nsight Systems, shows
+// each stage of a step under its name; without one the ranges cost nothing).
+inline const char* kernel_category_name(int cat) {
+    static const char* names[LHI_KERNEL_COUNT] = {"sort",          "liquid_phi", "p2g",     "g2p",     "extrapolate",
+                                                  "grid",          "lhs",        "smooth_fine", "smooth_coarse",
+                                                  "restrict",      "prolong",    "spmv",    "cg_vector"};
+    return (cat >= 0 && cat < LHI_KERNEL_COUNT) ? names[cat] : "lhi";
+}
+
 class ProfScope {
 public:
     ProfScope(Profiler& p, cudaStream_t s, int cat) : p_(p), s_(s), cat_(cat) {
+        nvtxRangePushA(kernel_category_name(cat));
         if (p_.on) {
             a_ = p_.get();
             LHI_CUDA(cudaEventRecord(a_, s_));
         }
     }
+    ProfScope(const ProfScope&) = delete;
+    ProfScope& operator=(const ProfScope&) = delete;
     ~ProfScope() {
+        nvtxRangePop();
         if (!a_) return;
         cudaEvent_t b = nullptr;
         if (cudaEventCreate(&b) != cudaSuccess) return;
