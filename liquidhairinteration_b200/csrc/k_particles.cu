@@ -98,12 +98,65 @@ __global__ void k_rank_scatter(const uint32_t* __restrict__ keys, long long n, c
     order[pos] = int32_t(i);
 }
 
-// Orders every cell's particles by particle ID (insertion sort for the usual
-// handful, nearly in order already since most particles stay in their cell;
-// heap sort for a crowded cell).  The sorted order is then the stable sort
+// Orders every cell's particles by particle ID (a sorting network in
+// registers for up to 16, insertion sort up to 64, heap sort beyond).  The sorted order is then the stable sort
 // of the caller's order by cell key whatever order the device held before,
 // so every walk of the sorted lists (P2G's per-cell sums, CorrectVolume's
 // neighbour sums) visits the particles in an order fixed by their state.
+// Compare-exchange of (key, value) pairs: the smaller key first.
+__device__ __forceinline__ void ce(int32_t& ka, int32_t& kb, int32_t& va, int32_t& vb) {
+    const bool sw = ka > kb;
+    const int32_t k0 = sw ? kb : ka, k1 = sw ? ka : kb, v0 = sw ? vb : va, v1 = sw ? va : vb;
+    ka = k0;
+    kb = k1;
+    va = v0;
+    vb = v1;
+}
+
+// A cell's indices sorted by particle id in registers: all loads issued at
+// once, then Batcher's odd-even merge sort network (Batcher 1968) for 8 or
+// 16 keys (19 / 63 compare-exchanges, checked exhaustively by the 0-1
+// principle); the ids are distinct and the padding sorts last.
+template <int N>
+__device__ __forceinline__ void cell_order_net(int32_t* a, int len, const int32_t* __restrict__ pid) {
+    int32_t v[N], k[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = i < len ? a[i] : 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) k[i] = i < len ? pid[v[i]] : 0x7fffffff;
+    if constexpr (N == 8) {
+        ce(k[0], k[1], v[0], v[1]); ce(k[2], k[3], v[2], v[3]); ce(k[0], k[2], v[0], v[2]); ce(k[1], k[3], v[1], v[3]);
+        ce(k[1], k[2], v[1], v[2]); ce(k[4], k[5], v[4], v[5]); ce(k[6], k[7], v[6], v[7]); ce(k[4], k[6], v[4], v[6]);
+        ce(k[5], k[7], v[5], v[7]); ce(k[5], k[6], v[5], v[6]); ce(k[0], k[4], v[0], v[4]); ce(k[2], k[6], v[2], v[6]);
+        ce(k[2], k[4], v[2], v[4]); ce(k[1], k[5], v[1], v[5]); ce(k[3], k[7], v[3], v[7]); ce(k[3], k[5], v[3], v[5]);
+        ce(k[1], k[2], v[1], v[2]); ce(k[3], k[4], v[3], v[4]); ce(k[5], k[6], v[5], v[6]);
+    } else {
+        static_assert(N == 16, "networks for 8 and 16 keys");
+        ce(k[0], k[1], v[0], v[1]); ce(k[2], k[3], v[2], v[3]); ce(k[0], k[2], v[0], v[2]); ce(k[1], k[3], v[1], v[3]);
+        ce(k[1], k[2], v[1], v[2]); ce(k[4], k[5], v[4], v[5]); ce(k[6], k[7], v[6], v[7]); ce(k[4], k[6], v[4], v[6]);
+        ce(k[5], k[7], v[5], v[7]); ce(k[5], k[6], v[5], v[6]); ce(k[0], k[4], v[0], v[4]); ce(k[2], k[6], v[2], v[6]);
+        ce(k[2], k[4], v[2], v[4]); ce(k[1], k[5], v[1], v[5]); ce(k[3], k[7], v[3], v[7]); ce(k[3], k[5], v[3], v[5]);
+        ce(k[1], k[2], v[1], v[2]); ce(k[3], k[4], v[3], v[4]); ce(k[5], k[6], v[5], v[6]); ce(k[8], k[9], v[8], v[9]);
+        ce(k[10], k[11], v[10], v[11]); ce(k[8], k[10], v[8], v[10]); ce(k[9], k[11], v[9], v[11]);
+        ce(k[9], k[10], v[9], v[10]); ce(k[12], k[13], v[12], v[13]); ce(k[14], k[15], v[14], v[15]);
+        ce(k[12], k[14], v[12], v[14]); ce(k[13], k[15], v[13], v[15]); ce(k[13], k[14], v[13], v[14]);
+        ce(k[8], k[12], v[8], v[12]); ce(k[10], k[14], v[10], v[14]); ce(k[10], k[12], v[10], v[12]);
+        ce(k[9], k[13], v[9], v[13]); ce(k[11], k[15], v[11], v[15]); ce(k[11], k[13], v[11], v[13]);
+        ce(k[9], k[10], v[9], v[10]); ce(k[11], k[12], v[11], v[12]); ce(k[13], k[14], v[13], v[14]);
+        ce(k[0], k[8], v[0], v[8]); ce(k[4], k[12], v[4], v[12]); ce(k[4], k[8], v[4], v[8]);
+        ce(k[2], k[10], v[2], v[10]); ce(k[6], k[14], v[6], v[14]); ce(k[6], k[10], v[6], v[10]);
+        ce(k[2], k[4], v[2], v[4]); ce(k[6], k[8], v[6], v[8]); ce(k[10], k[12], v[10], v[12]);
+        ce(k[1], k[9], v[1], v[9]); ce(k[5], k[13], v[5], v[13]); ce(k[5], k[9], v[5], v[9]);
+        ce(k[3], k[11], v[3], v[11]); ce(k[7], k[15], v[7], v[15]); ce(k[7], k[11], v[7], v[11]);
+        ce(k[3], k[5], v[3], v[5]); ce(k[7], k[9], v[7], v[9]); ce(k[11], k[13], v[11], v[13]);
+        ce(k[1], k[2], v[1], v[2]); ce(k[3], k[4], v[3], v[4]); ce(k[5], k[6], v[5], v[6]); ce(k[7], k[8], v[7], v[8]);
+        ce(k[9], k[10], v[9], v[10]); ce(k[11], k[12], v[11], v[12]); ce(k[13], k[14], v[13], v[14]);
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (i < len) a[i] = v[i];
+}
+
 __global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, const int32_t* __restrict__ pid,
                              int32_t* __restrict__ order) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -112,6 +165,14 @@ __global__ void k_cell_order(const int32_t* __restrict__ cs, long long ncell, co
     const int len = e - s;
     if (len <= 1) return;
     int32_t* a = order + s;
+    if (len <= 8) {
+        cell_order_net<8>(a, len, pid);
+        return;
+    }
+    if (len <= 16) {
+        cell_order_net<16>(a, len, pid);
+        return;
+    }
     if (len <= 64) {
         for (int i = 1; i < len; ++i) {
             const int32_t v = a[i];
@@ -356,7 +417,7 @@ __host__ __device__ constexpr int p2g_region(int a) {
 //     [0, 12)   wf[a][4]: face weights of component a along its own axis,
 //               window slots -1..2 (node = cell + slot)
 //     [12, 24)  tf[a][4] = C_aa * (x_a - face node a)
-//     [24]      z offset of the particle's cell in its row (bits of an int)
+//     [24, 28)  unused (padding to 16 bytes)
 //   B (kP2GRecB values, odd stride: the staging lanes' stores fall in
 //     distinct banks)
 //     [0, 27)   W[l], column l = 9a + 3s + t of the warp loop: the product of
@@ -486,7 +547,8 @@ __device__ int p2g_stage(const GridP<T>& g, int d0, int d1, int d2, const PView<
 // row's particles are staged 16 at a time (one lane per particle computes
 // its per-axis weights and C.(x_p - x_node) terms once, for all three
 // components, and the per-column products below), then the warp walks them
-// in order, two at a time while they share a cell: lane l < 27 owns one
+// run by run (a ballot over the staged cell offsets marks where each cell's
+// particles start), two at a time within a run: lane l < 27 owns one
 // column of 4 window nodes of one component (component l / 9, along that
 // component's own axis; the 3 x 3 columns across it) and sums the weights
 // and APIC values of the current cell's particles in registers.  When the
@@ -573,40 +635,36 @@ __global__ void __launch_bounds__(kP2GWarps * 32, sizeof(T) == 4 ? 3 : 1) k_p2g(
                 av[k] = fma(w, B + tf[k], av[k]);
             }
         };
-        auto zoff = [&](int j) { return reinterpret_cast<const int*>(stA + j * kP2GRecA + 24)[0]; };
         for (int chunk = pbeg; chunk < pend; chunk += kP2GChunk) {
             const int n = min(kP2GChunk, pend - chunk);
             __syncwarp();
-            if (lane < n) {
-                T* ra = stA + lane * kP2GRecA;
-                const int zo = p2g_stage<T>(g, d0, d1, d2, pv, chunk + lane, rx, ry, z0, zend, ra,
-                                            stB + lane * kP2GRecB, ov_count, ov_list);
-                ra[24] = T(0);
-                reinterpret_cast<int*>(ra + 24)[0] = zo;
-            }
+            int zo = -1;  // this lane's particle: z offset of its cell in the row (-1: overflow)
+            if (lane < n)
+                zo = p2g_stage<T>(g, d0, d1, d2, pv, chunk + lane, rx, ry, z0, zend, stA + lane * kP2GRecA,
+                                  stB + lane * kP2GRecB, ov_count, ov_list);
             __syncwarp();
-            int j = 0;
-            while (j < n) {
-                const int zo0 = zoff(j);
-                if (j + 1 < n) {
-                    const int zo1 = zoff(j + 1);
-                    if (zo0 == cur && zo1 == cur) {  // both in the current cell
-                        if (col) {
-                            add(j);
-                            add(j + 1);
-                        }
-                        j += 2;
-                        continue;
-                    }
+            // the chunk's runs of particles of one cell (sorted order: a cell's particles are contiguous);
+            // every lane walks the same runs
+            const int zprev = __shfl_up_sync(0xffffffffu, zo, 1);
+            unsigned starts = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || zprev != zo));
+            while (starts) {
+                const int sb = __ffs(starts) - 1;
+                starts &= starts - 1;
+                const int se = starts ? __ffs(starts) - 1 : n;
+                const int run = __shfl_sync(0xffffffffu, zo, sb);
+                if (run < 0) continue;  // overflow particles: k_p2g_overflow adds them
+                if (run != cur) {
+                    flush();
+                    cur = run;
                 }
-                if (zo0 >= 0) {
-                    if (zo0 != cur) {
-                        flush();
-                        cur = zo0;
+                if (col) {
+                    int j = sb;
+                    for (; j + 1 < se; j += 2) {
+                        add(j);
+                        add(j + 1);
                     }
-                    if (col) add(j);
+                    if (j < se) add(j);
                 }
-                ++j;
             }
         }
         flush();
