@@ -195,8 +195,9 @@ def algorithmic_bytes(cat, A, C_cells, P, scalar=4):
         # once per face of the three components
         "p2g": 15 * s * P + 6 * s * C_cells,
         # G2P + advection: position read, velocity/affine/position written,
-        # cell key and index written, face velocities read once
-        "g2p": (3 + 15) * s * P + 8 * P + 3 * s * C_cells,
+        # cell key and index written, face velocities read once; the sort's
+        # deferred permutation: its index and the id read, the id written
+        "g2p": (3 + 15) * s * P + 8 * P + 12 * P + 3 * s * C_cells,
     }
     return table.get(cat)
 
@@ -297,6 +298,13 @@ def run_ours(args):
         per_kernel[k] = {"achieved": round(gbs, 1), "frac": round(gbs / peak, 4), "avg_launch_ms": round(ms / nl, 5),
                          "algorithmic_bytes_per_launch": int(b)}
     roofline["kernels"] = per_kernel
+    # the whole step against HBM: the byte model of liquidhairinteration_b200/roofline.py over the
+    # timed steps' mean iteration count
+    from liquidhairinteration_b200 import roofline as step_model
+    sb = step_model.step_bytes(n_particles, cells, active_cells, float(sum(iters)) / len(iters), scalar)
+    roofline["step"] = {"algorithmic_bytes": int(sb), "achieved": round(sb / (ms_step * 1e-3) / 1e9, 1),
+                        "frac": round(sb / (ms_step * 1e-3) / 1e9 / peak, 4),
+                        "what": "whole step: algorithmic bytes of every stage (roofline.step_bytes) / ms_per_step"}
 
     # ---- learned-preconditioner FPCG on the same scene (V-cycle fallback on
     # a < 5% residual drop), timed the same way over a few steps

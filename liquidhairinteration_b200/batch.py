@@ -97,6 +97,7 @@ class BatchRunner:
         Returns the solve statistics of the scenes stepped."""
         from ._lib import LhiError
         live = [k for k, a in enumerate(self.alive) if a]
+        self.last_live = live  # the scenes of the returned statistics, in order
         for k in live:
             try:
                 self.models[k].PreStep(self.specs[k].dt)
@@ -164,17 +165,38 @@ def main(argv=None):
     torch.cuda.synchronize()
     t1 = time.time()
     bad, iters, scene_steps = 0, [], 0
+    scene_iters, scene_n = np.zeros(len(specs)), np.zeros(len(specs))
     for _ in range(a.steps):
         st = runner.step()
         scene_steps += len(st)
         bad += sum(1 for s in st if s["status"] != abi.LHI_OK)
         iters.append(np.mean([s["iterations"] for s in st]) if st else 0.0)
+        for k, s in zip(runner.last_live, st):
+            scene_iters[k] += s["iterations"]
+            scene_n[k] += 1
     wall = time.time() - t1
     cells = sum(s.n ** 3 for s in specs)
+    # the batch against HBM: the step byte model (roofline.step_bytes) of every scene over its steps
+    # (active cells of its finest level as after the last step)
+    from . import roofline
+    moved = 0.0
+    for k, (spec, m) in enumerate(zip(specs, runner.models)):
+        if scene_n[k] == 0:
+            continue
+        active = m.GetSolver().ActiveTiles(0)[0] * 8 * 8 * 32
+        P = m.GetParticleSystem().NumParticles()
+        s_b = 8 if a.precision == "fp64" else 4
+        moved += scene_n[k] * (roofline.particle_bytes(P, s_b) + roofline.grid_bytes(spec.n ** 3, s_b))
+        moved += roofline.solve_bytes(active, scene_iters[k], s_b)
+    peak, peak_kind = roofline.hbm_peak()
+    gbs = moved / wall / 1e9
     res = {"scenes": a.scenes, "steps": a.steps, "sizes": sorted({s.n for s in specs}),
            "cells": cells, "wall_s": round(wall, 3), "scene_steps_per_s": round(scene_steps / wall, 2),
            "ms_per_batch_step": round(1000 * wall / a.steps, 3), "mean_cg_iterations": round(float(np.mean(iters)), 2),
            "failed_solves": bad, "diverged_scenes": {str(k): v for k, v in runner.diverged.items()},
+           "hbm": {"algorithmic_bytes_per_batch_step": int(moved / a.steps), "achieved_gbs": round(gbs, 1),
+                   "frac": round(gbs / peak, 4), "peak_gbs": peak, "peak_kind": peak_kind,
+                   "what": "every scene's step bytes (roofline.step_bytes) / wall time of the batch steps"},
            "coarse_operator": a.coarse,
            "setup_s": round(setup_s, 1),
            "autotuned": {str(k): {"sweeps": v[0], "coarse_cells": v[1]} for k, v in runner.tuned.items()},

@@ -744,10 +744,20 @@ template <class T> __device__ __forceinline__ bool in_grid(const GridP<T>& g, T 
 }
 
 // Grid<3>::GetSolidPhi for a point inside the grid (Grid.cpp:144-154)
-template <class T> __device__ T solid_phi_in(const GridP<T>& g, const T* sp, T x, T y, T z) {
-    T lx = X<T>::div(X<T>::sub(x, g.mn[0]), g.dx[0]);
-    T ly = X<T>::div(X<T>::sub(y, g.mn[1]), g.dx[1]);
-    T lz = X<T>::div(X<T>::sub(z, g.mn[2]), g.dx[2]);
+// EXACT = false (the mixed-precision gather's advection): the grid
+// coordinates by a multiply with 1 / dx, equal up to rounding.
+template <class T, bool EXACT = true>
+__device__ T solid_phi_in(const GridP<T>& g, const T* sp, T x, T y, T z) {
+    T lx, ly, lz;
+    if constexpr (EXACT) {
+        lx = X<T>::div(X<T>::sub(x, g.mn[0]), g.dx[0]);
+        ly = X<T>::div(X<T>::sub(y, g.mn[1]), g.dx[1]);
+        lz = X<T>::div(X<T>::sub(z, g.mn[2]), g.dx[2]);
+    } else {
+        lx = (x - g.mn[0]) * g.idx[0];
+        ly = (y - g.mn[1]) * g.idx[1];
+        lz = (z - g.mn[2]) * g.idx[2];
+    }
     int xi, yi, zi;
     T fx, fy, fz;
     barycentric(lx, 0, g.nx + 1, xi, fx);
@@ -1065,7 +1075,11 @@ __device__ __forceinline__ void g2p_particle(const GridP<T>& g, T* __restrict__ 
     if (do_advect) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) q[k] = X<T>::add(q[k], X<T>::mul(vel[k], dt));
-        T sphi = solid_phi_at(g, sp, q[0], q[1], q[2]);
+        T sphi;
+        if (FACTORED && in_grid(g, q[0], q[1], q[2]))
+            sphi = solid_phi_in<T, false>(g, sp, q[0], q[1], q[2]);
+        else
+            sphi = solid_phi_at(g, sp, q[0], q[1], q[2]);
         if (sphi < T(0)) {
             T gr[3];
             solid_grad_at(g, sp, q[0], q[1], q[2], gr);
