@@ -100,6 +100,14 @@ extern "C" {
    being a usable preconditioner); no counterpart in the reference. */
 #define LHI_COARSE_REFERENCE 0
 #define LHI_COARSE_GALERKIN 1
+/* Initial guess of the PCG (lhi_solver_params.initial_guess).  ZERO is the
+   reference's (x = 0, PressureSolver.cpp:841-856).  PREVIOUS starts from the
+   last solve's solution on the cells that are fluid now (0 elsewhere); the
+   relative stopping rule then measures ||r|| against ||b|| rather than
+   ||r0||, so the solve still ends at ||r||/||b|| <= tolerance.  No
+   counterpart in the reference. */
+#define LHI_GUESS_ZERO 0
+#define LHI_GUESS_PREVIOUS 1
 
 typedef struct lhi_grid_desc {
     int32_t dim[3];        /* gridDimension (SceneParameter.h:137)          */
@@ -133,6 +141,7 @@ typedef struct lhi_solver_params {   /* SolverParameter<3> (SceneParameter.h:10-
     int32_t sweep_kernel;            /* LHI_SWEEP_* (0 = fused where the level
                                         allows it)                             */
     int32_t coarse_operator;         /* LHI_COARSE_* (0 = reference)           */
+    int32_t initial_guess;           /* LHI_GUESS_* (0 = reference)            */
 } lhi_solver_params;
 
 typedef struct lhi_liquid_params {   /* LiquidParameter<3> + SceneParameter<3> */

@@ -48,6 +48,8 @@ SWEEP_FUSED = 0
 SWEEP_SPLIT = 1
 COARSE_REFERENCE = 0
 COARSE_GALERKIN = 1
+GUESS_ZERO = 0
+GUESS_PREVIOUS = 1
 
 BOUNDARY_RECT = 0
 BOUNDARY_SOLID = 1
@@ -129,7 +131,8 @@ class SolverParams(C.Structure):
                 ("tolerance_mode", C.c_int32), ("cg_variant", C.c_int32),
                 ("true_residual_every", C.c_int32), ("update_region", C.c_int32),
                 ("smoother", C.c_int32), ("coarse_cells", C.c_int32), ("eager", C.c_int32),
-                ("sweep_kernel", C.c_int32), ("coarse_operator", C.c_int32)]
+                ("sweep_kernel", C.c_int32), ("coarse_operator", C.c_int32),
+                ("initial_guess", C.c_int32)]
 
 
 class LiquidParams(C.Structure):
@@ -170,7 +173,7 @@ def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECON
                        num_level=4, num_pre_smooth=5, num_post_smooth=5, num_final_smooth=20,
                        smoothing_factor=0.5, tolerance_mode=TOL_ABSOLUTE, cg_variant=CG_REFERENCE,
                        true_residual_every=0, update_region=REGION_INTERIOR, smoother=SMOOTHER_REFERENCE,
-                       coarse_cells=0, eager=0, sweep_kernel=0, coarse_operator=0):
+                       coarse_cells=0, eager=0, sweep_kernel=0, coarse_operator=0, initial_guess=0):
     s = SolverParams()
     s.max_iterations = int(max_iterations)
     s.tolerance = float(tolerance)
@@ -189,6 +192,7 @@ def make_solver_params(max_iterations=100, tolerance=1e-5, preconditioner=PRECON
     s.eager = int(eager)
     s.sweep_kernel = int(sweep_kernel)
     s.coarse_operator = int(coarse_operator)
+    s.initial_guess = int(initial_guess)
     return s
 
 

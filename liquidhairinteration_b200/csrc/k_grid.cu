@@ -440,6 +440,8 @@ LiquidImpl<T, TX>::LiquidImpl(const lhi_grid_desc& g, const lhi_solver_params& s
         throw std::invalid_argument("unknown cg_variant");
     if (sp.coarse_operator != LHI_COARSE_REFERENCE && sp.coarse_operator != LHI_COARSE_GALERKIN)
         throw std::invalid_argument("unknown coarse_operator");
+    if (sp.initial_guess != LHI_GUESS_ZERO && sp.initial_guess != LHI_GUESS_PREVIOUS)
+        throw std::invalid_argument("unknown initial_guess");
     nlev_ = std::max(1, sp.num_level);
     if (sp.preconditioner != LHI_PRECOND_MULTIGRID && sp.preconditioner != LHI_PRECOND_LEARNED) nlev_ = 1;
     if (sp.preconditioner == LHI_PRECOND_LEARNED && precision == LHI_PRECISION_FP64)

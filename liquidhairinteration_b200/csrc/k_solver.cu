@@ -1122,6 +1122,7 @@ struct CgConf {
     double tol;
     cudaGraphConditionalHandle cond;
     int use_cond;
+    int warm;        // LHI_GUESS_PREVIOUS: the relative threshold comes from ||b||, not ||r0||
 };
 
 // Stopping rule after an update of r (PressureSolver.cpp:889-902): with a
@@ -1162,6 +1163,35 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_r(LevelK<T> L, TileK t
     });
 }
 
+// LHI_GUESS_PREVIOUS: x keeps the last solve's values on the cells that are
+// fluid now and is 0 elsewhere (so the pressure written from it is 0 off
+// the liquid, as the reference's cleared grid has it).
+template <class TX>
+__global__ void k_x_fluid_only(long long n, const uint8_t* __restrict__ type, TX* __restrict__ x) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && type[i] != 2) x[i] = TX(0);
+}
+
+// LHI_GUESS_PREVIOUS: r0 = b - A x0 on the cells with a row (where the
+// reference's r0 = b is set), and sum b^2 over them into red[0]: the
+// relative stopping rule's reference norm.
+template <class T, class TX>
+__global__ void __launch_bounds__(kTileThreads) k_cg_init_warm(LevelK<T> L, TileK tk, const T* __restrict__ b,
+                                                               const TX* __restrict__ x, T* __restrict__ r,
+                                                               double* __restrict__ partials,
+                                                               unsigned* __restrict__ counter,
+                                                               SolveScalars* __restrict__ sc) {
+    double v[1] = {0.0};
+    for_tiles(tk, L.nx, L.ny, L.nz, [&](int xi, int yi, int zi, long long i) {
+        if (L.type[i] == 0) return;
+        r[i] = T(double(b[i]) - ax_at<double>(L, x, i, xi, yi, zi));
+        v[0] += double(b[i]) * double(b[i]);
+    });
+    double tot[1];
+    if (!grid_sum_last<1>(v, partials, counter, tot)) return;
+    sc->red[0] = tot[0];
+}
+
 // p = z on fluid cells; rz = r.z and rr = r.r over all cells; the stopping
 // threshold from ||r0|| (PressureSolver.cpp:858-871)
 template <class T>
@@ -1184,7 +1214,9 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK t
     const T t = T(cf.tol);
     sc->residual0 = r0;
     sc->residual = r0;
-    sc->threshold = cf.rel ? double(T(t * T(r0))) : double(t);
+    // with a previous solution as the guess, ||r|| is measured against ||b|| (k_cg_init_warm)
+    const double ref = cf.warm ? sqrt(sc->red[0]) : r0;
+    sc->threshold = cf.rel ? double(T(t * T(ref))) : double(t);
     sc->iter = 0;
     sc->true_now = 0;
     // a zero right-hand side is solved by x = 0 (under the relative rule the
@@ -1780,7 +1812,8 @@ template <class T, class TX> void LiquidImpl<T, TX>::read_scalars() {
 // CGSolver<3>::Init (PressureSolver.cpp:666-680)
 template <class T, class TX> void LiquidImpl<T, TX>::solver_init() {
     LHI_CUDA(cudaMemsetAsync(p_, 0, sizeof(T) * ncell_, cur_));
-    LHI_CUDA(cudaMemsetAsync(x_, 0, sizeof(TX) * ncell_, cur_));
+    if (sp_.initial_guess != LHI_GUESS_PREVIOUS)  // else the last solution is the guess (k_x_fluid_only)
+        LHI_CUDA(cudaMemsetAsync(x_, 0, sizeof(TX) * ncell_, cur_));
     LHI_CUDA(cudaMemsetAsync(rhs_, 0, sizeof(T) * ncell_, cur_));
     for (int l = 0; l < nlev_; ++l) {
         LevelDev<T>& L = lv_[l];
@@ -2135,6 +2168,7 @@ static CgConf make_conf(const lhi_solver_params& sp, unsigned long long cond, in
     c.tol = sp.tolerance;
     c.cond = cond;
     c.use_cond = use_cond;
+    c.warm = sp.initial_guess == LHI_GUESS_PREVIOUS ? 1 : 0;
     return c;
 }
 
@@ -2146,7 +2180,13 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_init(unsigned long 
     const CgConf cf = make_conf(sp_, cond, use_cond);
     {
         auto ps_ = scope(LHI_KERNEL_CG_VECTOR);
-        k_cg_init_r<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, L0.r);
+        if (sp_.initial_guess == LHI_GUESS_PREVIOUS) {
+            k_x_fluid_only<TX><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(ncell_, L0.type, x_);
+            LHI_LAUNCH_CHECK();
+            k_cg_init_warm<T, TX><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, x_, L0.r, partials_, counter_, sc_);
+        } else {
+            k_cg_init_r<T><<<G, kTileThreads, 0, cur_>>>(lk(L0), tk, rhs_, L0.r);
+        }
         LHI_LAUNCH_CHECK();
     }
     record_snapshot();
