@@ -98,52 +98,33 @@ __global__ void k_velocity_update(int nx, int ny, int nz, T hx, T hy, T hz, T dt
     if (ix <= 0 || iy <= 0 || iz <= 0) return;
     long long n = (long long)ix * iy * iz;
     if (i >= n) return;
-    int z = 1 + int(i % iz), y = 1 + int((i / iz) % iy), x = 1 + int(i / ((long long)iy * iz));
+    // 32-bit index arithmetic: the interior has fewer than 2^31 cells
+    const unsigned u = unsigned(i), t = u / unsigned(iz);
+    const int z = 1 + int(u - t * unsigned(iz)), y = 1 + int(t % unsigned(iy)), x = 1 + int(t / unsigned(iy));
     long long c = ((long long)x * ny + y) * nz + z;
-    const T center = phi[c];
-    const T pc = pr[c];
-    long long sx = (long long)ny * nz, sy = nz;
-    // x face (xi, yi, zi) of vx: (x * ny + y) * nz + z
-    {
-        long long f = ((long long)x * ny + y) * nz + z;
-        if (lwx[f] > T(0)) {
-            T nphi = phi[c - sx];
-            if (center < T(0) || nphi < T(0)) {
+    const long long sx = (long long)ny * nz, sy = nz;
+    const long long fx = ((long long)x * ny + y) * nz + z;        // face (x, y, z) of vx
+    const long long fy = ((long long)x * (ny + 1) + y) * nz + z;  // of vy
+    const long long fz = ((long long)x * ny + y) * (nz + 1) + z;  // of vz
+    // the operands of the tests first (all in bounds for an interior cell),
+    // so the loads overlap instead of waiting on one another behind branches
+    const T center = phi[c], pc = pr[c];
+    const T nphi[3] = {phi[c - sx], phi[c - sy], phi[c - 1]};
+    const T npr[3] = {pr[c - sx], pr[c - sy], pr[c - 1]};
+    const T lw[3] = {lwx[fx], lwy[fy], lwz[fz]};
+    T* const vv[3] = {vx + fx, vy + fy, vz + fz};
+    const T hh[3] = {hx, hy, hz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (lw[a] > T(0)) {
+            if (center < T(0) || nphi[a] < T(0)) {
                 T frac = T(1);
-                if (center >= T(0) || nphi >= T(0)) frac = frac_floor(fraction_in_region(center, nphi));
-                T grad = X<T>::div(X<T>::sub(pc, pr[c - sx]), X<T>::mul(hx, frac));
-                vx[f] = X<T>::sub(vx[f], X<T>::div(X<T>::mul(grad, dt), rho));
+                if (center >= T(0) || nphi[a] >= T(0)) frac = frac_floor(fraction_in_region(center, nphi[a]));
+                T grad = X<T>::div(X<T>::sub(pc, npr[a]), X<T>::mul(hh[a], frac));
+                *vv[a] = X<T>::sub(*vv[a], X<T>::div(X<T>::mul(grad, dt), rho));
             }
         } else {
-            vx[f] = T(0);
-        }
-    }
-    {
-        long long f = ((long long)x * (ny + 1) + y) * nz + z;
-        if (lwy[f] > T(0)) {
-            T nphi = phi[c - sy];
-            if (center < T(0) || nphi < T(0)) {
-                T frac = T(1);
-                if (center >= T(0) || nphi >= T(0)) frac = frac_floor(fraction_in_region(center, nphi));
-                T grad = X<T>::div(X<T>::sub(pc, pr[c - sy]), X<T>::mul(hy, frac));
-                vy[f] = X<T>::sub(vy[f], X<T>::div(X<T>::mul(grad, dt), rho));
-            }
-        } else {
-            vy[f] = T(0);
-        }
-    }
-    {
-        long long f = ((long long)x * ny + y) * (nz + 1) + z;
-        if (lwz[f] > T(0)) {
-            T nphi = phi[c - 1];
-            if (center < T(0) || nphi < T(0)) {
-                T frac = T(1);
-                if (center >= T(0) || nphi >= T(0)) frac = frac_floor(fraction_in_region(center, nphi));
-                T grad = X<T>::div(X<T>::sub(pc, pr[c - 1]), X<T>::mul(hz, frac));
-                vz[f] = X<T>::sub(vz[f], X<T>::div(X<T>::mul(grad, dt), rho));
-            }
-        } else {
-            vz[f] = T(0);
+            *vv[a] = T(0);
         }
     }
 }

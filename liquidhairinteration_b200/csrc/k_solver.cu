@@ -198,7 +198,9 @@ __global__ void k_level_phi(LevelGeom g, const T* __restrict__ fine_phi, T* __re
 template <class T, class TI = T>
 __global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI* __restrict__ lwx,
                                const TI* __restrict__ lwy, const TI* __restrict__ lwz, T h0, T h1, T h2, T dt, T rho,
-                               T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy, T* __restrict__ cz) {
+                               T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy, T* __restrict__ cz,
+                               uint8_t* __restrict__ type, uint8_t* __restrict__ tile_flag, int tdy, int tdz,
+                               uint8_t* __restrict__ mask, int mpitch) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)g.nx * g.ny * g.nz;
     if (i >= n) return;
@@ -214,41 +216,56 @@ __global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI
     auto term_of = [&](int a, T w) -> T {
         return X<T>::div(X<T>::mul(w, dt), X<T>::mul(X<T>::mul(rho, hh[a]), hh[a]));
     };
+    // The six faces (right, left, top, bottom, front, back) and the
+    // neighbours' phi, loaded up front so the loads overlap; each face's term
+    // w dt / (rho h^2) is formed once (the +x/+y/+z terms serve both this
+    // cell's couplings and its diagonal), in the reference's arithmetic.
+    const int xs[6] = {x + 1, x, x, x, x, x};
+    const int ys[6] = {y, y, y + 1, y, y, y};
+    const int zs[6] = {z, z, z, z, z + 1, z};
+    const int ax[6] = {0, 0, 1, 1, 2, 2};
+    const long long off[6] = {sx, -sx, sy, -sy, 1, -1};
+    const bool exists[6] = {x + 1 < g.nx, x - 1 >= 0, y + 1 < g.ny, y - 1 >= 0, z + 1 < g.nz, z - 1 >= 0};
+    const T center = T(phi[i]);
+    const bool row = !(center > T(0));
+    T w6[6], nphi6[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        w6[k] = exists[k] ? T(approx_w(lw[ax[k]], g, ax[k], xs[k], ys[k], zs[k])) : T(0);
+        nphi6[k] = exists[k] ? T(phi[i + off[k]]) : T(0);
+    }
+    T term6[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)  // the -x/-y/-z terms only for a row of the matrix
+        term6[k] = (w6[k] > T(0) && ((k & 1) == 0 || row)) ? term_of(ax[k], w6[k]) : T(0);
     // own +x/+y/+z face coefficients
-    T c[3] = {T(0), T(0), T(0)};
-    {
-        int cc[3] = {x, y, z};
-        int dd[3] = {g.nx, g.ny, g.nz};
-        for (int a = 0; a < 3; ++a) {
-            if (cc[a] + 1 < dd[a]) {
-                T w = T(approx_w(lw[a], g, a, x + (a == 0), y + (a == 1), z + (a == 2)));
-                if (w > T(0)) c[a] = -term_of(a, w);
-            }
+    cx[i] = (w6[0] > T(0)) ? -term6[0] : T(0);
+    cy[i] = (w6[2] > T(0)) ? -term6[2] : T(0);
+    cz[i] = (w6[4] > T(0)) ? -term6[4] : T(0);
+    // the finest level (type != nullptr) also classifies the cell, marks its
+    // tile active (k_level_phi's work) and, where the fused sweep runs, writes
+    // its neighbour mask (k_level_mask's), from the phi values at hand
+    if (type) {
+        const uint8_t t = (center > T(0)) ? 0 : ((center < T(0)) ? 2 : 1);
+        type[i] = t;
+        if (t != 0) tile_flag[((long long)(x / kTileX) * tdy + y / kTileY) * tdz + z / kTileZ] = 1;
+        if (mask) {
+            unsigned m = t != 0 ? 64u : 0u;
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                if (exists[k] && nphi6[k] < T(0)) m |= 1u << k;  // right, left, top, bottom, front, back
+            mask[((long long)x * g.ny + y) * mpitch + z] = uint8_t(m);
         }
     }
-    cx[i] = c[0];
-    cy[i] = c[1];
-    cz[i] = c[2];
-    const T center = T(phi[i]);
     T d = T(0);
-    if (!(center > T(0))) {
-        // right, left, top, bottom, front, back
-        const int xs[6] = {x + 1, x, x, x, x, x};
-        const int ys[6] = {y, y, y + 1, y, y, y};
-        const int zs[6] = {z, z, z, z, z + 1, z};
-        const int ax[6] = {0, 0, 1, 1, 2, 2};
-        const long long off[6] = {sx, -sx, sy, -sy, 1, -1};
-        const bool exists[6] = {x + 1 < g.nx, x - 1 >= 0, y + 1 < g.ny, y - 1 >= 0, z + 1 < g.nz, z - 1 >= 0};
+    if (row) {
+#pragma unroll
         for (int k = 0; k < 6; ++k) {
-            if (!exists[k]) continue;
-            const int a = ax[k];
-            T w = T(approx_w(lw[a], g, a, xs[k], ys[k], zs[k]));
-            if (w > T(0)) {
-                T term = term_of(a, w);
-                T nphi = T(phi[i + off[k]]);
-                if (nphi < T(0)) d = X<T>::add(d, term);
-                else d = X<T>::add(d, X<T>::div(term, frac_floor(fraction_in_region(center, nphi))));
-            }
+            if (!exists[k] || !(w6[k] > T(0))) continue;
+            const T term = term6[k];
+            const T nphi = nphi6[k];
+            if (nphi < T(0)) d = X<T>::add(d, term);
+            else d = X<T>::add(d, X<T>::div(term, frac_floor(fraction_in_region(center, nphi))));
         }
     }
     diag[i] = d;
@@ -1854,19 +1871,22 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
             LHI_LAUNCH_CHECK();
             continue;
         }
-        k_level_phi<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(g, liquid_phi_, L.phi, L.type, L.tile_flag, L.tdim[1],
-                                                              L.tdim[2]);
-        LHI_LAUNCH_CHECK();
+        if (l > 0) {  // the finest level's classes, tile flags and mask come with its matrix
+            k_level_phi<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(g, liquid_phi_, L.phi, L.type, L.tile_flag,
+                                                                  L.tdim[1], L.tdim[2]);
+            LHI_LAUNCH_CHECK();
+        }
         const T* phi = (l == 0) ? liquid_phi_ : L.phi;
-        k_level_matrix<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1],
-                                                                  L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1],
-                                                                  L.cf[2]);
+        k_level_matrix<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
+            g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1], L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1], L.cf[2],
+            l == 0 ? L.type : nullptr, L.tile_flag, L.tdim[1], L.tdim[2], (l == 0 && L.fused) ? L.mask : nullptr,
+            L.mpitch);
         LHI_LAUNCH_CHECK();
         if constexpr (kHiResidual) {
             if (l == 0) {
                 k_level_matrix<double, T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
                     g, liquid_phi_, lw_[0], lw_[1], lw_[2], dxd_[0], dxd_[1], dxd_[2], dt, rho, diag_hi_, cf_hi_[0],
-                    cf_hi_[1], cf_hi_[2]);
+                    cf_hi_[1], cf_hi_[2], nullptr, nullptr, 0, 0, nullptr, 0);
                 LHI_LAUNCH_CHECK();
             }
         }
@@ -1877,7 +1897,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_masks() {
-    for (int l = 0; l < nlev_; ++l) {
+    for (int l = 1; l < nlev_; ++l) {  // level 0's mask comes with its matrix (k_level_matrix)
         LevelDev<T>& L = lv_[l];
         if (!L.fused) continue;
         k_level_mask<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(lk(L), L.mask, L.mpitch);
