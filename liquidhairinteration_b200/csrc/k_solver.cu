@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "impl.cuh"
+#include "layouts.cuh"
 
 namespace lhi {
 
@@ -532,12 +533,12 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_sweep(LevelK<T> L, TileK tk
 // the arithmetic of smooth7 in the same order, so the values equal those of
 // two k_sweep launches.  Cells outside the grid read diag 0 and are skipped.
 namespace rb {
-constexpr int kZW = 40;
-constexpr int kZ = 12 * 12 * kZW;
-constexpr int kR = 10 * 10 * kZW;
-constexpr int kC = 11 * 10 * kZW;
-constexpr int kMW = 64;
-constexpr int kM = 10 * 10 * kMW;
+constexpr int kZW = layout::kZW;
+constexpr int kZ = layout::kZBox;
+constexpr int kR = layout::kRBox;
+constexpr int kC = layout::kCBox;
+constexpr int kMW = layout::kMW;
+constexpr int kM = layout::kMBox;
 constexpr uint32_t kTx = uint32_t((kZ + 3 * kR + 2 * kC) * 4 + kM);  // bytes the 7 boxes deliver
 constexpr int al(int b) { return (b + 127) & ~127; }
 // offsets inside one stage
@@ -561,21 +562,21 @@ __device__ __forceinline__ bool rb_eval(const float* __restrict__ Zs, const floa
                                         const float* __restrict__ CXs, const float* __restrict__ CYs,
                                         const uint8_t* __restrict__ Ms, int lx, int ly, int lz, float w, int variant,
                                         int& zi, float& out) {
-    const int ri = ((lx + 1) * 10 + (ly + 1)) * rb::kZW + (lz + 4);
-    zi = ((lx + 2) * 12 + (ly + 2)) * rb::kZW + (lz + 4);
+    const int ri = layout::rb_r(lx, ly, lz);
+    zi = layout::rb_z(lx, ly, lz);
     const float d = Ds[ri];
     if (is_small(d)) return false;
-    const unsigned m = Ms[((lx + 1) * 10 + (ly + 1)) * rb::kMW + (lz + 16)];
+    const unsigned m = Ms[layout::rb_m(lx, ly, lz)];
     const float zc = Zs[zi];
     float ax = 0.f;
     if (m & 64u) {
-        const int xi = ((lx + 2) * 10 + (ly + 1)) * rb::kZW + (lz + 4);
-        const int yi = ((lx + 1) * 11 + (ly + 2)) * rb::kZW + (lz + 4);
+        const int xi = layout::rb_cx(lx, ly, lz);
+        const int yi = layout::rb_cy(lx, ly, lz);
         ax = zc * d;
-        if (m & 1u) ax += Zs[zi + 12 * rb::kZW] * CXs[xi];
-        if (m & 2u) ax += Zs[zi - 12 * rb::kZW] * CXs[xi - 10 * rb::kZW];
-        if (m & 4u) ax += Zs[zi + rb::kZW] * CYs[yi];
-        if (m & 8u) ax += Zs[zi - rb::kZW] * CYs[yi - rb::kZW];
+        if (m & 1u) ax += Zs[zi + layout::kZStepX] * CXs[xi];
+        if (m & 2u) ax += Zs[zi - layout::kZStepX] * CXs[xi - layout::kCXStepX];
+        if (m & 4u) ax += Zs[zi + layout::kZStepY] * CYs[yi];
+        if (m & 8u) ax += Zs[zi - layout::kZStepY] * CYs[yi - layout::kCYStepY];
         if (m & 16u) ax += Zs[zi + 1] * CZs[ri];
         if (m & 32u) ax += Zs[zi - 1] * CZs[ri - 1];
     }
@@ -678,7 +679,7 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
         // a colour's updates read only the other colour: a thread evaluates
         // all of its cells before storing any, so their loads overlap
         {
-            constexpr int kN = (100 * 17 + rb::kThreads - 1) / rb::kThreads;
+            constexpr int kN = (layout::kRbColour0Items + rb::kThreads - 1) / rb::kThreads;
             int zi[kN];
             float out[kN];
             bool upd[kN];
@@ -686,10 +687,9 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
             for (int n = 0; n < kN; ++n) {
                 const int q = threadIdx.x + n * rb::kThreads;
                 upd[n] = false;
-                if (q < 100 * 17) {
-                    const int row = q / 17, k = q - row * 17;
-                    const int lx = row / 10 - 1, ly = row - (row / 10) * 10 - 1;
-                    const int lz = ((x0 + lx + y0 + ly + z0 - 1) & 1) - 1 + 2 * k;
+                if (q < layout::kRbColour0Items) {
+                    int lx, ly, lz;
+                    layout::rb_colour0(q, x0, y0, z0, lx, ly, lz);
                     upd[n] = rb_eval(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant, zi[n], out[n]);
                 }
             }
@@ -700,16 +700,15 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
         __syncthreads();
         // colour 1 on T: 8 x 8 rows of 16
         {
-            constexpr int kN = 64 * 16 / rb::kThreads;
+            constexpr int kN = layout::kRbColour1Items / rb::kThreads;
             int zi[kN];
             float out[kN];
             bool upd[kN];
 #pragma unroll
             for (int n = 0; n < kN; ++n) {
                 const int q = threadIdx.x + n * rb::kThreads;
-                const int row = q >> 4, k = q & 15;
-                const int lx = row >> 3, ly = row & 7;
-                const int lz = ((x0 + lx + y0 + ly + z0 + 1) & 1) + 2 * k;
+                int lx, ly, lz;
+                layout::rb_colour1(q, x0, y0, z0, lx, ly, lz);
                 upd[n] = rb_eval(Zs, Rs, Ds, CZs, CXs, CYs, Ms, lx, ly, lz, w, variant, zi[n], out[n]);
             }
 #pragma unroll
@@ -717,21 +716,21 @@ __global__ void __launch_bounds__(rb::kThreads, 1)
                 if (upd[n]) Zs[zi[n]] = out[n];
         }
         __syncthreads();
-        for (int q = threadIdx.x; q < 64 * 8; q += rb::kThreads) {
-            const int row = q >> 3, c = q & 7;
-            const int lx = row >> 3, ly = row & 7;
+        for (int q = threadIdx.x; q < layout::kRbOutItems; q += rb::kThreads) {
+            int lx, ly, c;
+            const int zo = layout::rb_out(q, lx, ly, c);
             const int x = x0 + lx, y = y0 + ly, z = z0 + 4 * c;
             if (x < nx && y < ny && z < nz) {
-                const float4 zv = *reinterpret_cast<const float4*>(Zs + ((lx + 2) * 12 + (ly + 2)) * rb::kZW + 4 + 4 * c);
+                const float4 zv = *reinterpret_cast<const float4*>(Zs + zo);
                 *reinterpret_cast<float4*>(zout + ((long long)x * ny + y) * nz + z) = zv;
                 if (final_dot) {  // k_cg_dot_rz's sums over the swept cells
                     const float zz[4] = {zv.x, zv.y, zv.z, zv.w}, aa[4] = {apv.x, apv.y, apv.z, apv.w};
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const int lz = 4 * c + j;
-                        const float rv = Rs[((lx + 1) * 10 + (ly + 1)) * rb::kZW + (lz + 4)];
+                        const float rv = Rs[layout::rb_r(lx, ly, lz)];
                         v[0] += double(rv) * double(zz[j]);
-                        const unsigned m = Ms[((lx + 1) * 10 + (ly + 1)) * rb::kMW + (lz + 16)];
+                        const unsigned m = Ms[layout::rb_m(lx, ly, lz)];
                         if ((m & 64u) && in_region(x, y, z + j, nx, ny, nz, region))
                             v[1] += double(aa[j]) * double(zz[j]);
                     }
@@ -1253,7 +1252,8 @@ __global__ void __launch_bounds__(kTileThreads) k_cg_init_p(LevelK<T> L, TileK t
 // does; the CTAs take other tiles than k_cg_spmv's, so p.Ap is grouped
 // differently in its last bits.
 namespace sp {
-constexpr int kP = 10 * 10 * 40, kD = 8 * 8 * 32, kCX = 9 * 8 * 32, kCY = 8 * 9 * 32, kCZ = 8 * 8 * 36, kM = kD;
+constexpr int kP = layout::kPBox, kD = layout::kDBox, kCX = layout::kCXBox, kCY = layout::kCYBox,
+              kCZ = layout::kCZBox, kM = kD;
 constexpr uint32_t kTx = uint32_t((kP + kD + kCX + kCY + kCZ) * 4 + kM);
 // offsets inside one stage; two mbarriers, then two stages
 constexpr int oP = 0, oD = oP + kP * 4, oCX = oD + kD * 4, oCY = oCX + kCX * 4, oCZ = oCY + kCY * 4,
@@ -1334,19 +1334,19 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             for (int ly = 0; ly < kTileY; ++ly) {
                 const int y = y0 + ly;
                 if (y >= ny) break;
-                const int pi = ((wp + 1) * 10 + (ly + 1)) * 40 + (lane + 4);
-                const int ci = (wp * 8 + ly) * 32 + lane;
+                const int pi = layout::sp_p(wp, ly, lane);
+                const int ci = layout::sp_c(wp, ly, lane);
                 const unsigned m = Ms[ci];
                 const float pc = Ps[pi];
                 float a = 0.f;
                 if (m & 64u) {
                     a = pc * Ds[ci];
-                    if (m & 1u) a += Ps[pi + 400] * CXs[ci + 256];
-                    if (m & 2u) a += Ps[pi - 400] * CXs[ci];
-                    if (m & 4u) a += Ps[pi + 40] * CYs[(wp * 9 + ly + 1) * 32 + lane];
-                    if (m & 8u) a += Ps[pi - 40] * CYs[(wp * 9 + ly) * 32 + lane];
-                    if (m & 16u) a += Ps[pi + 1] * CZs[(wp * 8 + ly) * 36 + lane + 4];
-                    if (m & 32u) a += Ps[pi - 1] * CZs[(wp * 8 + ly) * 36 + lane + 3];
+                    if (m & 1u) a += Ps[pi + layout::kPStepX] * CXs[layout::sp_cx(wp, ly, lane)];
+                    if (m & 2u) a += Ps[pi - layout::kPStepX] * CXs[layout::sp_cx_minus(wp, ly, lane)];
+                    if (m & 4u) a += Ps[pi + layout::kPStepY] * CYs[layout::sp_cy(wp, ly, lane)];
+                    if (m & 8u) a += Ps[pi - layout::kPStepY] * CYs[layout::sp_cy_minus(wp, ly, lane)];
+                    if (m & 16u) a += Ps[pi + 1] * CZs[layout::sp_cz(wp, ly, lane)];
+                    if (m & 32u) a += Ps[pi - 1] * CZs[layout::sp_cz_minus(wp, ly, lane)];
                 }
                 ap[((long long)x * ny + y) * nz + zz] = a;
                 if ((m & 64u) && in_region(x, y, zz, nx, ny, nz, cf.region)) v[0] += double(pc) * double(a);
@@ -1431,35 +1431,34 @@ __global__ void __launch_bounds__(kTileThreads, 3)
         float res[kTileY];  // all rows first, then the stores: their loads overlap
 #pragma unroll
         for (int ly = 0; ly < kTileY; ++ly) {
-            const int pi = ((wp + 1) * 10 + (ly + 1)) * 40 + (lane + 4);
-            const int ci = (wp * 8 + ly) * 32 + lane;
+            const int pi = layout::sp_p(wp, ly, lane);
+            const int ci = layout::sp_c(wp, ly, lane);
             const unsigned m = Ms[ci];
             const float zc0 = Ps[pi];
             float a = 0.f;
             if (m & 64u) {
                 a = zc0 * Ds[ci];
-                if (m & 1u) a += Ps[pi + 400] * CXs[ci + 256];
-                if (m & 2u) a += Ps[pi - 400] * CXs[ci];
-                if (m & 4u) a += Ps[pi + 40] * CYs[(wp * 9 + ly + 1) * 32 + lane];
-                if (m & 8u) a += Ps[pi - 40] * CYs[(wp * 9 + ly) * 32 + lane];
-                if (m & 16u) a += Ps[pi + 1] * CZs[(wp * 8 + ly) * 36 + lane + 4];
-                if (m & 32u) a += Ps[pi - 1] * CZs[(wp * 8 + ly) * 36 + lane + 3];
+                if (m & 1u) a += Ps[pi + layout::kPStepX] * CXs[layout::sp_cx(wp, ly, lane)];
+                if (m & 2u) a += Ps[pi - layout::kPStepX] * CXs[layout::sp_cx_minus(wp, ly, lane)];
+                if (m & 4u) a += Ps[pi + layout::kPStepY] * CYs[layout::sp_cy(wp, ly, lane)];
+                if (m & 8u) a += Ps[pi - layout::kPStepY] * CYs[layout::sp_cy_minus(wp, ly, lane)];
+                if (m & 16u) a += Ps[pi + 1] * CZs[layout::sp_cz(wp, ly, lane)];
+                if (m & 32u) a += Ps[pi - 1] * CZs[layout::sp_cz_minus(wp, ly, lane)];
             }
             res[ly] = Rs[ci] - a;
         }
 #pragma unroll
-        for (int ly = 0; ly < kTileY; ++ly) Res[(wp * 8 + ly) * 32 + lane] = res[ly];
+        for (int ly = 0; ly < kTileY; ++ly) Res[layout::sp_c(wp, ly, lane)] = res[ly];
         __syncthreads();
         {
-            const int t = threadIdx.x;
-            const int i = t >> 6, j = (t >> 4) & 3, k = t & 15;
+            int i, j, k;
+            layout::rs_coarse(threadIdx.x, i, j, k);
             const int cx = (x0 >> 1) + i, cy = (y0 >> 1) + j, cz = (z0 >> 1) + k;
             if (cx < cnx && cy < cny && cz < cnz) {
                 float acc = 0.f;
 #pragma unroll
                 for (int c8 = 0; c8 < 8; ++c8) {
-                    const int a = (c8 >> 2) & 1, b = (c8 >> 1) & 1, c = c8 & 1;
-                    const float res = Res[((2 * i + a) * 8 + (2 * j + b)) * 32 + 2 * k + c];
+                    const float res = Res[layout::rs_child(i, j, k, c8)];
                     acc = float(double(acc) + 0.125 * double(res));
                 }
                 const long long o = ((long long)cx * cny + cy) * cnz + cz;
