@@ -425,6 +425,10 @@ LHI_API int lhi_net_set_params(lhi_net* net, const float* in);
 /* Activation between layers: 0 = identity (default: a linear multilevel
    operator, a fixed preconditioner for each geometry), 1 = ReLU. */
 LHI_API int lhi_net_set_relu(lhi_net* net, int32_t relu);
+/* 1 (default): the forward passes of lhi_net_forward_host and of the solver
+   evaluate each convolution only on the output tiles that the cells with
+   type != 0 depend on (z is the same, bit for bit); 0: every tile. */
+LHI_API int lhi_net_set_sparse(lhi_net* net, int32_t on);
 /* z = M(r) on an n0 x n1 x n2 grid from host buffers: r (float per cell),
    type (uint8 per cell: 0 phi > 0, 1 phi == 0, 2 phi < 0), solid (uint8
    per cell, 1 = solid cell, may be NULL); scale > 0 fixes s, 0 uses the RMS

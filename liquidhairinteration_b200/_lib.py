@@ -54,6 +54,7 @@ SIGNATURES = {
     "lhi_net_set_params": [C.c_void_p, _vp],
     "lhi_net_save": [C.c_void_p, C.c_char_p],
     "lhi_net_set_relu": [C.c_void_p, C.c_int32],
+    "lhi_net_set_sparse": [C.c_void_p, C.c_int32],
     "lhi_net_load": [C.c_void_p, C.c_char_p],
     "lhi_solver_set_network": [_h, C.c_void_p, C.c_int32],
     "lhi_solver_learned_stats": [_h, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],

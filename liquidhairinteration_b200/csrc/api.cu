@@ -316,6 +316,12 @@ LHI_API int lhi_net_set_relu(lhi_net* net, int32_t relu) {
     return LHI_OK;
 }
 
+LHI_API int lhi_net_set_sparse(lhi_net* net, int32_t on) {
+    if (!net) return fail(LHI_E_INVALID_ARG, "null argument");
+    net->impl->sparse_enabled_ = on != 0;
+    return LHI_OK;
+}
+
 LHI_API int lhi_net_save(lhi_net* net, const char* path) {
     if (!net || !path) return fail(LHI_E_INVALID_ARG, "null argument");
     return guarded([&]() -> int {
@@ -464,7 +470,8 @@ LHI_API int lhi_net_forward_host(lhi_net* net, const int32_t dims[3], const floa
         NetHostArgs d;
         net_upload(d, n, r, type, solid, net->stream);
         const int dd[3] = {dims[0], dims[1], dims[2]};
-        net->impl->forward(dd, d.r, d.type, d.solid, d.z, scale, net->stream);
+        if (net->impl->sparse_enabled_) net->impl->plan_sparse(dd, d.type, net->stream);
+        net->impl->forward(dd, d.r, d.type, d.solid, d.z, scale, net->stream, true);
         LHI_CUDA(cudaMemcpyAsync(z, d.z, sizeof(float) * n, cudaMemcpyDeviceToHost, net->stream));
         LHI_CUDA(cudaStreamSynchronize(net->stream));
         const int st = net->impl->check_status(net->stream);

@@ -457,6 +457,7 @@ public:
     bool solid_cell_fresh_ = false;
     uint8_t* net_type_ = nullptr;    // level-0 type with skipped rows (small diagonal) as 0
     bool net_type_fresh_ = false;
+    bool net_plan_stale_ = true;     // the network's tile plan predates net_type_
     float* snaps_ = nullptr;         // recorded residuals [snap_cap_][ncell_]
     int snap_cap_ = 0, snap_count_ = 0, snap_next_ = 0;
     float* train_z_ = nullptr;

@@ -142,6 +142,8 @@ struct ConvParams {
     uint16_t* out_b;
     float* out_f;
     NetStatus* status;
+    const int32_t* tiles;  // brick kernel: the output tiles to evaluate (indices as the dense loop's), or null: all
+    const int* ntiles;     // their count (device)
 };
 
 // Epilogue of one output row (TMEM lane = this thread's row; warp-collective
@@ -307,15 +309,16 @@ __global__ void __launch_bounds__(kConvM) k_conv_brick(ConvParams P) {
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const int tyn = (P.ny + 15) / 16, tzn = (P.nz + 7) / 8;
-    const long long ntiles = (long long)P.nx * tyn * tzn;
+    const long long ntiles = P.tiles ? (long long)*P.ntiles : (long long)P.nx * tyn * tzn;
     const uint32_t idesc = idesc_bf16(kConvM, P.cout, 0, 0);
     const uint32_t bsbo = uint32_t(kc) * 128;
     unsigned phase = 0;
     bool ok = true;
     long long t = blockIdx.x;
     for (; t < ntiles; t += gridDim.x) {
-        const int tzi = int(t % tzn);
-        const long long rest = t / tzn;
+        const long long tt = P.tiles ? (long long)P.tiles[t] : t;
+        const int tzi = int(tt % tzn);
+        const long long rest = tt / tzn;
         const int tyi = int(rest % tyn), x0 = int(rest / tyn);
         const int y0 = tyi * 16, z0 = tzi * 8;
         for (int e = tid; e < kBrVox * kc; e += kConvM) {
@@ -760,6 +763,92 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 
 unsigned nb(long long n, int t = 256) { return unsigned(std::max<long long>(1, (n + t - 1) / t)); }
 
+
+// ------------------------------------------------- sparse evaluation plan
+// Byte masks of the voxels each convolution's output must be right on, and
+// from them the output tiles (the brick kernel's 128-voxel tiles) to
+// evaluate.  Voxels outside these sets may hold stale values: every value a
+// needed voxel reads (its 27 neighbours, its pooled children, its upsampled
+// parent, its skip input) is itself needed, and the tensor-core product of
+// a tile row reads that row's inputs only.
+__global__ void k_mask_type(const uint8_t* __restrict__ type, long long n, uint8_t* __restrict__ m) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) m[v] = type[v] != 0;
+}
+
+// out = in dilated by one voxel along z (axis 0) or along x and y (axis 1)
+__global__ void k_mask_dilate(const uint8_t* __restrict__ in, int nx, int ny, int nz, int axis,
+                              uint8_t* __restrict__ out) {
+    const long long n = (long long)nx * ny * nz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    int x, y, z;
+    dec3(v, ny, nz, x, y, z);
+    uint8_t o = 0;
+    if (axis == 0) {
+        o = in[v];
+        if (z > 0) o |= in[v - 1];
+        if (z + 1 < nz) o |= in[v + 1];
+    } else {
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int xx = x + dx, yy = y + dy;
+                if (xx >= 0 && xx < nx && yy >= 0 && yy < ny) o |= in[((long long)xx * ny + yy) * nz + z];
+            }
+    }
+    out[v] = o;
+}
+
+// coarse voxel set if any of its 8 children is (the voxels whose upsampled
+// value a needed fine voxel reads)
+__global__ void k_mask_up(const uint8_t* __restrict__ fine, int fny, int fnz, int cnx, int cny, int cnz,
+                          uint8_t* __restrict__ coarse) {
+    const long long n = (long long)cnx * cny * cnz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    int x, y, z;
+    dec3(v, cny, cnz, x, y, z);
+    uint8_t o = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        o |= fine[((long long)(2 * x + (k >> 2)) * fny + (2 * y + ((k >> 1) & 1))) * fnz + (2 * z + (k & 1))];
+    coarse[v] = o;
+}
+
+// out = other | (fine voxels whose parent is set: the children a needed
+// pooled voxel averages)
+__global__ void k_mask_down_or(const uint8_t* __restrict__ coarse, int cnx, int cny, int cnz,
+                               const uint8_t* __restrict__ other, int fnx, int fny, int fnz, uint8_t* __restrict__ out) {
+    const long long n = (long long)fnx * fny * fnz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    int x, y, z;
+    dec3(v, fny, fnz, x, y, z);
+    const int px = x >> 1, py = y >> 1, pz = z >> 1;
+    uint8_t o = other[v];
+    if (px < cnx && py < cny && pz < cnz) o |= coarse[((long long)px * cny + py) * cnz + pz];
+    out[v] = o;
+}
+
+// flag[t] = 1 for the brick tiles (x, y / 16, z / 8) holding a set voxel
+__global__ void k_mask_tile_flags(const uint8_t* __restrict__ m, int nx, int ny, int nz, uint8_t* __restrict__ flag) {
+    const long long n = (long long)nx * ny * nz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n || !m[v]) return;
+    int x, y, z;
+    dec3(v, ny, nz, x, y, z);
+    const int tyn = (ny + 15) / 16, tzn = (nz + 7) / 8;
+    flag[((long long)x * tyn + (y >> 4)) * tzn + (z >> 3)] = 1;
+}
+
+// list of the flagged tiles (in any order) and their count
+__global__ void k_mask_tile_list(const uint8_t* __restrict__ flag, long long ntiles, int32_t* __restrict__ list,
+                                 int* __restrict__ count) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles || !flag[t]) return;
+    list[atomicAdd(count, 1)] = int32_t(t);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- host side
@@ -812,6 +901,7 @@ static void free_buffers(NetBuffers& b) {
 
 LearnedNet::~LearnedNet() {
     free_buffers(b_);
+    free_plan();
     auto F = [](void* p) {
         if (p) cudaFree(p);
     };
@@ -897,8 +987,10 @@ void LearnedNet::format_weights(cudaStream_t s) {
 namespace {
 void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const float* bias, int cout_real,
                  const int* d, int mode, const uint16_t* skip, int relu, uint16_t* out_b, float* out_f, NetStatus* st,
-                 cudaStream_t s) {
+                 cudaStream_t s, const int32_t* tiles = nullptr, const int* ntiles_dev = nullptr) {
     ConvParams P;
+    P.tiles = nullptr;  // the gathering kernel evaluates every voxel
+    P.ntiles = nullptr;
     P.in = in;
     P.cin = cin;
     P.w = w;
@@ -930,6 +1022,8 @@ void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const
         const long long ntiles = (long long)d[0] * ((d[1] + 15) / 16) * ((d[2] + 7) / 8);
         const long long per_sm = std::max<long long>(1, (200LL * 1024) / (long long)smem);
         const unsigned grid = unsigned(std::min<long long>(ntiles, kSMs * per_sm));
+        P.tiles = tiles;
+        P.ntiles = tiles ? ntiles_dev : nullptr;
         k_conv_brick<<<grid, kConvM, smem, s>>>(P);
         LHI_LAUNCH_CHECK();
         return;
@@ -962,9 +1056,120 @@ void launch_wgrad(const uint16_t* g, int cout, int cout_real, const uint16_t* in
 }
 }  // namespace
 
-void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type, const uint8_t* solid, float* z,
-                         double scale_fixed, cudaStream_t s) {
+static long long brick_tiles(const int d[3]) { return (long long)d[0] * ((d[1] + 15) / 16) * ((d[2] + 7) / 8); }
+
+void LearnedNet::free_plan() {
+    for (auto& p : mask_) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    for (auto& p : tflag_) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    for (auto& p : tlist_) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    if (tcount_) cudaFree(tcount_);
+    tcount_ = nullptr;
+    plan_type_ = nullptr;
+    plan_cap_vox0_ = 0;
+    for (int& d : plan_dims_) d = 0;
+}
+
+// Needed voxel sets, from the output back to the input (F = type != 0;
+// dil = one-voxel dilation; up = coarse voxels with a needed child;
+// down = fine voxels with a needed parent):
+//   conv5 out F                      (T5)   u0 needed on D = dil(F)
+//   conv4 out D (skip h0 on D)       (T4)   q0 needed on dil(D)
+//   u1 needed on U1 = up(dil(D))
+//   conv3 out U1 (skip h1 on U1)     (T3)   q1 needed on dil(U1)
+//   h2 needed on U2 = up(dil(U1))
+//   conv2 out U2                     (T2)   p1 needed on dil(U2)
+//   h1 needed on H1 = U1 | down(dil(U2))
+//   conv1 out H1                     (T1)   p0 needed on dil(H1)
+//   h0 needed on H0 = D | down(dil(H1))
+//   conv0 out H0                     (T0)   a0 needed on dil(H0): computed everywhere
+// Masks: level 0 A, B; level 1 P, Q; level 2 U, W.
+void LearnedNet::plan_sparse(const int dims[3], const uint8_t* type, cudaStream_t s) {
     ensure(dims);
+    const int* d0 = b_.dims[0];
+    const int* d1 = b_.dims[1];
+    const int* d2 = b_.dims[2];
+    const long long V0 = b_.vox[0], V1 = b_.vox[1], V2 = b_.vox[2];
+    if (plan_cap_vox0_ != V0) {
+        free_plan();
+        const long long vl[7] = {V0, V0, V1, V1, V2, V2, V0};
+        for (int i = 0; i < 7; ++i) LHI_CUDA(cudaMalloc(&mask_[i], size_t(std::max(1LL, vl[i]))));
+        const int* dl[3] = {d0, d1, d2};
+        for (int l = 0; l < 3; ++l) LHI_CUDA(cudaMalloc(&tflag_[l], size_t(std::max(1LL, brick_tiles(dl[l])))));
+        const int lvl[kNetLayers] = {0, 1, 2, 1, 0, 0};
+        for (int l = 0; l < kNetLayers; ++l)
+            LHI_CUDA(cudaMalloc(&tlist_[l], sizeof(int32_t) * size_t(std::max(1LL, brick_tiles(dl[lvl[l]])))));
+        LHI_CUDA(cudaMalloc(&tcount_, sizeof(int) * kNetLayers));
+        plan_cap_vox0_ = V0;
+    }
+    uint8_t *A = mask_[0], *B = mask_[1], *P = mask_[2], *Q = mask_[3], *U = mask_[4], *W = mask_[5];
+    uint8_t* S = mask_[6];  // the dilations' intermediate (sized for level 0, used at every level)
+    LHI_CUDA(cudaMemsetAsync(tcount_, 0, sizeof(int) * kNetLayers, s));
+    auto dil = [&](const uint8_t* in, const int* d, uint8_t* out) {
+        const long long n = (long long)d[0] * d[1] * d[2];
+        if (n == 0) return;
+        k_mask_dilate<<<nb(n), 256, 0, s>>>(in, d[0], d[1], d[2], 0, S);
+        LHI_LAUNCH_CHECK();
+        k_mask_dilate<<<nb(n), 256, 0, s>>>(S, d[0], d[1], d[2], 1, out);
+        LHI_LAUNCH_CHECK();
+    };
+    auto up = [&](const uint8_t* fine, const int* fd, const int* cd, uint8_t* coarse) {
+        const long long n = (long long)cd[0] * cd[1] * cd[2];
+        if (n == 0) return;
+        k_mask_up<<<nb(n), 256, 0, s>>>(fine, fd[1], fd[2], cd[0], cd[1], cd[2], coarse);
+        LHI_LAUNCH_CHECK();
+    };
+    auto down_or = [&](const uint8_t* coarse, const int* cd, const uint8_t* other, const int* fd, uint8_t* out) {
+        const long long n = (long long)fd[0] * fd[1] * fd[2];
+        if (n == 0) return;
+        k_mask_down_or<<<nb(n), 256, 0, s>>>(coarse, cd[0], cd[1], cd[2], other, fd[0], fd[1], fd[2], out);
+        LHI_LAUNCH_CHECK();
+    };
+    auto tiles = [&](const uint8_t* m, const int* d, int level, int layer) {
+        const long long n = (long long)d[0] * d[1] * d[2], nt = brick_tiles(d);
+        if (n == 0) return;
+        LHI_CUDA(cudaMemsetAsync(tflag_[level], 0, size_t(nt), s));
+        k_mask_tile_flags<<<nb(n), 256, 0, s>>>(m, d[0], d[1], d[2], tflag_[level]);
+        LHI_LAUNCH_CHECK();
+        k_mask_tile_list<<<nb(nt), 256, 0, s>>>(tflag_[level], nt, tlist_[layer], tcount_ + layer);
+        LHI_LAUNCH_CHECK();
+    };
+    k_mask_type<<<nb(V0), 256, 0, s>>>(type, V0, A);  // A = F
+    LHI_LAUNCH_CHECK();
+    tiles(A, d0, 0, 5);
+    dil(A, d0, B);  // B = D
+    tiles(B, d0, 0, 4);
+    dil(B, d0, A);  // A = dil(D)
+    up(A, d0, d1, P);  // P = U1
+    tiles(P, d1, 1, 3);
+    dil(P, d1, Q);
+    up(Q, d1, d2, U);  // U = U2
+    tiles(U, d2, 2, 2);
+    dil(U, d2, W);
+    down_or(W, d2, P, d1, Q);  // Q = H1
+    tiles(Q, d1, 1, 1);
+    dil(Q, d1, P);
+    down_or(P, d1, B, d0, A);  // A = H0
+    tiles(A, d0, 0, 0);
+    plan_type_ = type;
+    for (int a = 0; a < 3; ++a) plan_dims_[a] = dims[a];
+}
+
+void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type, const uint8_t* solid, float* z,
+                         double scale_fixed, cudaStream_t s, bool sparse) {
+    ensure(dims);
+    sparse = sparse && sparse_enabled_ && plan_type_ == type && plan_cap_vox0_ == b_.vox[0] &&
+             plan_dims_[0] == dims[0] && plan_dims_[1] == dims[1] && plan_dims_[2] == dims[2];
+    auto TL = [&](int l) -> const int32_t* { return sparse ? tlist_[l] : nullptr; };
+    auto TC = [&](int l) -> const int* { return sparse ? tcount_ + l : nullptr; };
     if (wfmt_stale_) format_weights(s);
     last_type_ = type;
     const int* d0 = b_.dims[0];
@@ -987,20 +1192,20 @@ void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type,
         return nullptr;
     };
     const int act = relu_ ? 1 : 0;
-    launch_conv(b_.a0, 16, W(0), 16, Bv(0), 16, d0, 0, nullptr, act, b_.h0, nullptr, status_, s);
+    launch_conv(b_.a0, 16, W(0), 16, Bv(0), 16, d0, 0, nullptr, act, b_.h0, nullptr, status_, s, TL(0), TC(0));
     k_pool<<<nb(b_.vox[1] * 16), 256, 0, s>>>(b_.h0, d0[1], d0[2], b_.p0, d1[0], d1[1], d1[2], 16);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.p0, 16, W(1), 32, Bv(1), 32, d1, 0, nullptr, act, b_.h1, nullptr, status_, s);
+    launch_conv(b_.p0, 16, W(1), 32, Bv(1), 32, d1, 0, nullptr, act, b_.h1, nullptr, status_, s, TL(1), TC(1));
     k_pool<<<nb(b_.vox[2] * 32), 256, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[0], d2[1], d2[2], 32);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, act, b_.h2, nullptr, status_, s);
+    launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, act, b_.h2, nullptr, status_, s, TL(2), TC(2));
     k_upsample<<<nb(b_.vox[1] * 64 / 8), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, act, b_.u1, nullptr, status_, s);
+    launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, act, b_.u1, nullptr, status_, s, TL(3), TC(3));
     k_upsample<<<nb(V0 * 32 / 8), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
     LHI_LAUNCH_CHECK();
-    launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, act, b_.u0, nullptr, status_, s);
-    launch_conv(b_.u0, 16, W(5), 16, Bv(5), 1, d0, 2, nullptr, 0, nullptr, b_.y, status_, s);
+    launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, act, b_.u0, nullptr, status_, s, TL(4), TC(4));
+    launch_conv(b_.u0, 16, W(5), 16, Bv(5), 1, d0, 2, nullptr, 0, nullptr, b_.y, status_, s, TL(5), TC(5));
     k_net_output<<<nb(V0), 256, 0, s>>>(b_.y, type, V0, scale_, z);
     LHI_LAUNCH_CHECK();
 }

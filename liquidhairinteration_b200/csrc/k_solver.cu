@@ -2161,8 +2161,12 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_precond() {
                 ensure_solid_cells();
                 ensure_net_type();
                 const int dims[3] = {nx_, ny_, nz_};
+                if (net_->sparse_enabled_ && (net_plan_stale_ || net_->plan_type_ != net_type_)) {
+                    net_->plan_sparse(dims, net_type_, cur_);
+                    net_plan_stale_ = false;
+                }
                 net_->forward(dims, reinterpret_cast<const float*>(L0.r), net_type_, solid_cell_,
-                              reinterpret_cast<float*>(L0.z), 0.0, cur_);
+                              reinterpret_cast<float*>(L0.z), 0.0, cur_, true);
                 break;
             }
             enqueue_vcycle();
@@ -2531,6 +2535,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::ensure_net_type() {
     k_net_type<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(lv_[0].type, lv_[0].diag, ncell_, net_type_);
     LHI_LAUNCH_CHECK();
     net_type_fresh_ = true;
+    net_plan_stale_ = true;
 }
 
 template <class T, class TX> void LiquidImpl<T, TX>::record_residuals(int max_snapshots) {

@@ -110,8 +110,14 @@ public:
     void get_params(float* host);
     // z = M(r) on a grid of dims n (device pointers, float), fluid = type == 2
     // cells, solid from the cell-centre solid flag, stream s.
+    // sparse: evaluate each convolution only on the output tiles the cells
+    // with type != 0 depend on (the plan of plan_sparse for this type array;
+    // dense when there is none): the same values there, bit for bit.
     void forward(const int dims[3], const float* r, const uint8_t* type, const uint8_t* solid, float* z,
-                 double scale_fixed, cudaStream_t s);
+                 double scale_fixed, cudaStream_t s, bool sparse = false);
+    // Tile lists of the six convolutions for the output cells type != 0 of
+    // this grid (device type array; rebuilt whenever the cells change).
+    void plan_sparse(const int dims[3], const uint8_t* type, cudaStream_t s);
     // d(loss)/d(params) += backward of the last forward given dL/dz (device, float); returns in grad_
     void backward(const float* dz, cudaStream_t s);
     void zero_grad(cudaStream_t s);
@@ -141,6 +147,19 @@ public:
 
     void ensure(const int dims[3]);
     void format_weights(cudaStream_t s);
+
+    // sparse evaluation (plan_sparse): voxel masks (level 0: two, level 1:
+    // two, level 2: two, and the dilations' intermediate), tile flags per
+    // level, tile list and count per layer
+    bool sparse_enabled_ = true;
+    const uint8_t* plan_type_ = nullptr;
+    int plan_dims_[3] = {0, 0, 0};
+    uint8_t* mask_[7] = {};
+    uint8_t* tflag_[3] = {};
+    int32_t* tlist_[kNetLayers] = {};
+    int* tcount_ = nullptr;  // [kNetLayers] on the device
+    long long plan_cap_vox0_ = 0;
+    void free_plan();
 };
 
 // One-CTA tcgen05 GEMM check: D = A B^T, A 128 x K, B N x K (BF16 bits,

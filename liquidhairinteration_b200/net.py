@@ -74,6 +74,11 @@ class LearnedNet:
         """ReLU between layers (default off: a linear multilevel operator)."""
         call("lhi_net_set_relu", self._h, 1 if on else 0)
 
+    def set_sparse(self, on):
+        """Evaluate each convolution only on the output tiles the cells with
+        type != 0 depend on (default on; the result is the same, bit for bit)."""
+        call("lhi_net_set_sparse", self._h, 1 if on else 0)
+
     def save(self, path):
         call("lhi_net_save", self._h, str(path).encode())
 
