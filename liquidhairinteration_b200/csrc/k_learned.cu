@@ -21,6 +21,7 @@
 
 #include "net.cuh"
 #include "lhi.h"
+#include "tma.cuh"
 
 namespace lhi {
 
@@ -280,30 +281,65 @@ __global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
 // z fastest, so for any tap the 8 z of a y row are one contiguous 8 x 16-byte
 // core matrix: the tap's A operand is the brick at offset (dx, dy, dz), with
 // M-direction stride one brick row (160 bytes) and K-direction stride one
-// plane.  CTAs are persistent and keep all 27 weight tiles resident.
+// plane.  Each plane is one TMA box {8 channels, 10 z, 18 y, 3 x} of the
+// channels-last activations (a 4D tensor map, channels innermost), which
+// reads zeros outside the grid: the convolution's zero padding.  CTAs are
+// persistent, keep all 27 weight tiles resident and, where shared memory
+// holds two bricks, load the next tile's brick while the tensor cores work
+// on this one (with one brick, while this tile's epilogue runs).
 constexpr int kBrX = 3, kBrY = 18, kBrZ = 10;
 constexpr int kBrVox = kBrX * kBrY * kBrZ;  // 540
-constexpr int kBrPlane = kBrVox * 16;       // bytes of one 8-channel plane
+constexpr int kBrBox = kBrVox * 16;         // bytes of one 8-channel plane (one TMA box)
+constexpr int kBrPlane = 68 * 128;          // plane stride: the box rounded up to 128 bytes
 constexpr size_t kBrickSmemMax = 227 * 1024;
+constexpr int kBrBars = 32;                 // three mbarriers and the TMEM address slot
 
-__global__ void __launch_bounds__(kConvM) k_conv_brick(ConvParams P) {
+// Shared-memory bytes of the brick kernel for one layer with `stages` bricks.
+__host__ __device__ constexpr size_t brick_smem_bytes(int cin, int cout, int stages) {
+    return size_t(27) * cout * cin * 2 + size_t(stages) * (cin / 8) * kBrPlane + kBrBars;
+}
+
+__device__ __forceinline__ void brick_tile(const ConvParams& P, long long t, int tyn, int tzn, int& x0, int& y0,
+                                           int& z0) {
+    const long long tt = P.tiles ? (long long)P.tiles[t] : t;
+    const int tzi = int(tt % tzn);
+    const long long rest = tt / tzn;
+    y0 = int(rest % tyn) * 16;
+    x0 = int(rest / tyn);
+    z0 = tzi * 8;
+}
+
+// one thread: the kc planes of tile t's brick into brick buffer `stage`
+__device__ __forceinline__ void brick_issue(const CUtensorMap* tin, const ConvParams& P, long long t, int tyn, int tzn,
+                                            int kc, uint8_t* buf, uint64_t* bar) {
+    int x0, y0, z0;
+    brick_tile(P, t, tyn, tzn, x0, y0, z0);
+    bar_expect_tx(bar, uint32_t(kc * kBrBox));
+    for (int c = 0; c < kc; ++c) tma_load_box4(buf + c * kBrPlane, tin, c * 8, z0 - 1, y0 - 1, x0 - 1, bar);
+}
+
+__global__ void __launch_bounds__(kConvM) k_conv_brick(const __grid_constant__ CUtensorMap tin, ConvParams P,
+                                                       int stages) {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int kc = P.cin / 8;
     const int wbytes = P.cout * P.cin * 2;  // one tap's B tile
     uint8_t* Bs = sm;
-    uint8_t* Ab = sm + 27 * wbytes;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Ab + kc * kBrPlane);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    uint8_t* Ab = sm + 27 * wbytes;  // stage s at Ab + s * kc * kBrPlane
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ab + stages * kc * kBrPlane);  // [0], [1] bricks, [2] MMAs
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 3);
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t ncols = P.cout < 32 ? 32u : uint32_t(P.cout);
     if (tid == 0) {
         mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
     if (warp == 0) tmem_alloc(tslot, ncols);
     for (int i = tid; i < 27 * wbytes / 16; i += kConvM)
         reinterpret_cast<uint4*>(Bs)[i] = reinterpret_cast<const uint4*>(P.w)[i];
+    fence_async_smem();  // the weight tiles (generic stores) before the tensor cores read them
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -312,55 +348,71 @@ __global__ void __launch_bounds__(kConvM) k_conv_brick(ConvParams P) {
     const long long ntiles = P.tiles ? (long long)*P.ntiles : (long long)P.nx * tyn * tzn;
     const uint32_t idesc = idesc_bf16(kConvM, P.cout, 0, 0);
     const uint32_t bsbo = uint32_t(kc) * 128;
-    unsigned phase = 0;
+    bool pending[2] = {false, false};  // thread 0: a brick load in flight on bar[s] and not yet waited for
+    unsigned use[2] = {0u, 0u};        // thread 0: completed waits per brick barrier (its phase parity)
+    if (tid == 0 && (long long)blockIdx.x < ntiles) {
+        brick_issue(&tin, P, blockIdx.x, tyn, tzn, kc, Ab, &bar[0]);
+        pending[0] = true;
+    }
     bool ok = true;
+    int it = 0;
     long long t = blockIdx.x;
-    for (; t < ntiles; t += gridDim.x) {
-        const long long tt = P.tiles ? (long long)P.tiles[t] : t;
-        const int tzi = int(tt % tzn);
-        const long long rest = tt / tzn;
-        const int tyi = int(rest % tyn), x0 = int(rest / tyn);
-        const int y0 = tyi * 16, z0 = tzi * 8;
-        for (int e = tid; e < kBrVox * kc; e += kConvM) {
-            const int c = e / kBrVox, vb = e - c * kBrVox;
-            const int bx = vb / (kBrY * kBrZ), r2 = vb - bx * (kBrY * kBrZ);
-            const int by = r2 / kBrZ, bz = r2 - by * kBrZ;
-            const int xx = x0 - 1 + bx, yy = y0 - 1 + by, zz = z0 - 1 + bz;
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
-            if (xx >= 0 && xx < P.nx && yy >= 0 && yy < P.ny && zz >= 0 && zz < P.nz)
-                val = *reinterpret_cast<const uint4*>(P.in + (((long long)xx * P.ny + yy) * P.nz + zz) * P.cin + c * 8);
-            *reinterpret_cast<uint4*>(Ab + c * kBrPlane + vb * 16) = val;
-        }
-        fence_async_smem();
-        __syncthreads();
+    for (; t < ntiles; t += gridDim.x, ++it) {
+        const int s = stages == 2 ? (it & 1) : 0;
+        const long long tn = t + gridDim.x;
         if (tid == 0) {
-            tc_fence_after();
-            const uint32_t a0 = smem_u32(Ab), b0 = smem_u32(Bs);
-            for (int tap = 0; tap < kNetTaps; ++tap) {
-                int dx, dy, dz;
-                tap_offset(tap, dx, dy, dz);
-                const uint32_t at = a0 + uint32_t((((dx + 1) * kBrY + (dy + 1)) * kBrZ + (dz + 1)) * 16);
-                const uint32_t bt = b0 + uint32_t(tap * wbytes);
-                for (int k = 0; k < P.cin / 16; ++k)
-                    umma_bf16(tmem, sdesc(at + uint32_t(2 * k * kBrPlane), kBrPlane, kBrZ * 16),
-                              sdesc(bt + k * 256, 128, bsbo), idesc, (tap > 0 || k > 0) ? 1u : 0u);
+            // two bricks: the other one was last read by the previous tile's
+            // MMAs, which completed before that tile's epilogue
+            if (stages == 2 && tn < ntiles) {
+                brick_issue(&tin, P, tn, tyn, tzn, kc, Ab + (s ^ 1) * kc * kBrPlane, &bar[s ^ 1]);
+                pending[s ^ 1] = true;
             }
-            umma_commit(&bar[0]);
+            const bool landed = mbar_wait(&bar[s], use[s] & 1u);
+            if (landed) {
+                pending[s] = false;
+                ++use[s];
+                tc_fence_after();
+                const uint32_t a0 = smem_u32(Ab + s * kc * kBrPlane), b0 = smem_u32(Bs);
+                for (int tap = 0; tap < kNetTaps; ++tap) {
+                    int dx, dy, dz;
+                    tap_offset(tap, dx, dy, dz);
+                    const uint32_t at = a0 + uint32_t((((dx + 1) * kBrY + (dy + 1)) * kBrZ + (dz + 1)) * 16);
+                    const uint32_t bt = b0 + uint32_t(tap * wbytes);
+                    for (int k = 0; k < P.cin / 16; ++k)
+                        umma_bf16(tmem, sdesc(at + uint32_t(2 * k * kBrPlane), kBrPlane, kBrZ * 16),
+                                  sdesc(bt + k * 256, 128, bsbo), idesc, (tap > 0 || k > 0) ? 1u : 0u);
+                }
+            } else {
+                ok = false;
+            }
+            umma_commit(&bar[2]);  // with no MMA issued it arrives at once
         }
-        ok = mbar_wait(&bar[0], phase);
-        phase ^= 1u;
+        const bool mma_done = mbar_wait(&bar[2], unsigned(it) & 1u);
+        // the epilogue's TMEM loads are warp-collective: one decision for the CTA
+        ok = __syncthreads_and(ok && mma_done);
+        if (!ok) break;
+        if (tid == 0 && stages == 1 && tn < ntiles) {  // the brick is free: load the next one
+            brick_issue(&tin, P, tn, tyn, tzn, kc, Ab, &bar[0]);
+            pending[0] = true;
+        }
         tc_fence_after();
-        __syncwarp();
+        int x0, y0, z0;
+        brick_tile(P, t, tyn, tzn, x0, y0, z0);
         const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
         const bool valid = y < P.ny && z < P.nz;
-        if (ok) conv_store(P, tmem + (uint32_t(warp * 32) << 16), valid, ((long long)x0 * P.ny + y) * P.nz + z);
+        conv_store(P, tmem + (uint32_t(warp * 32) << 16), valid, ((long long)x0 * P.ny + y) * P.nz + z);
         tc_fence_before();
-        // the brick and TMEM are free for the next tile; a timeout ends the CTA
-        if (!__syncthreads_and(ok)) break;
+        __syncthreads();  // TMEM is free for the next tile's MMAs
     }
-    if (t < ntiles && tid == 0 && atomicExch(&P.status->timeout, 1) == 0) {
-        P.status->pad[0] = 3;  // kernel: brick convolution
-        P.status->pad[2] = int(blockIdx.x);
+    if (t < ntiles && tid == 0) {
+        if (atomicExch(&P.status->timeout, 1) == 0) {
+            P.status->pad[0] = 3;  // kernel: brick convolution
+            P.status->pad[2] = int(blockIdx.x);
+        }
+        // no brick load of this CTA may still be landing when it exits
+        for (int b = 0; b < 2; ++b)
+            if (pending[b]) mbar_wait(&bar[b], use[b] & 1u);
+        mbar_wait(&bar[2], unsigned(it) & 1u);
     }
     tc_fence_before();
     __syncthreads();
@@ -1010,21 +1062,36 @@ void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const
     if (P.nvox == 0) return;
     // the brick kernel keeps all 27 weight tiles and the brick in shared
     // memory: every layer but the 64 -> 64 input gradient fits
-    const size_t brick_smem = size_t(27) * cout * cin * 2 + size_t(cin / 8) * kBrPlane + 16;
-    if (brick_smem <= kBrickSmemMax) {
-        const size_t smem = brick_smem;
+    if (brick_smem_bytes(cin, cout, 1) <= kBrickSmemMax) {
+        const int stages = brick_smem_bytes(cin, cout, 2) <= kBrickSmemMax ? 2 : 1;
+        const size_t smem = brick_smem_bytes(cin, cout, stages);
         static bool attr = false;
         if (!attr) {
             LHI_CUDA(cudaFuncSetAttribute(k_conv_brick, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(kBrickSmemMax)));
             attr = true;
         }
+        // the input as a 4D tensor (channel, z, y, x), boxes of one 8-channel
+        // plane of a brick; zeros outside the grid
+        CUtensorMap tin;
+        const cuuint64_t dims[4] = {cuuint64_t(cin), cuuint64_t(d[2]), cuuint64_t(d[1]), cuuint64_t(d[0])};
+        const cuuint64_t strides[3] = {cuuint64_t(cin) * 2, cuuint64_t(cin) * 2 * d[2],
+                                       cuuint64_t(cin) * 2 * d[2] * d[1]};
+        const cuuint32_t box[4] = {8, cuuint32_t(kBrZ), cuuint32_t(kBrY), cuuint32_t(kBrX)};
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        const CUresult r = tensor_map_encoder()(&tin, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, const_cast<uint16_t*>(in),
+                                                dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            throw CudaError(cudaErrorInvalidValue, "brick tensor map: cuTensorMapEncodeTiled failed with CUresult " +
+                                                       std::to_string(int(r)));
         const long long ntiles = (long long)d[0] * ((d[1] + 15) / 16) * ((d[2] + 7) / 8);
-        const long long per_sm = std::max<long long>(1, (200LL * 1024) / (long long)smem);
+        const long long per_sm = std::max<long long>(1, (228LL * 1024) / (long long)(smem + 1024));
         const unsigned grid = unsigned(std::min<long long>(ntiles, kSMs * per_sm));
         P.tiles = tiles;
         P.ntiles = tiles ? ntiles_dev : nullptr;
-        k_conv_brick<<<grid, kConvM, smem, s>>>(P);
+        k_conv_brick<<<grid, kConvM, smem, s>>>(tin, P, stages);
         LHI_LAUNCH_CHECK();
         return;
     }

@@ -20,8 +20,7 @@ namespace lhi {
 
 // Host: a 3D tiled map over base[nx][ny][pitch] of esz-byte elements whose
 // valid z extent is nz, copying boxes of (bz, by, bx) elements.
-inline CUtensorMap make_box_map(const void* base, CUtensorMapDataType dt, int esz, int nx, int ny, int nz,
-                                int pitch, int bx, int by, int bz) {
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void* fn = nullptr;
@@ -31,6 +30,12 @@ inline CUtensorMap make_box_map(const void* base, CUtensorMapDataType dt, int es
             throw CudaError(cudaErrorNotSupported, "cuTensorMapEncodeTiled is not available from the driver");
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
+    return encode;
+}
+
+inline CUtensorMap make_box_map(const void* base, CUtensorMapDataType dt, int esz, int nx, int ny, int nz,
+                                int pitch, int bx, int by, int bz) {
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
     CUtensorMap m;
     const cuuint64_t dims[3] = {cuuint64_t(nz), cuuint64_t(ny), cuuint64_t(nx)};
     const cuuint64_t strides[2] = {cuuint64_t(pitch) * esz, cuuint64_t(pitch) * ny * esz};
@@ -66,6 +71,16 @@ __device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map, 
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
             smem_addr(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(z), "r"(y), "r"(x), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// 4D box load at element coordinates (c0 innermost .. c3) into dst.
+__device__ __forceinline__ void tma_load_box4(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                              uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
         : "memory");
 }
 

@@ -9,8 +9,9 @@ any change to them.
   work item.
 - Brick convolution (k_conv_brick): for every tap and K step, each 8-row
   core matrix the tensor-core instruction reads (16 along M, 2 along K) lies
-  inside the input brick and is the intended brick row of 8 z voxels, and
-  each weight core matrix lies inside its tap's tile.
+  inside the input brick and is the intended brick row of 8 z voxels, each
+  weight core matrix lies inside its tap's tile, and every TMA box of every
+  brick stage lands 128-byte aligned inside its own plane.
 """
 import os
 import re
@@ -59,16 +60,27 @@ def test_box_constants_match_the_kernels():
 def test_brick_convolution_operands_inside_tiles(cin, cout):
     by, bz = _const("k_learned.cu", "kBrY"), _const("k_learned.cu", "kBrZ")
     bx = _const("k_learned.cu", "kBrX")
-    plane = bx * by * bz * 16
+    box = bx * by * bz * 16  # bytes of one TMA box: 8 channels of every brick voxel
+    plane = _const("k_learned.cu", "kBrPlane")
     limit = _const("k_learned.cu", "kBrickSmemMax")
+    bars = _const("k_learned.cu", "kBrBars")
+    assert box <= plane and plane % 128 == 0
+    assert bars >= 3 * 8 + 4  # three mbarriers and the TMEM address slot
     kc = cin // 8
     wbytes = cout * cin * 2
     a_base = 27 * wbytes
-    brick_end = a_base + kc * plane
-    smem = brick_end + 16
-    if smem > limit:
+    smem1 = a_base + kc * plane + bars
+    if smem1 > limit:
         pytest.skip("this layer runs the gathering kernel")
-    assert a_base % 16 == 0 and brick_end % 8 == 0  # operands 16-byte, mbarrier 8-byte aligned
+    stages = 2 if a_base + 2 * kc * plane + bars <= limit else 1
+    brick_end = a_base + kc * plane  # stage 0; the operand checks below hold for stage 1 shifted by kc planes
+    smem = a_base + stages * kc * plane + bars
+    assert smem <= limit
+    assert a_base % 128 == 0 and (a_base + stages * kc * plane) % 8 == 0  # TMA 128-byte, mbarrier 8-byte aligned
+    for st in range(stages):
+        for c in range(kc):
+            dst = a_base + (st * kc + c) * plane
+            assert dst % 128 == 0 and dst + box <= a_base + (st * kc + c + 1) * plane
     assert smem < (1 << 18)  # 14-bit descriptor address field in 16-byte units
     for tap in range(27):
         dx, dy, dz = tap // 9 - 1, (tap // 3) % 3 - 1, tap % 3 - 1
