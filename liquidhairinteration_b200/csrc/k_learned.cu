@@ -283,16 +283,20 @@ __global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
 // M-direction stride one brick row (160 bytes) and K-direction stride one
 // plane.  Each plane is one TMA box {8 channels, 10 z, 18 y, 3 x} of the
 // channels-last activations (a 4D tensor map, channels innermost), which
-// reads zeros outside the grid: the convolution's zero padding.  CTAs are
-// persistent, keep all 27 weight tiles resident and, where shared memory
-// holds two bricks, load the next tile's brick while the tensor cores work
-// on this one (with one brick, while this tile's epilogue runs).
+// reads zeros outside the grid: the convolution's zero padding.
+//
+// CTAs are persistent and keep all 27 weight tiles resident.  The tiles of a
+// CTA run as a pipeline over two TMEM accumulators: in step i thread 0 issues
+// tile i's MMAs (the descriptors are compile-time offsets from two bases)
+// while all four warps drain tile i - 1's accumulator (with its skip input
+// loaded one step ahead); where shared memory holds two bricks, tile i + 1's
+// brick is loaded during step i as well.
 constexpr int kBrX = 3, kBrY = 18, kBrZ = 10;
 constexpr int kBrVox = kBrX * kBrY * kBrZ;  // 540
 constexpr int kBrBox = kBrVox * 16;         // bytes of one 8-channel plane (one TMA box)
 constexpr int kBrPlane = 68 * 128;          // plane stride: the box rounded up to 128 bytes
 constexpr size_t kBrickSmemMax = 227 * 1024;
-constexpr int kBrBars = 32;                 // three mbarriers and the TMEM address slot
+constexpr int kBrBars = 48;                 // four mbarriers and the TMEM address slot
 
 // Shared-memory bytes of the brick kernel for one layer with `stages` bricks.
 __host__ __device__ constexpr size_t brick_smem_bytes(int cin, int cout, int stages) {
@@ -309,7 +313,7 @@ __device__ __forceinline__ void brick_tile(const ConvParams& P, long long t, int
     z0 = tzi * 8;
 }
 
-// one thread: the kc planes of tile t's brick into brick buffer `stage`
+// one thread: the kc planes of tile t's brick into buf
 __device__ __forceinline__ void brick_issue(const CUtensorMap* tin, const ConvParams& P, long long t, int tyn, int tzn,
                                             int kc, uint8_t* buf, uint64_t* bar) {
     int x0, y0, z0;
@@ -318,26 +322,85 @@ __device__ __forceinline__ void brick_issue(const CUtensorMap* tin, const ConvPa
     for (int c = 0; c < kc; ++c) tma_load_box4(buf + c * kBrPlane, tin, c * 8, z0 - 1, y0 - 1, x0 - 1, bar);
 }
 
+// one thread: the 27 x CIN/16 MMAs of one tile, accumulating into acc
+template <int CIN, int COUT>
+__device__ __forceinline__ void brick_mmas(uint32_t acc, uint32_t a_stage, uint32_t b0) {
+    constexpr int KC = CIN / 8;
+    constexpr uint32_t idesc = idesc_bf16(kConvM, COUT, 0, 0);
+    const uint64_t ad0 = sdesc(a_stage, kBrPlane, kBrZ * 16);
+    const uint64_t bd0 = sdesc(b0, 128, uint32_t(KC) * 128);
+#pragma unroll
+    for (int tap = 0; tap < kNetTaps; ++tap) {
+        const int dx = tap / 9, dy = (tap / 3) % 3, dz = tap % 3;  // offsets + 1
+        const uint64_t aoff = uint64_t(((dx * kBrY + dy) * kBrZ + dz) * 16) >> 4;
+#pragma unroll
+        for (int k = 0; k < CIN / 16; ++k)
+            umma_bf16(acc, ad0 + aoff + (uint64_t(2 * k * kBrPlane) >> 4),
+                      bd0 + (uint64_t(tap * COUT * CIN * 2 + k * 256) >> 4), idesc, (tap > 0 || k > 0) ? 1u : 0u);
+    }
+}
+
+// Epilogue of one output row (TMEM lane = this thread's row; the loads are
+// warp-collective, so every lane calls it and only valid rows store), the
+// arithmetic of conv_store: mode 0 BF16 with bias, skip (sk, loaded ahead)
+// and activation; mode 1 FP32, all channels; mode 2 FP32 channel 0.
+template <int COUT>
+__device__ __forceinline__ void brick_store(const ConvParams& P, uint32_t trow, bool valid, long long v,
+                                            const uint4 (&sk)[COUT / 8]) {
+    if (P.mode == 2) {
+        float a[8];
+        tmem_ld8(trow, a);
+        if (valid) P.out_f[v] = a[0] + (P.bias ? P.bias[0] : 0.f);
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < COUT / 8; ++q) {
+        const int c0 = q * 8;
+        float a[8];
+        tmem_ld8(trow + c0, a);
+        if (!valid) continue;
+        if (P.mode == 1) {
+            float4* o = reinterpret_cast<float4*>(P.out_f + v * COUT + c0);
+            o[0] = make_float4(a[0], a[1], a[2], a[3]);
+            o[1] = make_float4(a[4], a[5], a[6], a[7]);
+        } else {
+            uint16_t s8[8];
+            *reinterpret_cast<uint4*>(s8) = sk[q];
+            uint16_t o[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int c = c0 + k;
+                float val = a[k];
+                if (P.bias && c < P.cout_real) val += P.bias[c];
+                if (P.skip) val += bf16_float(s8[k]);
+                if (P.relu) val = fmaxf(val, 0.f);
+                o[k] = (c < P.cout_real) ? bf16_bits(val) : uint16_t(0);
+            }
+            *reinterpret_cast<uint4*>(P.out_b + v * COUT + c0) = *reinterpret_cast<uint4*>(o);
+        }
+    }
+}
+
+// Barriers: [0], [1] brick stages (TMA), [2], [3] accumulators (MMA commit).
+template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvM) k_conv_brick(const __grid_constant__ CUtensorMap tin, ConvParams P,
                                                        int stages) {
     extern __shared__ __align__(1024) uint8_t sm[];
-    const int kc = P.cin / 8;
-    const int wbytes = P.cout * P.cin * 2;  // one tap's B tile
+    constexpr int KC = CIN / 8;
+    constexpr int WBYTES = COUT * CIN * 2;  // one tap's B tile
+    constexpr uint32_t NCOLS = COUT < 32 ? 32u : uint32_t(COUT);
     uint8_t* Bs = sm;
-    uint8_t* Ab = sm + 27 * wbytes;  // stage s at Ab + s * kc * kBrPlane
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Ab + stages * kc * kBrPlane);  // [0], [1] bricks, [2] MMAs
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 3);
+    uint8_t* Ab = sm + 27 * WBYTES;  // stage s at Ab + s * KC * kBrPlane
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ab + stages * KC * kBrPlane);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 4);
     const int tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t ncols = P.cout < 32 ? 32u : uint32_t(P.cout);
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_init(&bar[2], 1);
+        for (int b = 0; b < 4; ++b) mbar_init(&bar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
-    if (warp == 0) tmem_alloc(tslot, ncols);
-    for (int i = tid; i < 27 * wbytes / 16; i += kConvM)
+    if (warp == 0) tmem_alloc(tslot, 2 * NCOLS);
+    for (int i = tid; i < 27 * WBYTES / 16; i += kConvM)
         reinterpret_cast<uint4*>(Bs)[i] = reinterpret_cast<const uint4*>(P.w)[i];
     fence_async_smem();  // the weight tiles (generic stores) before the tensor cores read them
     tc_fence_before();
@@ -346,78 +409,103 @@ __global__ void __launch_bounds__(kConvM) k_conv_brick(const __grid_constant__ C
     const uint32_t tmem = *tslot;
     const int tyn = (P.ny + 15) / 16, tzn = (P.nz + 7) / 8;
     const long long ntiles = P.tiles ? (long long)*P.ntiles : (long long)P.nx * tyn * tzn;
-    const uint32_t idesc = idesc_bf16(kConvM, P.cout, 0, 0);
-    const uint32_t bsbo = uint32_t(kc) * 128;
-    bool pending[2] = {false, false};  // thread 0: a brick load in flight on bar[s] and not yet waited for
-    unsigned use[2] = {0u, 0u};        // thread 0: completed waits per brick barrier (its phase parity)
+    const long long G = gridDim.x;
+    // thread 0's bookkeeping: brick loads in flight and completed per stage,
+    // and the step of its last MMA commit
+    bool pending[2] = {false, false};
+    unsigned use[2] = {0u, 0u};
+    int last_commit = -1;
     if (tid == 0 && (long long)blockIdx.x < ntiles) {
-        brick_issue(&tin, P, blockIdx.x, tyn, tzn, kc, Ab, &bar[0]);
+        brick_issue(&tin, P, blockIdx.x, tyn, tzn, KC, Ab, &bar[0]);
         pending[0] = true;
     }
+    uint4 sk_next[COUT / 8], sk_cur[COUT / 8];  // skip rows of this step's tile, of the previous one
+#pragma unroll
+    for (int q = 0; q < COUT / 8; ++q) sk_next[q] = sk_cur[q] = make_uint4(0u, 0u, 0u, 0u);
     bool ok = true;
     int it = 0;
     long long t = blockIdx.x;
-    for (; t < ntiles; t += gridDim.x, ++it) {
+    for (;; ++it, t += G) {
+        const bool have = t < ntiles;
+        if (!have && it == 0) break;
         const int s = stages == 2 ? (it & 1) : 0;
-        const long long tn = t + gridDim.x;
-        if (tid == 0) {
-            // two bricks: the other one was last read by the previous tile's
-            // MMAs, which completed before that tile's epilogue
-            if (stages == 2 && tn < ntiles) {
-                brick_issue(&tin, P, tn, tyn, tzn, kc, Ab + (s ^ 1) * kc * kBrPlane, &bar[s ^ 1]);
-                pending[s ^ 1] = true;
+        if (tid == 0 && have) {
+            const long long tn = t + G;
+            if (stages == 1 && it > 0) {
+                // the one brick was read by the previous tile's MMAs: reload it when they are done
+                if (mbar_wait(&bar[2 + ((it - 1) & 1)], unsigned((it - 1) >> 1) & 1u)) {
+                    brick_issue(&tin, P, t, tyn, tzn, KC, Ab, &bar[0]);
+                    pending[0] = true;
+                } else {
+                    ok = false;
+                }
             }
-            const bool landed = mbar_wait(&bar[s], use[s] & 1u);
-            if (landed) {
+            if (ok && stages == 2 && tn < ntiles) {
+                // the other brick was read by the previous tile's MMAs
+                if (it == 0 || mbar_wait(&bar[2 + ((it - 1) & 1)], unsigned((it - 1) >> 1) & 1u)) {
+                    brick_issue(&tin, P, tn, tyn, tzn, KC, Ab + (s ^ 1) * KC * kBrPlane, &bar[s ^ 1]);
+                    pending[s ^ 1] = true;
+                } else {
+                    ok = false;
+                }
+            }
+            if (ok && mbar_wait(&bar[s], use[s] & 1u)) {
                 pending[s] = false;
                 ++use[s];
                 tc_fence_after();
-                const uint32_t a0 = smem_u32(Ab + s * kc * kBrPlane), b0 = smem_u32(Bs);
-                for (int tap = 0; tap < kNetTaps; ++tap) {
-                    int dx, dy, dz;
-                    tap_offset(tap, dx, dy, dz);
-                    const uint32_t at = a0 + uint32_t((((dx + 1) * kBrY + (dy + 1)) * kBrZ + (dz + 1)) * 16);
-                    const uint32_t bt = b0 + uint32_t(tap * wbytes);
-                    for (int k = 0; k < P.cin / 16; ++k)
-                        umma_bf16(tmem, sdesc(at + uint32_t(2 * k * kBrPlane), kBrPlane, kBrZ * 16),
-                                  sdesc(bt + k * 256, 128, bsbo), idesc, (tap > 0 || k > 0) ? 1u : 0u);
-                }
+                brick_mmas<CIN, COUT>(tmem + uint32_t(it & 1) * NCOLS, smem_u32(Ab + s * KC * kBrPlane),
+                                      smem_u32(Bs));
+                umma_commit(&bar[2 + (it & 1)]);
+                last_commit = it;
             } else {
                 ok = false;
             }
-            umma_commit(&bar[2]);  // with no MMA issued it arrives at once
         }
-        const bool mma_done = mbar_wait(&bar[2], unsigned(it) & 1u);
-        // the epilogue's TMEM loads are warp-collective: one decision for the CTA
-        ok = __syncthreads_and(ok && mma_done);
-        if (!ok) break;
-        if (tid == 0 && stages == 1 && tn < ntiles) {  // the brick is free: load the next one
-            brick_issue(&tin, P, tn, tyn, tzn, kc, Ab, &bar[0]);
-            pending[0] = true;
+        // this tile's skip rows, for its epilogue in the next step
+        if (have && P.mode == 0 && P.skip) {
+            int x0, y0, z0;
+            brick_tile(P, t, tyn, tzn, x0, y0, z0);
+            const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
+            if (y < P.ny && z < P.nz) {
+                const uint4* src = reinterpret_cast<const uint4*>(P.skip + (((long long)x0 * P.ny + y) * P.nz + z) * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) sk_next[q] = src[q];
+            }
         }
-        tc_fence_after();
-        int x0, y0, z0;
-        brick_tile(P, t, tyn, tzn, x0, y0, z0);
-        const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
-        const bool valid = y < P.ny && z < P.nz;
-        conv_store(P, tmem + (uint32_t(warp * 32) << 16), valid, ((long long)x0 * P.ny + y) * P.nz + z);
-        tc_fence_before();
-        __syncthreads();  // TMEM is free for the next tile's MMAs
+        if (it > 0) {
+            // the previous tile's epilogue, while this tile's MMAs run
+            const int ip = it - 1;
+            const bool done = mbar_wait(&bar[2 + (ip & 1)], unsigned(ip >> 1) & 1u);
+            ok = __syncthreads_and(ok && done);  // the TMEM loads are warp-collective
+            if (!ok) break;
+            tc_fence_after();
+            int x0, y0, z0;
+            brick_tile(P, t - G, tyn, tzn, x0, y0, z0);
+            const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
+            brick_store<COUT>(P, tmem + uint32_t(ip & 1) * NCOLS + (uint32_t(warp * 32) << 16), y < P.ny && z < P.nz,
+                              ((long long)x0 * P.ny + y) * P.nz + z, sk_cur);
+            tc_fence_before();
+        }
+        // the drained accumulator is free for the next tile's MMAs
+        ok = __syncthreads_and(ok);
+        if (!ok || !have) break;
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q) sk_cur[q] = sk_next[q];
     }
-    if (t < ntiles && tid == 0) {
+    if (!ok && tid == 0) {
         if (atomicExch(&P.status->timeout, 1) == 0) {
             P.status->pad[0] = 3;  // kernel: brick convolution
             P.status->pad[2] = int(blockIdx.x);
         }
-        // no brick load of this CTA may still be landing when it exits
+        // no brick load or MMA of this CTA may still be in flight when it exits
         for (int b = 0; b < 2; ++b)
             if (pending[b]) mbar_wait(&bar[b], use[b] & 1u);
-        mbar_wait(&bar[2], unsigned(it) & 1u);
+        if (last_commit >= 0) mbar_wait(&bar[2 + (last_commit & 1)], unsigned(last_commit >> 1) & 1u);
     }
     tc_fence_before();
     __syncthreads();
     __syncwarp();
-    if (warp == 0) tmem_dealloc(tmem, ncols);
+    if (warp == 0) tmem_dealloc(tmem, 2 * NCOLS);
 }
 
 // ------------------------------------------------------- weight gradient
@@ -1037,6 +1125,30 @@ void LearnedNet::format_weights(cudaStream_t s) {
 }
 
 namespace {
+template <int CIN, int COUT>
+void launch_brick_t(const CUtensorMap& tin, const ConvParams& P, int stages, unsigned grid, size_t smem, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        LHI_CUDA(cudaFuncSetAttribute(k_conv_brick<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kBrickSmemMax)));
+        attr = true;
+    }
+    k_conv_brick<CIN, COUT><<<grid, kConvM, smem, s>>>(tin, P, stages);
+    LHI_LAUNCH_CHECK();
+}
+
+// The brick kernel's instances: the (input, output) channel counts of the
+// network's forward and input-gradient convolutions.
+bool launch_brick(const CUtensorMap& tin, const ConvParams& P, int stages, unsigned grid, size_t smem, cudaStream_t s) {
+    if (P.cin == 16 && P.cout == 16) launch_brick_t<16, 16>(tin, P, stages, grid, smem, s);
+    else if (P.cin == 16 && P.cout == 32) launch_brick_t<16, 32>(tin, P, stages, grid, smem, s);
+    else if (P.cin == 32 && P.cout == 16) launch_brick_t<32, 16>(tin, P, stages, grid, smem, s);
+    else if (P.cin == 32 && P.cout == 64) launch_brick_t<32, 64>(tin, P, stages, grid, smem, s);
+    else if (P.cin == 64 && P.cout == 32) launch_brick_t<64, 32>(tin, P, stages, grid, smem, s);
+    else return false;
+    return true;
+}
+
 void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const float* bias, int cout_real,
                  const int* d, int mode, const uint16_t* skip, int relu, uint16_t* out_b, float* out_f, NetStatus* st,
                  cudaStream_t s, const int32_t* tiles = nullptr, const int* ntiles_dev = nullptr) {
@@ -1065,12 +1177,6 @@ void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const
     if (brick_smem_bytes(cin, cout, 1) <= kBrickSmemMax) {
         const int stages = brick_smem_bytes(cin, cout, 2) <= kBrickSmemMax ? 2 : 1;
         const size_t smem = brick_smem_bytes(cin, cout, stages);
-        static bool attr = false;
-        if (!attr) {
-            LHI_CUDA(cudaFuncSetAttribute(k_conv_brick, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int(kBrickSmemMax)));
-            attr = true;
-        }
         // the input as a 4D tensor (channel, z, y, x), boxes of one 8-channel
         // plane of a brick; zeros outside the grid
         CUtensorMap tin;
@@ -1091,9 +1197,9 @@ void launch_conv(const uint16_t* in, int cin, const uint16_t* w, int cout, const
         const unsigned grid = unsigned(std::min<long long>(ntiles, kSMs * per_sm));
         P.tiles = tiles;
         P.ntiles = tiles ? ntiles_dev : nullptr;
-        k_conv_brick<<<grid, kConvM, smem, s>>>(tin, P, stages);
-        LHI_LAUNCH_CHECK();
-        return;
+        if (launch_brick(tin, P, stages, grid, smem, s)) return;
+        P.tiles = nullptr;  // no instance for these channel counts: the gathering kernel
+        P.ntiles = nullptr;
     }
     const size_t smem = size_t(2) * kConvM * cin * 2 + size_t(2) * cout * cin * 2 + 32;
     k_conv<<<unsigned((P.nvox + kConvM - 1) / kConvM), kConvM, smem, s>>>(P);
