@@ -726,12 +726,10 @@ __global__ void k_net_scale(const float* __restrict__ r, const uint8_t* __restri
 // Input channels, all linear in r so that M(a r) = a M(r) for a > 0 and
 // M(0) = 0: [r/s, r/s on cells next to air, r/s on cells next to a solid
 // (or the domain edge), 0], on cells with type != 0.
-__global__ void k_net_input(const float* __restrict__ r, const uint8_t* __restrict__ type,
-                            const uint8_t* __restrict__ solid, int nx, int ny, int nz, const float* __restrict__ scale,
-                            uint16_t* __restrict__ a0) {
-    const long long n = (long long)nx * ny * nz;
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
+__device__ __forceinline__ void net_input_voxel(const float* __restrict__ r, const uint8_t* __restrict__ type,
+                                                const uint8_t* __restrict__ solid, int nx, int ny, int nz,
+                                                const float* __restrict__ scale, uint16_t* __restrict__ a0,
+                                                long long v) {
     const bool fl = type[v] != 0;
     bool air = false, sol = false;
     if (fl) {
@@ -760,6 +758,86 @@ __global__ void k_net_input(const float* __restrict__ r, const uint8_t* __restri
     uint4* dst = reinterpret_cast<uint4*>(a0 + v * 16);
     dst[0] = reinterpret_cast<uint4*>(o)[0];
     dst[1] = reinterpret_cast<uint4*>(o)[1];
+}
+
+__global__ void k_net_input(const float* __restrict__ r, const uint8_t* __restrict__ type,
+                            const uint8_t* __restrict__ solid, int nx, int ny, int nz, const float* __restrict__ scale,
+                            uint16_t* __restrict__ a0) {
+    const long long n = (long long)nx * ny * nz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    net_input_voxel(r, type, solid, nx, ny, nz, scale, a0, v);
+}
+
+// The voxel of this thread in tile u of a brick-tile list (one x plane,
+// 16 y, 8 z; thread = (y - y0) * 8 + (z - z0), as the convolution's rows);
+// false past the grid's edge.
+__device__ __forceinline__ bool list_voxel(const int32_t* __restrict__ list, int u, int ny, int nz, int& x, int& y,
+                                           int& z) {
+    const int tyn = (ny + 15) / 16, tzn = (nz + 7) / 8;
+    const long long tt = list[u];
+    const int tzi = int(tt % tzn);
+    const long long rest = tt / tzn;
+    x = int(rest / tyn);
+    y = int(rest % tyn) * 16 + (threadIdx.x >> 3);
+    z = tzi * 8 + (threadIdx.x & 7);
+    return y < ny && z < nz;
+}
+
+// k_net_input on the voxels of the listed tiles (128 threads per block)
+__global__ void __launch_bounds__(128) k_net_input_tiles(const float* __restrict__ r, const uint8_t* __restrict__ type,
+                                                         const uint8_t* __restrict__ solid, int nx, int ny, int nz,
+                                                         const float* __restrict__ scale, uint16_t* __restrict__ a0,
+                                                         const int32_t* __restrict__ list, const int* __restrict__ count) {
+    const int n = *count;
+    for (int u = blockIdx.x; u < n; u += gridDim.x) {
+        int x, y, z;
+        if (list_voxel(list, u, ny, nz, x, y, z)) net_input_voxel(r, type, solid, nx, ny, nz, scale, a0, ((long long)x * ny + y) * nz + z);
+    }
+}
+
+// k_pool on the coarse voxels of the listed tiles: the same per-channel sums
+// (children in order, FP32) for the voxel's C channels
+__global__ void __launch_bounds__(128) k_pool_tiles(const uint16_t* __restrict__ fine, int fny, int fnz,
+                                                    uint16_t* __restrict__ coarse, int cny, int cnz, int C,
+                                                    const int32_t* __restrict__ list, const int* __restrict__ count) {
+    const int n = *count;
+    for (int u = blockIdx.x; u < n; u += gridDim.x) {
+        int x, y, z;
+        if (!list_voxel(list, u, cny, cnz, x, y, z)) continue;
+        const long long v = ((long long)x * cny + y) * cnz + z;
+        for (int q = 0; q < C / 8; ++q) {
+            float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const long long f = ((long long)(2 * x + (k >> 2)) * fny + (2 * y + ((k >> 1) & 1))) * fnz + (2 * z + (k & 1));
+                uint16_t c8[8];
+                *reinterpret_cast<uint4*>(c8) = reinterpret_cast<const uint4*>(fine + f * C)[q];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[j] += bf16_float(c8[j]);
+            }
+            uint16_t o[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) o[j] = bf16_bits(acc[j] * 0.125f);
+            reinterpret_cast<uint4*>(coarse + v * C)[q] = *reinterpret_cast<uint4*>(o);
+        }
+    }
+}
+
+// k_upsample on the fine voxels of the listed tiles
+__global__ void __launch_bounds__(128) k_upsample_tiles(const uint16_t* __restrict__ coarse, int cnx, int cny, int cnz,
+                                                        uint16_t* __restrict__ fine, int fny, int fnz, int C,
+                                                        const int32_t* __restrict__ list, const int* __restrict__ count) {
+    const int n = *count;
+    for (int u = blockIdx.x; u < n; u += gridDim.x) {
+        int x, y, z;
+        if (!list_voxel(list, u, fny, fnz, x, y, z)) continue;
+        const int px = x >> 1, py = y >> 1, pz = z >> 1;
+        const bool in = px < cnx && py < cny && pz < cnz;
+        const uint4* src = reinterpret_cast<const uint4*>(coarse + (((long long)px * cny + py) * cnz + pz) * C);
+        uint4* dst = reinterpret_cast<uint4*>(fine + (((long long)x * fny + y) * fnz + z) * C);
+        for (int q = 0; q < C / 8; ++q) dst[q] = in ? src[q] : make_uint4(0u, 0u, 0u, 0u);
+    }
 }
 
 // coarse[v][c] = bf16(0.125 * sum of the 8 children), children in (x, y, z) order
@@ -937,6 +1015,45 @@ __global__ void k_mask_dilate(const uint8_t* __restrict__ in, int nx, int ny, in
             }
     }
     out[v] = o;
+}
+
+// k_mask_dilate over 4-voxel words along z (nz a multiple of 4, so a word
+// never spans two z rows): axis 0 along z, axis 1 along x and y
+__global__ void k_mask_dilate4(const uint32_t* __restrict__ in, int nx, int ny, int nzw, int axis,
+                               uint32_t* __restrict__ out) {
+    const long long n = (long long)nx * ny * nzw;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    int x, y, zw;
+    dec3(v, ny, nzw, x, y, zw);
+    uint32_t o;
+    if (axis == 0) {
+        const uint32_t w = in[v];
+        o = w | (w << 8) | (w >> 8);
+        if (zw > 0) o |= in[v - 1] >> 24;       // z - 1 of the first voxel
+        if (zw + 1 < nzw) o |= in[v + 1] << 24;  // z + 1 of the last voxel
+    } else {
+        o = 0u;
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int xx = x + dx, yy = y + dy;
+                if (xx >= 0 && xx < nx && yy >= 0 && yy < ny) o |= in[((long long)xx * ny + yy) * nzw + zw];
+            }
+    }
+    out[v] = o;
+}
+
+// k_mask_tile_flags over 4-voxel words (nz a multiple of 4: a word lies in
+// one tile's 8 z)
+__global__ void k_mask_tile_flags4(const uint32_t* __restrict__ m, int nx, int ny, int nzw, int nz,
+                                   uint8_t* __restrict__ flag) {
+    const long long n = (long long)nx * ny * nzw;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n || !m[v]) return;
+    int x, y, zw;
+    dec3(v, ny, nzw, x, y, zw);
+    const int tyn = (ny + 15) / 16, tzn = (nz + 7) / 8;
+    flag[((long long)x * tyn + (y >> 4)) * tzn + (zw >> 1)] = 1;
 }
 
 // coarse voxel set if any of its 8 children is (the voxels whose upsampled
@@ -1277,18 +1394,30 @@ void LearnedNet::plan_sparse(const int dims[3], const uint8_t* type, cudaStream_
         for (int i = 0; i < 7; ++i) LHI_CUDA(cudaMalloc(&mask_[i], size_t(std::max(1LL, vl[i]))));
         const int* dl[3] = {d0, d1, d2};
         for (int l = 0; l < 3; ++l) LHI_CUDA(cudaMalloc(&tflag_[l], size_t(std::max(1LL, brick_tiles(dl[l])))));
-        const int lvl[kNetLayers] = {0, 1, 2, 1, 0, 0};
-        for (int l = 0; l < kNetLayers; ++l)
+        // list levels: the six convolutions' outputs, then the input
+        // channels (0), pool to 1, pool to 2, upsample to 1, upsample to 0
+        const int lvl[kPlanLists] = {0, 1, 2, 1, 0, 0, 0, 1, 2, 1, 0};
+        for (int l = 0; l < kPlanLists; ++l)
             LHI_CUDA(cudaMalloc(&tlist_[l], sizeof(int32_t) * size_t(std::max(1LL, brick_tiles(dl[lvl[l]])))));
-        LHI_CUDA(cudaMalloc(&tcount_, sizeof(int) * kNetLayers));
+        LHI_CUDA(cudaMalloc(&tcount_, sizeof(int) * kPlanLists));
         plan_cap_vox0_ = V0;
     }
     uint8_t *A = mask_[0], *B = mask_[1], *P = mask_[2], *Q = mask_[3], *U = mask_[4], *W = mask_[5];
     uint8_t* S = mask_[6];  // the dilations' intermediate (sized for level 0, used at every level)
-    LHI_CUDA(cudaMemsetAsync(tcount_, 0, sizeof(int) * kNetLayers, s));
+    LHI_CUDA(cudaMemsetAsync(tcount_, 0, sizeof(int) * kPlanLists, s));
     auto dil = [&](const uint8_t* in, const int* d, uint8_t* out) {
         const long long n = (long long)d[0] * d[1] * d[2];
         if (n == 0) return;
+        if (d[2] % 4 == 0) {  // 4-voxel words (the mask buffers are 256-byte aligned)
+            const long long nw = n / 4;
+            k_mask_dilate4<<<nb(nw), 256, 0, s>>>(reinterpret_cast<const uint32_t*>(in), d[0], d[1], d[2] / 4, 0,
+                                                  reinterpret_cast<uint32_t*>(S));
+            LHI_LAUNCH_CHECK();
+            k_mask_dilate4<<<nb(nw), 256, 0, s>>>(reinterpret_cast<const uint32_t*>(S), d[0], d[1], d[2] / 4, 1,
+                                                  reinterpret_cast<uint32_t*>(out));
+            LHI_LAUNCH_CHECK();
+            return;
+        }
         k_mask_dilate<<<nb(n), 256, 0, s>>>(in, d[0], d[1], d[2], 0, S);
         LHI_LAUNCH_CHECK();
         k_mask_dilate<<<nb(n), 256, 0, s>>>(S, d[0], d[1], d[2], 1, out);
@@ -1310,7 +1439,11 @@ void LearnedNet::plan_sparse(const int dims[3], const uint8_t* type, cudaStream_
         const long long n = (long long)d[0] * d[1] * d[2], nt = brick_tiles(d);
         if (n == 0) return;
         LHI_CUDA(cudaMemsetAsync(tflag_[level], 0, size_t(nt), s));
-        k_mask_tile_flags<<<nb(n), 256, 0, s>>>(m, d[0], d[1], d[2], tflag_[level]);
+        if (d[2] % 4 == 0)
+            k_mask_tile_flags4<<<nb(n / 4), 256, 0, s>>>(reinterpret_cast<const uint32_t*>(m), d[0], d[1], d[2] / 4,
+                                                         d[2], tflag_[level]);
+        else
+            k_mask_tile_flags<<<nb(n), 256, 0, s>>>(m, d[0], d[1], d[2], tflag_[level]);
         LHI_LAUNCH_CHECK();
         k_mask_tile_list<<<nb(nt), 256, 0, s>>>(tflag_[level], nt, tlist_[layer], tcount_ + layer);
         LHI_LAUNCH_CHECK();
@@ -1320,18 +1453,24 @@ void LearnedNet::plan_sparse(const int dims[3], const uint8_t* type, cudaStream_
     tiles(A, d0, 0, 5);
     dil(A, d0, B);  // B = D
     tiles(B, d0, 0, 4);
-    dil(B, d0, A);  // A = dil(D)
+    dil(B, d0, A);  // A = dil(D): q0 needed
+    tiles(A, d0, 0, kPlanUp0);
     up(A, d0, d1, P);  // P = U1
     tiles(P, d1, 1, 3);
-    dil(P, d1, Q);
+    dil(P, d1, Q);  // q1 needed
+    tiles(Q, d1, 1, kPlanUp1);
     up(Q, d1, d2, U);  // U = U2
     tiles(U, d2, 2, 2);
-    dil(U, d2, W);
+    dil(U, d2, W);  // p1 needed
+    tiles(W, d2, 2, kPlanPool1);
     down_or(W, d2, P, d1, Q);  // Q = H1
     tiles(Q, d1, 1, 1);
-    dil(Q, d1, P);
+    dil(Q, d1, P);  // p0 needed
+    tiles(P, d1, 1, kPlanPool0);
     down_or(P, d1, B, d0, A);  // A = H0
     tiles(A, d0, 0, 0);
+    dil(A, d0, B);  // a0 needed
+    tiles(B, d0, 0, kPlanInput);
     plan_type_ = type;
     for (int a = 0; a < 3; ++a) plan_dims_[a] = dims[a];
 }
@@ -1356,7 +1495,15 @@ void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type,
         k_net_scale<<<std::min<unsigned>(nb(V0), 1024), 256, 0, s>>>(r, type, V0, red_, counter_, scale_);
         LHI_LAUNCH_CHECK();
     }
-    k_net_input<<<nb(V0), 256, 0, s>>>(r, type, solid, d0[0], d0[1], d0[2], scale_, b_.a0);
+    // the elementwise stages on their plan's tiles: a persistent grid
+    const auto tgrid = [](const int* d) {
+        return unsigned(std::max(1LL, std::min<long long>(brick_tiles(d), (long long)kSMs * 16)));
+    };
+    if (sparse)
+        k_net_input_tiles<<<tgrid(d0), 128, 0, s>>>(r, type, solid, d0[0], d0[1], d0[2], scale_, b_.a0,
+                                                    tlist_[kPlanInput], tcount_ + kPlanInput);
+    else
+        k_net_input<<<nb(V0), 256, 0, s>>>(r, type, solid, d0[0], d0[1], d0[2], scale_, b_.a0);
     LHI_LAUNCH_CHECK();
     auto W = [&](int l) { return wfwd_ + wfwd_off_[l]; };
     // bias-free: M(0) = 0 (the packed bias entries are kept and ignored)
@@ -1366,16 +1513,32 @@ void LearnedNet::forward(const int dims[3], const float* r, const uint8_t* type,
     };
     const int act = relu_ ? 1 : 0;
     launch_conv(b_.a0, 16, W(0), 16, Bv(0), 16, d0, 0, nullptr, act, b_.h0, nullptr, status_, s, TL(0), TC(0));
-    k_pool<<<nb(b_.vox[1] * 16), 256, 0, s>>>(b_.h0, d0[1], d0[2], b_.p0, d1[0], d1[1], d1[2], 16);
+    if (sparse)
+        k_pool_tiles<<<tgrid(d1), 128, 0, s>>>(b_.h0, d0[1], d0[2], b_.p0, d1[1], d1[2], 16, tlist_[kPlanPool0],
+                                               tcount_ + kPlanPool0);
+    else
+        k_pool<<<nb(b_.vox[1] * 16), 256, 0, s>>>(b_.h0, d0[1], d0[2], b_.p0, d1[0], d1[1], d1[2], 16);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.p0, 16, W(1), 32, Bv(1), 32, d1, 0, nullptr, act, b_.h1, nullptr, status_, s, TL(1), TC(1));
-    k_pool<<<nb(b_.vox[2] * 32), 256, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[0], d2[1], d2[2], 32);
+    if (sparse)
+        k_pool_tiles<<<tgrid(d2), 128, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[1], d2[2], 32, tlist_[kPlanPool1],
+                                               tcount_ + kPlanPool1);
+    else
+        k_pool<<<nb(b_.vox[2] * 32), 256, 0, s>>>(b_.h1, d1[1], d1[2], b_.p1, d2[0], d2[1], d2[2], 32);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.p1, 32, W(2), 64, Bv(2), 64, d2, 0, nullptr, act, b_.h2, nullptr, status_, s, TL(2), TC(2));
-    k_upsample<<<nb(b_.vox[1] * 64 / 8), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
+    if (sparse)
+        k_upsample_tiles<<<tgrid(d1), 128, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[1], d1[2], 64,
+                                                   tlist_[kPlanUp1], tcount_ + kPlanUp1);
+    else
+        k_upsample<<<nb(b_.vox[1] * 64 / 8), 256, 0, s>>>(b_.h2, d2[0], d2[1], d2[2], b_.q1, d1[0], d1[1], d1[2], 64);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.q1, 64, W(3), 32, Bv(3), 32, d1, 0, b_.h1, act, b_.u1, nullptr, status_, s, TL(3), TC(3));
-    k_upsample<<<nb(V0 * 32 / 8), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
+    if (sparse)
+        k_upsample_tiles<<<tgrid(d0), 128, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[1], d0[2], 32,
+                                                   tlist_[kPlanUp0], tcount_ + kPlanUp0);
+    else
+        k_upsample<<<nb(V0 * 32 / 8), 256, 0, s>>>(b_.u1, d1[0], d1[1], d1[2], b_.q0, d0[0], d0[1], d0[2], 32);
     LHI_LAUNCH_CHECK();
     launch_conv(b_.q0, 32, W(4), 16, Bv(4), 16, d0, 0, b_.h0, act, b_.u0, nullptr, status_, s, TL(4), TC(4));
     launch_conv(b_.u0, 16, W(5), 16, Bv(5), 1, d0, 2, nullptr, 0, nullptr, b_.y, status_, s, TL(5), TC(5));

@@ -150,14 +150,18 @@ public:
 
     // sparse evaluation (plan_sparse): voxel masks (level 0: two, level 1:
     // two, level 2: two, and the dilations' intermediate), tile flags per
-    // level, tile list and count per layer
+    // level, tile list and count per layer's output and per elementwise
+    // stage (kPlanInput .. kPlanUp0: the input channels, the two poolings,
+    // the two upsamplings)
+    static constexpr int kPlanInput = kNetLayers, kPlanPool0 = kNetLayers + 1, kPlanPool1 = kNetLayers + 2,
+                         kPlanUp1 = kNetLayers + 3, kPlanUp0 = kNetLayers + 4, kPlanLists = kNetLayers + 5;
     bool sparse_enabled_ = true;
     const uint8_t* plan_type_ = nullptr;
     int plan_dims_[3] = {0, 0, 0};
     uint8_t* mask_[7] = {};
     uint8_t* tflag_[3] = {};
-    int32_t* tlist_[kNetLayers] = {};
-    int* tcount_ = nullptr;  // [kNetLayers] on the device
+    int32_t* tlist_[kPlanLists] = {};
+    int* tcount_ = nullptr;  // [kPlanLists] on the device
     long long plan_cap_vox0_ = 0;
     void free_plan();
 };
