@@ -363,7 +363,9 @@ LHI_API int lhi_liquid_set_field(lhi_liquid* h, int32_t field, int32_t level, co
    still wait. */
 LHI_API int lhi_liquid_set_async(lhi_liquid* h, int32_t on);
 /* Empty string while solves run as CUDA graphs; otherwise why the solve
-   graph could not be built, in which case every solve runs host-driven. */
+   graph could not be built, in which case every solve runs host-driven (or,
+   for the learned preconditioner, why the graph of the iterations after its
+   fallback could not be built, in which case those stay host-driven). */
 LHI_API const char* lhi_solver_graph_error(lhi_liquid* h);
 
 /* ------------------------------------------------------- measurement */
@@ -442,7 +444,10 @@ LHI_API int lhi_net_forward_host(lhi_net* net, const int32_t dims[3], const floa
    fallback_iterations (0 = the solver's max_iterations); from then on it
    applies the multigrid V-cycle of the handle's solver parameters.
    fallback_iterations = -1 turns the fallback off (network only).  The
-   loop is host-driven (one synchronisation per iteration). */
+   network's iterations are host-driven (one synchronisation each); after
+   the fallback the rest of the solve is one replay of a CUDA graph of the
+   V-cycle loop (from the second V-cycle iteration of the handle's first
+   fallback on). */
 LHI_API int lhi_solver_set_network(lhi_liquid* h, lhi_net* net, int32_t fallback_iterations);
 /* Iterations of the last solve that used the network, and the iteration
    at which the fallback started (-1 if it did not). */

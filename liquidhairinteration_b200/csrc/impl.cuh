@@ -298,7 +298,7 @@ public:
         return stats_;
     }
     void set_async(bool on) override { async_ = on; }
-    const std::string& graph_error() const override { return graph_error_; }
+    const std::string& graph_error() const override { return graph_error_.empty() ? tail_error_ : graph_error_; }
     void finish_stats();
     void get_ax(int level, const void* x, void* out) override;
     double spmv_p(int* tma) override;
@@ -354,7 +354,7 @@ public:
     void enqueue_init(unsigned long long cond, int use_cond);
     void enqueue_body(unsigned long long cond, int use_cond);
     void enqueue_final();
-    void build_solve_graph();
+    void build_solve_graph(bool with_init);
     void spmv(int level, const T* x, T* y);
     void get_acoef(int level, T* host_out);
     void device_sum_launch_prep();
@@ -441,6 +441,10 @@ public:
     cudaStream_t cur_ = nullptr;   // stream the enqueue helpers launch on
     cudaStream_t side_ = nullptr;  // capture stream of the graph's loop body
     cudaGraphExec_t solve_exec_ = nullptr;
+    cudaGraphExec_t tail_exec_ = nullptr;  // the loop and final pass without init (FPCG after its fallback)
+    std::string tail_error_;               // why the tail graph could not be built (the loop stays host-driven)
+    bool fallback_body_ran_ = false;       // a V-cycle body of an FPCG fallback has run host-driven
+    int tail_from_iter_ = -1;              // iteration at which the last solve's tail graph took over
     long long graph_init_kernels_ = 0, graph_body_kernels_ = 0, graph_final_kernels_ = 0;
     bool async_ = false;         // steps do not wait for the solve; statistics are read on demand
     bool stats_pending_ = false; // the last graph solve's statistics are still on the device

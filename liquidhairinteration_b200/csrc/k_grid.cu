@@ -579,6 +579,7 @@ template <class T, class TX> LiquidImpl<T, TX>::~LiquidImpl() {
     F(coarse_list_);
     F(coarse_counts_);
     if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+    if (tail_exec_) cudaGraphExecDestroy(tail_exec_);
     F(solid_cell_);
     F(net_type_);
     F(snaps_);

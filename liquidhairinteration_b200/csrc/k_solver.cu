@@ -2292,7 +2292,12 @@ template <class T, class TX> void LiquidImpl<T, TX>::enqueue_final() {
 // The solve after BuildLHS as one graph: init; while (!stop) { iteration };
 // final.  Pointers and parameters are fixed for the handle's lifetime, so
 // the graph is built on the first solve and replayed after.
-template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
+// with_init: the whole solve (init, the loop, the final pass).  Without it:
+// the loop from the current iterate on and the final pass (the tail of a
+// solve whose first iterations ran host-driven); its loop condition starts
+// at 1 at every launch, and a solve that has already stopped leaves the
+// loop in its first body's first kernel.
+template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph(bool with_init) {
     cudaGraph_t g = nullptr;
     LHI_CUDA(cudaStreamSynchronize(stream_));  // surfaces any earlier asynchronous error before capturing
     LHI_CUDA(cudaGetLastError());
@@ -2304,9 +2309,12 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         cudaGraph_t cg = nullptr;
         LHI_CUDA(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cg, nullptr, nullptr));
         cudaGraphConditionalHandle h;
-        LHI_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+        if (with_init)
+            LHI_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+        else
+            LHI_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault));
         const long long c0 = g_kernel_launches.load();
-        enqueue_init(h, 1);
+        if (with_init) enqueue_init(h, 1);
         const long long c1 = g_kernel_launches.load();
         LHI_CUDA(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cg, &deps, &nd));
         cudaGraphNodeParams cp = {};
@@ -2336,7 +2344,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
         enqueue_final();
         const long long c3 = g_kernel_launches.load();
         LHI_CUDA(cudaStreamEndCapture(stream_, &g));
-        graph_init_kernels_ = c1 - c0;
+        if (with_init) graph_init_kernels_ = c1 - c0;
         graph_body_kernels_ = c2 - c1;
         graph_final_kernels_ = c3 - c2;
         // captured launches did not run: the replays below count what runs
@@ -2361,7 +2369,7 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_solve_graph() {
     }
     cudaGraphDestroy(g);
     if (e != cudaSuccess) throw CudaError(e, why);
-    solve_exec_ = exec;
+    (with_init ? solve_exec_ : tail_exec_) = exec;
 }
 
 // CGSolver<3>::Solve (PressureSolver.cpp:839-934)
@@ -2384,7 +2392,7 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     solved_once_ = true;
     if (!sp_.eager && !prof_.on && !learned && snap_cap_ == 0 && graph_ok && graph_error_.empty() && !solve_exec_) {
         try {
-            build_solve_graph();
+            build_solve_graph(true);
         } catch (const CudaError& err) {
             graph_error_ = err.what();  // keep solving, host-driven (lhi_solver_graph_error)
             cudaGetLastError();         // the failed capture's error is not this solve's
@@ -2411,6 +2419,11 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
             }
         }
         double prev = -1.0;
+        // after the fallback (and once one V-cycle body has run here, so no
+        // kernel loads for the first time inside a capture) the rest of the
+        // solve is one replay of the tail graph
+        const bool tail_ok = learned && !sp_.eager && !prof_.on && snap_cap_ == 0;
+        bool tail = false;
         for (;;) {
             read_scalars();
             if (sc_host_->stop) break;
@@ -2424,9 +2437,26 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
                 prev = res;
             }
             if (learned && !use_fallback_) ++learned_iters_;
+            if (tail_ok && use_fallback_ && fallback_body_ran_ && tail_error_.empty()) {
+                if (!tail_exec_) {
+                    try {
+                        build_solve_graph(false);
+                    } catch (const CudaError& err) {
+                        tail_error_ = err.what();  // keep the loop host-driven
+                        cudaGetLastError();
+                    }
+                }
+                if (tail_exec_) {
+                    tail_from_iter_ = sc_host_->iter;
+                    LHI_CUDA(cudaGraphLaunch(tail_exec_, stream_));
+                    tail = true;
+                    break;
+                }
+            }
             enqueue_body(0, 0);
+            if (use_fallback_) fallback_body_ran_ = true;
         }
-        enqueue_final();
+        if (!tail) enqueue_final();
     }
     LHI_CUDA(cudaEventRecord(ev1_, stream_));
     last_solve_graph_ = graph_replayed;
@@ -2444,6 +2474,10 @@ template <class T, class TX> void LiquidImpl<T, TX>::finish_stats() {
     if (last_solve_graph_)  // kernels the replay ran: init, one body per loop trip, final
         g_kernel_launches.fetch_add(graph_init_kernels_ + graph_final_kernels_ +
                                     graph_body_kernels_ * (long long)std::max(sc_host_->iter, 0));
+    if (tail_from_iter_ >= 0)  // the tail graph: one body per loop trip from where it started (at least one), final
+        g_kernel_launches.fetch_add(graph_final_kernels_ +
+                                    graph_body_kernels_ * (long long)std::max(sc_host_->iter - tail_from_iter_, 1));
+    tail_from_iter_ = -1;
     stats_.iterations = sc_host_->iter;
     stats_.initial_residual = sc_host_->residual0;
     stats_.final_residual = sc_host_->residual;

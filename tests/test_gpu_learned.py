@@ -111,3 +111,36 @@ def test_untrained_network_falls_back_to_vcycle(oracle_mod, lhi):
     assert st["status"] == abi.LHI_OK, st
     assert 0 <= fallback_at <= 3, fallback_at
     net.close()
+
+
+def test_fpcg_tail_graph_matches_host_loop(oracle_mod, lhi):
+    """After the fallback the rest of an FPCG solve replays a graph of the
+    V-cycle loop; the same solves run host-driven all the way (eager) give
+    the same iterations, fallback points and pressure, bit for bit.  Both
+    start from the same fields (P2G's cross-tile sums land in a run-dependent
+    order, so whole steps are compared elsewhere within tolerances); the first
+    solve builds the tail graph, the second replays it again."""
+    import os
+    from liquidhairinteration_b200.net import LearnedNet
+    spec = scenes.dam(64)
+    net = LearnedNet(seed=0)
+    net.load(os.path.join(os.path.dirname(abi.__file__), "weights", "fpcg.lhinet"))
+    runs = {}
+    for eager in (0, 1):
+        g = _scene_after_p2g(oracle_mod, spec, spec.solver_params(preconditioner=abi.PRECOND_LEARNED,
+                                                                  coarse_cells=64, eager=eager))
+        s = g.GetSolver()
+        s.SetNetwork(net, fallbackIterations=0)
+        out = []
+        for _ in range(2):
+            st = s.Solve(spec.density, spec.dt)
+            assert st["status"] == abi.LHI_OK, st
+            out.append((st["iterations"], s.LearnedStats(), g.field("pressure").copy()))
+        assert lhi.lib().lhi_solver_graph_error(g._h) in (b"", None), lhi.lib().lhi_solver_graph_error(g._h)
+        runs[eager] = out
+        g.close()
+    for (it0, ls0, p0), (it1, ls1, p1) in zip(runs[0], runs[1]):
+        assert it0 == it1 and ls0 == ls1, (it0, it1, ls0, ls1)
+        assert ls0[1] >= 0  # the fallback happened, so the tail graph ran
+        assert np.array_equal(p0.view(np.uint32), p1.view(np.uint32))
+    net.close()
