@@ -285,18 +285,20 @@ __global__ void __launch_bounds__(kConvM) k_conv(ConvParams P) {
 // channels-last activations (a 4D tensor map, channels innermost), which
 // reads zeros outside the grid: the convolution's zero padding.
 //
-// CTAs are persistent and keep all 27 weight tiles resident.  The tiles of a
-// CTA run as a pipeline over two TMEM accumulators: in step i thread 0 issues
-// tile i's MMAs (the descriptors are compile-time offsets from two bases)
-// while all four warps drain tile i - 1's accumulator (with its skip input
-// loaded one step ahead); where shared memory holds two bricks, tile i + 1's
-// brick is loaded during step i as well.
+// CTAs are persistent, keep all 27 weight tiles resident and run their tiles
+// as a warp-specialised pipeline over two TMEM accumulators: warp 4 (one
+// lane) loads the bricks and issues each tile's MMAs (compile-time
+// descriptor offsets from two bases); warps 0-3 drain the accumulators, each
+// its 32 TMEM lanes.  They hand over through mbarriers only: a brick has
+// landed, a tile's MMAs are done, an accumulator is drained.  Where shared
+// memory holds two bricks, tile i + 1's brick loads while tile i's MMAs run.
 constexpr int kBrX = 3, kBrY = 18, kBrZ = 10;
 constexpr int kBrVox = kBrX * kBrY * kBrZ;  // 540
 constexpr int kBrBox = kBrVox * 16;         // bytes of one 8-channel plane (one TMA box)
 constexpr int kBrPlane = 68 * 128;          // plane stride: the box rounded up to 128 bytes
 constexpr size_t kBrickSmemMax = 227 * 1024;
-constexpr int kBrBars = 48;                 // four mbarriers and the TMEM address slot
+constexpr int kBrBars = 64;                 // six mbarriers, the TMEM address slot and the abort flag
+constexpr int kBrThreads = 160;             // warps 0-3 drain, warp 4 produces
 
 // Shared-memory bytes of the brick kernel for one layer with `stages` bricks.
 __host__ __device__ constexpr size_t brick_smem_bytes(int cin, int cout, int stages) {
@@ -381,26 +383,56 @@ __device__ __forceinline__ void brick_store(const ConvParams& P, uint32_t trow, 
     }
 }
 
-// Barriers: [0], [1] brick stages (TMA), [2], [3] accumulators (MMA commit).
+// Bounded wait on a pipeline barrier that also gives up once another warp of
+// the CTA has set the abort flag (a wait of its own that timed out).
+__device__ __forceinline__ bool brick_wait(uint64_t* bar, unsigned parity, volatile int* abort_flag) {
+    const uint32_t addr = smem_u32(bar);
+    const uint64_t deadline = global_ns() + 200000000ull;
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (*abort_flag || global_ns() > deadline) return false;
+    }
+}
+
+// Barriers: full[2] (a brick stage has landed), done[2] (an accumulator's
+// MMAs completed), empty[2] (an accumulator has been drained: one arrival
+// per draining warp).  Tile i of this CTA uses accumulator i & 1 and, with
+// two bricks, brick i & 1.
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kConvM) k_conv_brick(const __grid_constant__ CUtensorMap tin, ConvParams P,
-                                                       int stages) {
+__global__ void __launch_bounds__(kBrThreads) k_conv_brick(const __grid_constant__ CUtensorMap tin, ConvParams P,
+                                                           int stages) {
     extern __shared__ __align__(1024) uint8_t sm[];
     constexpr int KC = CIN / 8;
     constexpr int WBYTES = COUT * CIN * 2;  // one tap's B tile
     constexpr uint32_t NCOLS = COUT < 32 ? 32u : uint32_t(COUT);
     uint8_t* Bs = sm;
-    uint8_t* Ab = sm + 27 * WBYTES;  // stage s at Ab + s * KC * kBrPlane
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Ab + stages * KC * kBrPlane);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 4);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    uint8_t* Ab = sm + 27 * WBYTES;  // brick s at Ab + s * KC * kBrPlane
+    uint64_t* full = reinterpret_cast<uint64_t*>(Ab + stages * KC * kBrPlane);
+    uint64_t* done = full + 2;
+    uint64_t* empty = full + 4;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 6);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
-        for (int b = 0; b < 4; ++b) mbar_init(&bar[b], 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&full[b], 1);
+            mbar_init(&done[b], 1);
+            mbar_init(&empty[b], 4);
+        }
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
     if (warp == 0) tmem_alloc(tslot, 2 * NCOLS);
-    for (int i = tid; i < 27 * WBYTES / 16; i += kConvM)
+    for (int i = tid; i < 27 * WBYTES / 16; i += kBrThreads)
         reinterpret_cast<uint4*>(Bs)[i] = reinterpret_cast<const uint4*>(P.w)[i];
     fence_async_smem();  // the weight tiles (generic stores) before the tensor cores read them
     tc_fence_before();
@@ -410,101 +442,90 @@ __global__ void __launch_bounds__(kConvM) k_conv_brick(const __grid_constant__ C
     const int tyn = (P.ny + 15) / 16, tzn = (P.nz + 7) / 8;
     const long long ntiles = P.tiles ? (long long)*P.ntiles : (long long)P.nx * tyn * tzn;
     const long long G = gridDim.x;
-    // thread 0's bookkeeping: brick loads in flight and completed per stage,
-    // and the step of its last MMA commit
-    bool pending[2] = {false, false};
-    unsigned use[2] = {0u, 0u};
-    int last_commit = -1;
-    if (tid == 0 && (long long)blockIdx.x < ntiles) {
-        brick_issue(&tin, P, blockIdx.x, tyn, tzn, KC, Ab, &bar[0]);
-        pending[0] = true;
-    }
-    uint4 sk_next[COUT / 8], sk_cur[COUT / 8];  // skip rows of this step's tile, of the previous one
-#pragma unroll
-    for (int q = 0; q < COUT / 8; ++q) sk_next[q] = sk_cur[q] = make_uint4(0u, 0u, 0u, 0u);
-    bool ok = true;
-    int it = 0;
-    long long t = blockIdx.x;
-    for (;; ++it, t += G) {
-        const bool have = t < ntiles;
-        if (!have && it == 0) break;
-        const int s = stages == 2 ? (it & 1) : 0;
-        if (tid == 0 && have) {
-            const long long tn = t + G;
-            if (stages == 1 && it > 0) {
-                // the one brick was read by the previous tile's MMAs: reload it when they are done
-                if (mbar_wait(&bar[2 + ((it - 1) & 1)], unsigned((it - 1) >> 1) & 1u)) {
-                    brick_issue(&tin, P, t, tyn, tzn, KC, Ab, &bar[0]);
+    const int nmine = (long long)blockIdx.x < ntiles ? int((ntiles - 1 - blockIdx.x) / G) + 1 : 0;
+    if (warp == 4) {
+        // ---- producer (one lane)
+        if (lane == 0 && nmine > 0) {
+            bool pending[2] = {false, false};  // a brick load in flight, not yet waited for
+            unsigned use[2] = {0u, 0u};        // completed waits per brick barrier: its next phase's parity
+            int last_commit = -1;
+            bool ok = true;
+            auto brick_buf = [&](int s) { return Ab + s * KC * kBrPlane; };
+            brick_issue(&tin, P, blockIdx.x, tyn, tzn, KC, brick_buf(0), &full[0]);
+            pending[0] = true;
+            for (int i = 0; i < nmine; ++i) {
+                const long long t = blockIdx.x + (long long)i * G;
+                const int s = stages == 2 ? (i & 1) : 0, b = i & 1;
+                if (stages == 1 && i > 0) {
+                    // the one brick was read by tile i - 1's MMAs
+                    if (!(ok = brick_wait(&done[(i - 1) & 1], unsigned((i - 1) >> 1) & 1u, abort_flag))) break;
+                    brick_issue(&tin, P, t, tyn, tzn, KC, brick_buf(0), &full[0]);
                     pending[0] = true;
-                } else {
-                    ok = false;
                 }
-            }
-            if (ok && stages == 2 && tn < ntiles) {
-                // the other brick was read by the previous tile's MMAs
-                if (it == 0 || mbar_wait(&bar[2 + ((it - 1) & 1)], unsigned((it - 1) >> 1) & 1u)) {
-                    brick_issue(&tin, P, tn, tyn, tzn, KC, Ab + (s ^ 1) * KC * kBrPlane, &bar[s ^ 1]);
-                    pending[s ^ 1] = true;
-                } else {
-                    ok = false;
-                }
-            }
-            if (ok && mbar_wait(&bar[s], use[s] & 1u)) {
+                if (!(ok = brick_wait(&full[s], use[s] & 1u, abort_flag))) break;
                 pending[s] = false;
                 ++use[s];
+                // accumulator b was last drained after tile i - 2
+                if (i >= 2 && !(ok = brick_wait(&empty[b], unsigned((i >> 1) + 1) & 1u, abort_flag))) break;
                 tc_fence_after();
-                brick_mmas<CIN, COUT>(tmem + uint32_t(it & 1) * NCOLS, smem_u32(Ab + s * KC * kBrPlane),
-                                      smem_u32(Bs));
-                umma_commit(&bar[2 + (it & 1)]);
-                last_commit = it;
-            } else {
-                ok = false;
+                brick_mmas<CIN, COUT>(tmem + uint32_t(b) * NCOLS, smem_u32(brick_buf(s)), smem_u32(Bs));
+                umma_commit(&done[b]);
+                last_commit = i;
+                if (stages == 2 && i + 1 < nmine) {
+                    // the other brick was read by tile i - 1's MMAs
+                    if (i >= 1 && !(ok = brick_wait(&done[(i - 1) & 1], unsigned((i - 1) >> 1) & 1u, abort_flag)))
+                        break;
+                    brick_issue(&tin, P, t + G, tyn, tzn, KC, brick_buf(s ^ 1), &full[s ^ 1]);
+                    pending[s ^ 1] = true;
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                if (atomicExch(&P.status->timeout, 1) == 0) {
+                    P.status->pad[0] = 3;  // kernel: brick convolution
+                    P.status->pad[2] = int(blockIdx.x);
+                }
+                // no brick load or MMA of this CTA may still be in flight when it exits
+                for (int s2 = 0; s2 < 2; ++s2)
+                    if (pending[s2]) mbar_wait(&full[s2], use[s2] & 1u);
+                if (last_commit >= 0) mbar_wait(&done[last_commit & 1], unsigned(last_commit >> 1) & 1u);
             }
         }
-        // this tile's skip rows, for its epilogue in the next step
-        if (have && P.mode == 0 && P.skip) {
+        __syncwarp();
+    } else {
+        // ---- drain: warp w reads TMEM lanes 32w .. 32w + 31
+        for (int i = 0; i < nmine; ++i) {
+            const long long t = blockIdx.x + (long long)i * G;
+            const int b = i & 1;
             int x0, y0, z0;
             brick_tile(P, t, tyn, tzn, x0, y0, z0);
             const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
-            if (y < P.ny && z < P.nz) {
-                const uint4* src = reinterpret_cast<const uint4*>(P.skip + (((long long)x0 * P.ny + y) * P.nz + z) * COUT);
+            const bool valid = y < P.ny && z < P.nz;
+            const long long v = ((long long)x0 * P.ny + y) * P.nz + z;
+            uint4 sk[COUT / 8];
 #pragma unroll
-                for (int q = 0; q < COUT / 8; ++q) sk_next[q] = src[q];
+            for (int q = 0; q < COUT / 8; ++q) sk[q] = make_uint4(0u, 0u, 0u, 0u);
+            if (valid && P.mode == 0 && P.skip) {  // loaded while the MMAs run
+                const uint4* src = reinterpret_cast<const uint4*>(P.skip + v * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) sk[q] = src[q];
             }
-        }
-        if (it > 0) {
-            // the previous tile's epilogue, while this tile's MMAs run
-            const int ip = it - 1;
-            const bool done = mbar_wait(&bar[2 + (ip & 1)], unsigned(ip >> 1) & 1u);
-            ok = __syncthreads_and(ok && done);  // the TMEM loads are warp-collective
-            if (!ok) break;
+            // one decision per warp: the TMEM loads are warp-collective
+            if (!__all_sync(0xffffffffu, brick_wait(&done[b], unsigned(i >> 1) & 1u, abort_flag))) {
+                if (lane == 0) *abort_flag = 1;
+                break;
+            }
             tc_fence_after();
-            int x0, y0, z0;
-            brick_tile(P, t - G, tyn, tzn, x0, y0, z0);
-            const int y = y0 + (tid >> 3), z = z0 + (tid & 7);
-            brick_store<COUT>(P, tmem + uint32_t(ip & 1) * NCOLS + (uint32_t(warp * 32) << 16), y < P.ny && z < P.nz,
-                              ((long long)x0 * P.ny + y) * P.nz + z, sk_cur);
+            brick_store<COUT>(P, tmem + uint32_t(b) * NCOLS + (uint32_t(warp * 32) << 16), valid, v, sk);
             tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
         }
-        // the drained accumulator is free for the next tile's MMAs
-        ok = __syncthreads_and(ok);
-        if (!ok || !have) break;
-#pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) sk_cur[q] = sk_next[q];
-    }
-    if (!ok && tid == 0) {
-        if (atomicExch(&P.status->timeout, 1) == 0) {
-            P.status->pad[0] = 3;  // kernel: brick convolution
-            P.status->pad[2] = int(blockIdx.x);
-        }
-        // no brick load or MMA of this CTA may still be in flight when it exits
-        for (int b = 0; b < 2; ++b)
-            if (pending[b]) mbar_wait(&bar[b], use[b] & 1u);
-        if (last_commit >= 0) mbar_wait(&bar[2 + (last_commit & 1)], unsigned(last_commit >> 1) & 1u);
     }
     tc_fence_before();
     __syncthreads();
-    __syncwarp();
+    tc_fence_after();
     if (warp == 0) tmem_dealloc(tmem, 2 * NCOLS);
 }
 
@@ -1250,7 +1271,7 @@ void launch_brick_t(const CUtensorMap& tin, const ConvParams& P, int stages, uns
                                       int(kBrickSmemMax)));
         attr = true;
     }
-    k_conv_brick<CIN, COUT><<<grid, kConvM, smem, s>>>(tin, P, stages);
+    k_conv_brick<CIN, COUT><<<grid, kBrThreads, smem, s>>>(tin, P, stages);
     LHI_LAUNCH_CHECK();
 }
 

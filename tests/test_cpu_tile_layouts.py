@@ -65,7 +65,7 @@ def test_brick_convolution_operands_inside_tiles(cin, cout):
     limit = _const("k_learned.cu", "kBrickSmemMax")
     bars = _const("k_learned.cu", "kBrBars")
     assert box <= plane and plane % 128 == 0
-    assert bars >= 4 * 8 + 4  # four mbarriers and the TMEM address slot
+    assert bars >= 6 * 8 + 4 + 4  # six mbarriers, the TMEM address slot and the abort flag
     kc = cin // 8
     wbytes = cout * cin * 2
     a_base = 27 * wbytes
