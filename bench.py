@@ -282,7 +282,11 @@ def run_ours(args):
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if os.path.exists(tpath):
         tj = json.load(open(tpath))
-        traffic = tj.get(args.scene, {}).get(dominant)
+        tv = tj.get(args.scene, {}).get(dominant)
+        if isinstance(tv, dict):  # measured at another active-tile count of the scene: scaled by active tiles
+            traffic = int(round(tv["bytes_per_launch"] * active / max(tv["active_tiles"], 1)))
+        else:
+            traffic = tv
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": int(algo), "avg_launch_ms": round(avg_ms, 5),
