@@ -11,10 +11,16 @@
 //     channels-last activations already are, so each voxel's channels are
 //     one 16-byte shared-memory store.
 // One thread issues tcgen05.mma into a TMEM accumulator; tcgen05.commit
-// arrives on an mbarrier per shared-memory stage (two stages, so loading tap
-// t + 1 overlaps the MMAs of tap t); the epilogue reads TMEM with tcgen05.ld.
+// arrives on an mbarrier; the epilogue reads TMEM with tcgen05.ld.  The
+// gathering kernel (k_conv) stages two taps at a time; the brick kernel
+// (k_conv_brick, every layer of this network) stages each output tile's
+// input brick once by TMA and runs its tiles as a warp-specialised pipeline
+// over two accumulators.  The solver's forward passes run tile-sparse: a
+// plan (plan_sparse) lists, per stage, the tiles the cells with type != 0
+// depend on.
 // Every mbarrier wait is bounded: on timeout the kernel records it in
-// NetStatus, waits (bounded) for its last commit, frees TMEM and returns.
+// NetStatus, waits (bounded) for its own copies and MMAs in flight, frees
+// TMEM and returns.
 #include <algorithm>
 #include <cmath>
 #include <random>
