@@ -378,10 +378,12 @@ LHI_API int lhi_liquid_stream(lhi_liquid* h, void** stream);
    at once, included). */
 LHI_API int lhi_kernel_launch_count(int64_t* count);
 /* Limit, in milliseconds, of every bounded wait of the solver kernels on
-   their TMA staging copies, on the current device (default 200; 0 gives up
-   at once).  A kernel that gives up records LHI_E_TIMEOUT in the solve's
-   status, waits (200 ms at most) for its own copies in flight and returns,
-   so the context stays usable.  For tests of that path. */
+   their TMA staging copies and of the network's brick convolution on its
+   pipeline barriers, on the current device (default 200; 0 gives up at
+   once).  A kernel that gives up records LHI_E_TIMEOUT (in the solve's
+   status, or the network's, which the next network call or learned solve
+   reports), waits (200 ms at most) for its own copies and MMAs in flight
+   and returns, so the context stays usable.  For tests of that path. */
 LHI_API int lhi_debug_set_stage_wait_limit(double ms);
 /* Kernel categories timed by the optional profiler. */
 #define LHI_KERNEL_SORT 0         /* cell keys, radix sort, permutation, cell ranges */

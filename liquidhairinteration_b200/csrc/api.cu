@@ -545,6 +545,7 @@ LHI_API int lhi_debug_set_stage_wait_limit(double ms) {
     if (!(ms >= 0.0) || ms > 1e6) return fail(LHI_E_INVALID_ARG, "wait limit must be in [0, 1e6] ms");
     return guarded([&]() -> int {
         lhi::set_stage_wait_limit_ns((unsigned long long)(ms * 1e6));
+        lhi::set_net_wait_limit_ns((unsigned long long)(ms * 1e6));
         return LHI_OK;
     });
 }

@@ -389,11 +389,19 @@ __device__ __forceinline__ void brick_store(const ConvParams& P, uint32_t trow, 
     }
 }
 
+// Limit of the brick convolution's pipeline waits (200 ms;
+// lhi_debug_set_stage_wait_limit lowers it to test the timeout path, 0
+// gives up at once).  The waits for a CTA's own copies and MMAs in flight
+// before it leaves keep the fixed 200 ms.
+__device__ unsigned long long g_net_wait_ns = 200000000ull;
+
 // Bounded wait on a pipeline barrier that also gives up once another warp of
 // the CTA has set the abort flag (a wait of its own that timed out).
 __device__ __forceinline__ bool brick_wait(uint64_t* bar, unsigned parity, volatile int* abort_flag) {
+    const unsigned long long limit = g_net_wait_ns;
+    if (limit == 0) return false;
     const uint32_t addr = smem_u32(bar);
-    const uint64_t deadline = global_ns() + 200000000ull;
+    const uint64_t deadline = global_ns() + limit;
     for (;;) {
         uint32_t ok;
         asm volatile(
@@ -1214,8 +1222,15 @@ int LearnedNet::check_status(cudaStream_t s) {
         last_timeout_[0] = h.pad[0];
         last_timeout_[1] = h.pad[1];
         last_timeout_[2] = h.pad[2];
+        // reported once: the next call starts from a clear status
+        LHI_CUDA(cudaMemsetAsync(status_, 0, sizeof(NetStatus), s));
+        LHI_CUDA(cudaStreamSynchronize(s));
     }
     return h.timeout ? LHI_E_TIMEOUT : LHI_OK;
+}
+
+void set_net_wait_limit_ns(unsigned long long ns) {
+    LHI_CUDA(cudaMemcpyToSymbol(g_net_wait_ns, &ns, sizeof(ns)));
 }
 
 void LearnedNet::ensure(const int dims[3]) {

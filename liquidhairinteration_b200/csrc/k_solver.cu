@@ -2463,6 +2463,8 @@ template <class T, class TX> int LiquidImpl<T, TX>::solve(double rho, double dt)
     stats_pending_ = true;
     if (async_ && graph_replayed) return LHI_OK;  // read by stats() later
     finish_stats();
+    // a network application whose pipeline wait ran out left no usable direction
+    if (learned && net_ && net_->check_status(stream_) != LHI_OK) stats_.status = LHI_E_TIMEOUT;
     return stats_.status;
 }
 

@@ -123,7 +123,7 @@ public:
     void zero_grad(cudaStream_t s);
     void adam_step(double lr, double beta1, double beta2, double eps, cudaStream_t s);
     void get_grads(float* host, cudaStream_t s);
-    int check_status(cudaStream_t s);  // 0 or LHI_E_TIMEOUT
+    int check_status(cudaStream_t s);  // 0 or LHI_E_TIMEOUT (once: the status is cleared after a timeout)
 
     // parameters
     float* w32_ = nullptr;      // master FP32 parameters (packed order)
@@ -165,6 +165,9 @@ public:
     long long plan_cap_vox0_ = 0;
     void free_plan();
 };
+
+// Limit of the brick convolution's pipeline waits on the current device.
+void set_net_wait_limit_ns(unsigned long long ns);
 
 // One-CTA tcgen05 GEMM check: D = A B^T, A 128 x K, B N x K (BF16 bits,
 // row-major), D 128 x N; *stage reports how far the kernel got.
