@@ -197,14 +197,13 @@ __global__ void k_level_phi(LevelGeom g, const T* __restrict__ fine_phi, T* __re
 // from fields of type TI (TI = float, T = double: the FP64 finest-level
 // matrix the mixed mode's outer residual uses).
 template <class T, class TI = T>
-__global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI* __restrict__ lwx,
-                               const TI* __restrict__ lwy, const TI* __restrict__ lwz, T h0, T h1, T h2, T dt, T rho,
-                               T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy, T* __restrict__ cz,
-                               uint8_t* __restrict__ type, uint8_t* __restrict__ tile_flag, int tdy, int tdz,
-                               uint8_t* __restrict__ mask, int mpitch) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long n = (long long)g.nx * g.ny * g.nz;
-    if (i >= n) return;
+__device__ __forceinline__ void level_matrix_cell(long long i, LevelGeom g, const TI* __restrict__ phi,
+                                                  const TI* __restrict__ lwx, const TI* __restrict__ lwy,
+                                                  const TI* __restrict__ lwz, T h0, T h1, T h2, T dt, T rho,
+                                                  T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy,
+                                                  T* __restrict__ cz, uint8_t* __restrict__ type,
+                                                  uint8_t* __restrict__ tile_flag, int tdy, int tdz,
+                                                  uint8_t* __restrict__ mask, int mpitch) {
     // the FP64 copy is read only on rows with phi <= 0 (and their fluid
     // neighbours): air cells need no entries
     if constexpr (!std::is_same<T, TI>::value)
@@ -272,6 +271,39 @@ __global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI
     diag[i] = d;
 }
 
+template <class T, class TI = T>
+__global__ void k_level_matrix(LevelGeom g, const TI* __restrict__ phi, const TI* __restrict__ lwx,
+                               const TI* __restrict__ lwy, const TI* __restrict__ lwz, T h0, T h1, T h2, T dt, T rho,
+                               T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy, T* __restrict__ cz,
+                               uint8_t* __restrict__ type, uint8_t* __restrict__ tile_flag, int tdy, int tdz,
+                               uint8_t* __restrict__ mask, int mpitch) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)g.nx * g.ny * g.nz) return;
+    level_matrix_cell<T, TI>(i, g, phi, lwx, lwy, lwz, h0, h1, h2, dt, rho, diag, cx, cy, cz, type, tile_flag, tdy,
+                             tdz, mask, mpitch);
+}
+
+// The mixed mode's finest level: the FP32 matrix (with the cell classes,
+// tile flags and neighbour mask) and the FP64 matrix of the outer residual
+// from one read of the fields, each in its own arithmetic (the same bits as
+// two k_level_matrix launches).
+template <class T>
+__global__ void k_level_matrix_mixed(LevelGeom g, const T* __restrict__ phi, const T* __restrict__ lwx,
+                                     const T* __restrict__ lwy, const T* __restrict__ lwz, T h0, T h1, T h2, T dt,
+                                     T rho, T* __restrict__ diag, T* __restrict__ cx, T* __restrict__ cy,
+                                     T* __restrict__ cz, uint8_t* __restrict__ type, uint8_t* __restrict__ tile_flag,
+                                     int tdy, int tdz, uint8_t* __restrict__ mask, int mpitch, double hd0, double hd1,
+                                     double hd2, double dtd, double rhod, double* __restrict__ diag_hi,
+                                     double* __restrict__ cx_hi, double* __restrict__ cy_hi,
+                                     double* __restrict__ cz_hi) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)g.nx * g.ny * g.nz) return;
+    level_matrix_cell<T, T>(i, g, phi, lwx, lwy, lwz, h0, h1, h2, dt, rho, diag, cx, cy, cz, type, tile_flag, tdy,
+                            tdz, mask, mpitch);
+    level_matrix_cell<double, T>(i, g, phi, lwx, lwy, lwz, hd0, hd1, hd2, dtd, rhod, diag_hi, cx_hi, cy_hi, cz_hi,
+                                 nullptr, nullptr, 0, 0, nullptr, 0);
+}
+
 // Galerkin coarse level (LHI_COARSE_GALERKIN): A_c = P^T A P / 8 of the
 // finer level f under the V-cycle's transfers (constant injection P, the
 // 1/8 averaging restriction), with A_ij = [type_i >= 1][type_j == 2] c_ij as
@@ -337,13 +369,12 @@ __global__ void k_level_galerkin(LevelK<T> F, int cnx, int cny, int cnz, T* __re
 // (TI = float, T = double: the FP64 right-hand side of the mixed mode's
 // outer residual, from the same float fields)
 template <class T, class TI = T>
-__global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const TI* __restrict__ phi,
-                            const TI* __restrict__ lwx, const TI* __restrict__ lwy, const TI* __restrict__ lwz,
-                            const TI* __restrict__ vx, const TI* __restrict__ vy, const TI* __restrict__ vz,
-                            T* __restrict__ rhs) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long n = (long long)nx * ny * nz;
-    if (i >= n) return;
+__device__ __forceinline__ void build_rhs_cell(long long i, int nx, int ny, int nz, T h0, T h1, T h2,
+                                               const TI* __restrict__ phi, const TI* __restrict__ lwx,
+                                               const TI* __restrict__ lwy, const TI* __restrict__ lwz,
+                                               const TI* __restrict__ vx, const TI* __restrict__ vy,
+                                               const TI* __restrict__ vz, T* __restrict__ rhs) {
+    (void)nx;
     if constexpr (!std::is_same<T, TI>::value)  // the FP64 copy is read only where phi <= 0
         if (T(phi[i]) > T(0)) return;
     T b = T(0);
@@ -361,6 +392,29 @@ __global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const TI* 
         b = X<T>::add(b, X<T>::div(X<T>::mul(T(lwz[fzi]), T(vz[fzi])), h2));
     }
     rhs[i] = b;
+}
+
+template <class T, class TI = T>
+__global__ void k_build_rhs(int nx, int ny, int nz, T h0, T h1, T h2, const TI* __restrict__ phi,
+                            const TI* __restrict__ lwx, const TI* __restrict__ lwy, const TI* __restrict__ lwz,
+                            const TI* __restrict__ vx, const TI* __restrict__ vy, const TI* __restrict__ vz,
+                            T* __restrict__ rhs) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nx * ny * nz) return;
+    build_rhs_cell<T, TI>(i, nx, ny, nz, h0, h1, h2, phi, lwx, lwy, lwz, vx, vy, vz, rhs);
+}
+
+// The mixed mode's two right-hand sides (FP32 for the loop, FP64 for the
+// outer residual) from one read of the fields, each in its own arithmetic.
+template <class T>
+__global__ void k_build_rhs_mixed(int nx, int ny, int nz, T h0, T h1, T h2, double hd0, double hd1, double hd2,
+                                  const T* __restrict__ phi, const T* __restrict__ lwx, const T* __restrict__ lwy,
+                                  const T* __restrict__ lwz, const T* __restrict__ vx, const T* __restrict__ vy,
+                                  const T* __restrict__ vz, T* __restrict__ rhs, double* __restrict__ rhs_hi) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nx * ny * nz) return;
+    build_rhs_cell<T, T>(i, nx, ny, nz, h0, h1, h2, phi, lwx, lwy, lwz, vx, vy, vz, rhs);
+    build_rhs_cell<double, T>(i, nx, ny, nz, hd0, hd1, hd2, phi, lwx, lwy, lwz, vx, vy, vz, rhs_hi);
 }
 
 // ------------------------------------------------------------ active tiles
@@ -1844,14 +1898,15 @@ template <class T, class TX> void LiquidImpl<T, TX>::solver_init() {
 
 template <class T, class TX> void LiquidImpl<T, TX>::build_rhs() {
     auto ps_ = scope(LHI_KERNEL_GRID);
-    k_build_rhs<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], liquid_phi_,
-                                                              lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_);
-    LHI_LAUNCH_CHECK();
     if constexpr (kHiResidual) {
-        k_build_rhs<double, T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(
-            nx_, ny_, nz_, dxd_[0], dxd_[1], dxd_[2], liquid_phi_, lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_hi_);
-        LHI_LAUNCH_CHECK();
+        k_build_rhs_mixed<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(
+            nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], dxd_[0], dxd_[1], dxd_[2], liquid_phi_, lw_[0], lw_[1], lw_[2],
+            v_[0], v_[1], v_[2], rhs_, rhs_hi_);
+    } else {
+        k_build_rhs<T><<<blocks_for(ncell_, 256), 256, 0, cur_>>>(nx_, ny_, nz_, dx_[0], dx_[1], dx_[2], liquid_phi_,
+                                                                  lw_[0], lw_[1], lw_[2], v_[0], v_[1], v_[2], rhs_);
     }
+    LHI_LAUNCH_CHECK();
 }
 
 // CGSolver<3>::BuildLHS (PressureSolver.cpp:544-664) for every level, then
@@ -1876,18 +1931,23 @@ template <class T, class TX> void LiquidImpl<T, TX>::build_lhs(double rho, doubl
             LHI_LAUNCH_CHECK();
         }
         const T* phi = (l == 0) ? liquid_phi_ : L.phi;
-        k_level_matrix<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
-            g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1], L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1], L.cf[2],
-            l == 0 ? L.type : nullptr, L.tile_flag, L.tdim[1], L.tdim[2], (l == 0 && L.fused) ? L.mask : nullptr,
-            L.mpitch);
-        LHI_LAUNCH_CHECK();
+        bool done = false;
         if constexpr (kHiResidual) {
-            if (l == 0) {
-                k_level_matrix<double, T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
-                    g, liquid_phi_, lw_[0], lw_[1], lw_[2], dxd_[0], dxd_[1], dxd_[2], dt, rho, diag_hi_, cf_hi_[0],
-                    cf_hi_[1], cf_hi_[2], nullptr, nullptr, 0, 0, nullptr, 0);
+            if (l == 0) {  // with the FP64 matrix of the outer residual
+                k_level_matrix_mixed<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
+                    g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1], L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1],
+                    L.cf[2], L.type, L.tile_flag, L.tdim[1], L.tdim[2], L.fused ? L.mask : nullptr, L.mpitch, dxd_[0],
+                    dxd_[1], dxd_[2], dt, rho, diag_hi_, cf_hi_[0], cf_hi_[1], cf_hi_[2]);
                 LHI_LAUNCH_CHECK();
+                done = true;
             }
+        }
+        if (!done) {
+            k_level_matrix<T><<<blocks_for(L.n, 256), 256, 0, cur_>>>(
+                g, phi, lw_[0], lw_[1], lw_[2], L.h[0], L.h[1], L.h[2], T(dt), T(rho), L.diag, L.cf[0], L.cf[1],
+                L.cf[2], l == 0 ? L.type : nullptr, L.tile_flag, L.tdim[1], L.tdim[2],
+                (l == 0 && L.fused) ? L.mask : nullptr, L.mpitch);
+            LHI_LAUNCH_CHECK();
         }
     }
     build_tiles();
