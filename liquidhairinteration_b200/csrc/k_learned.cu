@@ -720,21 +720,6 @@ __global__ void __launch_bounds__(128) k_umma_selftest(const uint16_t* __restric
     if (warp == 0) tmem_dealloc(tmem, 64);
 }
 
-// db[c] += sum_v g[v][c]
-__global__ void k_bias_grad(const uint16_t* __restrict__ g, int cpad, int creal, long long nvox, float* __restrict__ db) {
-    __shared__ float part[64];
-    if (threadIdx.x < 64) part[threadIdx.x] = 0.f;
-    __syncthreads();
-    const int c = threadIdx.x % cpad;
-    const int lanes = blockDim.x / cpad;
-    float acc = 0.f;
-    for (long long v = (long long)blockIdx.x * lanes + threadIdx.x / cpad; v < nvox; v += (long long)gridDim.x * lanes)
-        acc += bf16_float(g[v * cpad + c]);
-    atomicAdd(&part[c], acc);
-    __syncthreads();
-    if (threadIdx.x < creal) atomicAdd(&db[threadIdx.x], part[threadIdx.x]);
-}
-
 // ------------------------------------------------------------ elementwise
 __device__ __forceinline__ void dec3(long long v, int ny, int nz, int& x, int& y, int& z) {
     z = int(v % nz);
@@ -1595,25 +1580,16 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     const long long V0 = b_.vox[0], V1 = b_.vox[1], V2 = b_.vox[2];
     auto WB = [&](int l) { return wbwd_ + wbwd_off_[l]; };
     auto GW = [&](int l) { return grad_ + net_param_offset(l); };
-    auto GB = [&](int l) { return grad_ + net_param_offset(l) + (long long)kNetTaps * kNetCout[l] * kNetCin[l]; };
-    auto bias_grad = [&](const uint16_t* g, int cpad, int creal, long long nv, float* db) {
-        (void)g, (void)cpad, (void)creal, (void)db;
-        return;  // bias-free network: the bias entries keep zero gradient
-        if (nv == 0) return;
-        k_bias_grad<<<std::min<unsigned>(nb(nv * cpad), 512), 256, 0, s>>>(g, cpad, creal, nv, db);
-        LHI_LAUNCH_CHECK();
-    };
+    // the network is bias-free: the packed bias entries keep zero gradient
     // layer 5
     k_net_dy<<<nb(V0), 256, 0, s>>>(dz, last_type_, V0, scale_, b_.g[5]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[5], 16, 1, b_.u0, 16, 16, d0, GW(5), status_, s);
-    bias_grad(b_.g[5], 16, 1, V0, GB(5));
     launch_conv(b_.g[5], 16, WB(5), 16, nullptr, 16, d0, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     // layer 4
     k_relu_grad<<<nb(V0 * 16), 256, 0, s>>>(b_.dx, b_.u0, V0 * 16, relu_ ? 1 : 0, b_.g[4]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[4], 16, 16, b_.q0, 32, 32, d0, GW(4), status_, s);
-    bias_grad(b_.g[4], 16, 16, V0, GB(4));
     launch_conv(b_.g[4], 16, WB(4), 32, nullptr, 32, d0, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     k_sum_children<<<nb(V1 * 32), 256, 0, s>>>(b_.dx, d0[1], d0[2], b_.acc, d1[0], d1[1], d1[2], 32);
     LHI_LAUNCH_CHECK();
@@ -1621,7 +1597,6 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     k_relu_grad<<<nb(V1 * 32), 256, 0, s>>>(b_.acc, b_.u1, V1 * 32, relu_ ? 1 : 0, b_.g[3]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[3], 32, 32, b_.q1, 64, 64, d1, GW(3), status_, s);
-    bias_grad(b_.g[3], 32, 32, V1, GB(3));
     launch_conv(b_.g[3], 32, WB(3), 64, nullptr, 64, d1, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     k_sum_children<<<nb(V2 * 64), 256, 0, s>>>(b_.dx, d1[1], d1[2], b_.acc, d2[0], d2[1], d2[2], 64);
     LHI_LAUNCH_CHECK();
@@ -1629,21 +1604,18 @@ void LearnedNet::backward(const float* dz, cudaStream_t s) {
     k_relu_grad<<<nb(V2 * 64), 256, 0, s>>>(b_.acc, b_.h2, V2 * 64, relu_ ? 1 : 0, b_.g[2]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[2], 64, 64, b_.p1, 32, 32, d2, GW(2), status_, s);
-    bias_grad(b_.g[2], 64, 64, V2, GB(2));
     launch_conv(b_.g[2], 64, WB(2), 32, nullptr, 32, d2, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     // layer 1: dh1 = g3 (skip) + unpool(dp1) / 8
     k_relu_grad_unpool<<<nb(V1 * 32), 256, 0, s>>>(b_.g[3], b_.dx, d2[0], d2[1], d2[2], b_.h1, d1[0], d1[1], d1[2], 32,
                                                     relu_ ? 1 : 0, b_.g[1]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[1], 32, 32, b_.p0, 16, 16, d1, GW(1), status_, s);
-    bias_grad(b_.g[1], 32, 32, V1, GB(1));
     launch_conv(b_.g[1], 32, WB(1), 16, nullptr, 16, d1, 1, nullptr, 0, nullptr, b_.dx, status_, s);
     // layer 0: dh0 = g4 (skip) + unpool(dp0) / 8
     k_relu_grad_unpool<<<nb(V0 * 16), 256, 0, s>>>(b_.g[4], b_.dx, d1[0], d1[1], d1[2], b_.h0, d0[0], d0[1], d0[2], 16,
                                                     relu_ ? 1 : 0, b_.g[0]);
     LHI_LAUNCH_CHECK();
     launch_wgrad(b_.g[0], 16, 16, b_.a0, 16, 4, d0, GW(0), status_, s);
-    bias_grad(b_.g[0], 16, 16, V0, GB(0));
 }
 
 int umma_selftest(const uint16_t* a_host, const uint16_t* b_host, int N, int K, float* d_host, int* stage) {
